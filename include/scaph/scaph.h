@@ -1,0 +1,239 @@
+/*
+ * scaph.h - C ABI of the B200 (sm_100a) Scaph BFS engine.
+ *
+ * Plain C: opaque handles, plain pointers and sizes, int status codes
+ * (0 = ok, negative = error, message in scaph_last_error()).  Nothing here
+ * exits the process or prints.  The reference engine reports errors with
+ * H_ERR -> printf + exit (src/gpu_engine.cuh:28-39) and assert; every entry
+ * point below returns a status instead.
+ *
+ * Each declaration names the reference interface (file:line in the
+ * N-E-E/Scaph tree) whose job it takes over.
+ */
+#ifndef SCAPH_H
+#define SCAPH_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+#define SCAPH_OK           0
+#define SCAPH_EINVAL      -1   /* bad argument                                */
+#define SCAPH_EIO         -2   /* file missing, short or unwritable           */
+#define SCAPH_ENOMEM      -3   /* host or device allocation failed            */
+#define SCAPH_ECUDA       -4   /* CUDA runtime error                          */
+#define SCAPH_EFORMAT     -5   /* paged-CSR files inconsistent                */
+#define SCAPH_ETIMEOUT    -6   /* a bounded device wait gave up               */
+#define SCAPH_EUNSUPPORTED -7  /* feature not available for this graph/config */
+#define SCAPH_EDEVICE     -8   /* a kernel reported a bad index / overflow    */
+
+/* Message of the last failing call on this thread ("" if none). */
+const char *scaph_last_error(void);
+/* Library version string. */
+const char *scaph_version(void);
+
+/* ---- on-disk / in-memory records (byte layouts of the reference) ------- */
+
+/* One page descriptor of <p>page.info.  Same 16-byte layout as
+ * `struct Page` (tools/pagegencsr.cpp:74-80, src/page.h:22-28). */
+typedef struct scaph_page_info {
+    uint32_t left;      /* first vertex of the page                          */
+    uint32_t right;     /* last vertex of the page (inclusive)               */
+    uint32_t nodenum;   /* right - left + 1                                  */
+    uint32_t edgenum;   /* edges stored in the page                          */
+} scaph_page_info;
+
+/* <p>graph.info: 16 bytes {u32 pagesize_words, u32 V, u64 E}, as written by
+ * save_graph_info (tools/pagegencsr.cpp:82-87,181-195).  (The reference
+ * loader reads only the first 12 bytes, src/graph.h:79-86; this one reads
+ * all 16.) */
+typedef struct scaph_graph_info {
+    uint32_t pagesize;  /* words per page file                               */
+    uint32_t V;
+    uint64_t E;
+    int32_t  npages;
+    int32_t  weighted;  /* pages hold {ngr,wgh} pairs (src/page.h:39-46)     */
+} scaph_graph_info;
+
+/* Flat CSR held by the library (generators, readers).  idx has V+1 64-bit
+ * offsets, ngh has E neighbour ids, wgh is NULL or E weights. */
+typedef struct scaph_csr {
+    uint32_t  V;
+    uint64_t  E;
+    uint64_t *idx;
+    uint32_t *ngh;
+    uint32_t *wgh;
+} scaph_csr;
+
+/* ---- synthetic graph generators (seeded, deterministic for any thread
+ *      count).  Output adjacency lists are sorted and duplicate-free. ----- */
+
+/* RMAT (Chakrabarti et al.) with quadrant probabilities a,b,c (d=1-a-b-c):
+ * 2^scale vertices, round(edgefactor*2^scale/2) generated pairs, self-loops
+ * and duplicates removed, symmetrised (so E ~ edgefactor*V directed edges).
+ * scramble != 0 relabels vertices by a seeded permutation. */
+int scaph_gen_rmat(int scale, double edgefactor, double a, double b, double c,
+                   uint64_t seed, int scramble, scaph_csr *out);
+
+/* Directed power-law graph: out-degrees Zipf-like with exponent `zipf_s`
+ * (capped at max_degree), destinations by preferential attachment
+ * (copy model, probability proportional to in-degree + 1).  ~E edges. */
+int scaph_gen_powerlaw(uint32_t V, uint64_t E, double zipf_s, uint32_t max_degree,
+                       uint64_t seed, scaph_csr *out);
+
+/* Directed web-crawl-like graph: power-law out-degrees (exponent s, capped),
+ * a fraction `local_frac` of each vertex's edges inside its block of `block`
+ * consecutive ids, the rest uniform over all vertices. */
+int scaph_gen_web(uint32_t V, uint64_t E, double s, uint32_t max_degree,
+                  uint32_t block, double local_frac, uint64_t seed, scaph_csr *out);
+
+/* Reverse every edge (in-edge CSR for pull on directed graphs). */
+int scaph_csr_transpose(const scaph_csr *in, scaph_csr *out);
+/* Copies caller arrays into a library-owned CSR. */
+int scaph_csr_from_arrays(uint32_t V, uint64_t E, const uint64_t *idx,
+                          const uint32_t *ngh, const uint32_t *wgh, scaph_csr *out);
+void scaph_csr_free(scaph_csr *csr);
+
+/* Flat CSR files <p>_csr.idx (u32[V+1]), _csr.ngh (u32[E]), _csr.deg (u32[V])
+ * and _csr.wgh (u32[E]; written as zeros when csr->wgh is NULL because the
+ * reference generator always reads it, tools/pagegencsr.cpp:281-287).
+ * Same files that fetch_graph reads (src/graph.h:27-75). */
+int scaph_csr_write(const char *prefix, const scaph_csr *csr);
+int scaph_csr_read(const char *prefix, int with_weights, scaph_csr *out);
+
+/* ---- paged CSR --------------------------------------------------------- */
+
+/* Writes <p>page<N>, <p>page.info and <p>graph.info byte-identical to
+ * tools/pagegencsr.cpp (page_gen, :197-252): greedy cut so that
+ * 3*nodes + edges (x2 if weighted) < pagesize_words, Node{vtx,idx,len}
+ * triples then the edges, zero-padded to pagesize_words.  A vertex whose
+ * adjacency alone does not fit a page is rejected (SCAPH_EUNSUPPORTED). */
+int scaph_pages_write(const char *prefix, const scaph_csr *csr,
+                      uint32_t pagesize_words, int weighted);
+
+typedef struct scaph_graph scaph_graph;
+
+/* Loads a paged CSR written by pagegencsr / scaph_pages_write into host
+ * memory (replaces fetch_graph, src/graph.h:24-108).  The flat _csr.* files
+ * are not needed; degrees come from the page Node records.  `weighted` says
+ * whether the pages hold {ngr,wgh} pairs; the reference decides this at
+ * compile time (-DAPPSSSP -> WEIGHT, src/graph.h:7-9). */
+int scaph_graph_open(const char *prefix, int weighted, scaph_graph **g);
+/* Pages a flat CSR in memory with the same cut rule (no files). */
+int scaph_graph_from_csr(const scaph_csr *csr, uint32_t pagesize_words,
+                         int weighted, scaph_graph **g);
+int scaph_graph_get_info(const scaph_graph *g, scaph_graph_info *info);
+/* Host view of page p (pagesize words) and of the page list. */
+const uint32_t *scaph_graph_page(const scaph_graph *g, int p);
+const scaph_page_info *scaph_graph_page_list(const scaph_graph *g);
+/* Per-vertex out-degree (u32[V]), the reference's csr_deg / d_degree. */
+const uint32_t *scaph_graph_degree(const scaph_graph *g);
+void scaph_graph_close(scaph_graph *g);
+
+/* ---- engine ------------------------------------------------------------ */
+
+/* Direction policy (the reference has only push: gpu_push_csr,
+ * src/gpu_engine.cuh:41-169; gpu_pull_iteration is a stub, src/app.cuh:365-369). */
+#define SCAPH_DIR_ALPHABETA 0   /* Beamer alpha/beta switch (plain engine)    */
+#define SCAPH_DIR_PUSH      1   /* top-down every level                       */
+#define SCAPH_DIR_PULL      2   /* bottom-up every level after the first      */
+#define SCAPH_DIR_LEARNED   3   /* MLP scheduler (falls back to alpha/beta)   */
+
+/* Engine configuration; zero-initialise and set what you need
+ * (replaces the FLAGS_* globals, src/app.cuh:38-52). */
+typedef struct scaph_config {
+    int64_t  pool_bytes;       /* HBM page-pool cap; 0 = every page resident
+                                  (FLAGS_max_memory, src/app.cuh:39,152)    */
+    uint32_t unreached;        /* depth of unreached vertices; 0 = 0xFFFFFFFF
+                                  (reference app uses 63, app/bfs.cu:18)    */
+    int32_t  direction;        /* SCAPH_DIR_*                               */
+    float    alpha;            /* 0 -> 14                                   */
+    float    beta;             /* 0 -> 24                                   */
+    int32_t  block_size;       /* threads per CTA of the level kernels; 0=256
+                                  (FLAGS_num_thds, src/app.cuh:43)          */
+    int32_t  ctas_per_sm;      /* 0 = from occupancy                        */
+    int32_t  copy_streams;     /* side streams for page staging; 0 = 2
+                                  (FLAGS_num_stream, src/app.cuh:41)        */
+    int32_t  prefetch;         /* out-of-core: 1 = prefetch predicted pages */
+    int32_t  compact_threshold;/* out-of-core: pages with active data <=
+                                  threshold/32 of a page are read zero-copy
+                                  instead of copied (FLAGS_threshold,
+                                  src/app.cuh:45,151); 0 = 3                */
+    int32_t  use_graph;        /* 1 = run each BFS as one CUDA-graph launch */
+    int32_t  device;           /* CUDA device ordinal                       */
+    void    *stream;           /* cudaStream_t to run on; NULL = own stream */
+} scaph_config;
+
+typedef struct scaph_engine scaph_engine;
+
+/* Uploads the graph (all pages, or up to pool_bytes of them) and allocates
+ * the per-vertex state (replaces App::App + App::load_graph,
+ * src/app.cuh:137-156,267-345).  `gt` is the transposed graph used by pull
+ * on directed graphs; NULL means the graph is symmetric and pull reads g. */
+int scaph_engine_create(const scaph_graph *g, const scaph_graph *gt,
+                        const scaph_config *cfg, scaph_engine **e);
+int scaph_engine_destroy(scaph_engine *e);
+
+/* Per-run summary. */
+typedef struct scaph_bfs_stats {
+    int32_t  levels;            /* BFS levels executed                      */
+    int32_t  push_levels;
+    int32_t  pull_levels;
+    int32_t  _pad;
+    uint64_t reached;           /* vertices with a finite depth             */
+    uint64_t reached_edges;     /* sum of out-degrees of reached vertices   */
+    uint64_t edges_inspected;   /* adjacency words read by the kernels      */
+    uint64_t alg_bytes;         /* algorithmic HBM bytes    */
+    uint64_t h2d_bytes;         /* page bytes copied host->HBM              */
+    uint64_t zc_bytes;          /* page bytes read zero-copy over PCIe      */
+    uint64_t page_faults;       /* page loads on demand                     */
+    uint64_t prefetched;        /* page loads issued ahead by the scheduler */
+    double   ms;                /* device time of the traversal (events)    */
+} scaph_bfs_stats;
+
+/* Single-source level-synchronous BFS (replaces App::run, src/app.cuh:220-265,
+ * with the bfs app hooks app/bfs.cu:20-37, app/bfs_kernel.cuh:6-16).
+ * depths: u32[V] (unreached = cfg.unreached); parents: u32[V] or NULL
+ * (parent[src] = src, unreached = 0xFFFFFFFF).  out_on_device != 0 means the
+ * pointers are device pointers; otherwise host memory (copied back).
+ * stats may be NULL. */
+int scaph_bfs(scaph_engine *e, uint32_t src, uint32_t *depths, uint32_t *parents,
+              int out_on_device, scaph_bfs_stats *stats);
+
+/* Per-level trace of the last scaph_bfs (direction, frontier, edges, time,
+ * per-page histogram).  Writes up to `cap` records, returns the count. */
+typedef struct scaph_level_trace {
+    int32_t  level;
+    int32_t  direction;         /* 0 push, 1 pull                           */
+    uint64_t frontier;          /* vertices in the frontier of this level   */
+    uint64_t frontier_edges;    /* their out-degree sum                     */
+    uint64_t unvisited;         /* vertices not yet reached                 */
+    uint64_t unvisited_edges;   /* their out-degree sum                     */
+    uint64_t next;              /* vertices discovered by this level        */
+    uint64_t edges_inspected;
+    uint64_t h2d_bytes;
+    double   ms;
+} scaph_level_trace;
+int scaph_bfs_trace(const scaph_engine *e, scaph_level_trace *out, int cap);
+/* Active-vertex histogram of the frontier at `level` of the last run:
+ * nodes[p] / datas[p] as get_page_info computes them (src/gpu_engine.cuh:397-441). */
+int scaph_bfs_page_hist(const scaph_engine *e, int level, uint32_t *nodes,
+                        uint32_t *datas, int npages);
+
+/* ---- host helpers ------------------------------------------------------ */
+
+/* Page-locked host memory for outputs copied back by scaph_bfs (faster
+ * device->host copies than pageable memory).  NULL on failure. */
+void *scaph_host_alloc(size_t bytes);
+void scaph_host_free(void *p);
+/* Number of CUDA devices visible (0 when there is no GPU). */
+int scaph_device_count(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SCAPH_H */

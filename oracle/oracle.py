@@ -1,0 +1,158 @@
+"""ctypes front end of the CPU oracle (TEST INFRASTRUCTURE ONLY).
+
+Imported only by tests/, __graft_entry__.smoke() and bench.py's CPU-baseline
+legs, as the checker.  The engine (scaph_b200) never imports this module.
+
+* liboracle.so      - bfs_oracle.c, the C restatement of the reference's
+                      CPU BFS (app/bfs.cu:70-101) and helpers.
+* _ref/libscaphref.so, _ref/pagegencsr - the reference's own code compiled
+                      from its sources by oracle/Makefile (only present where
+                      the reference tree was available at build time).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ORACLE_SO = os.path.join(HERE, "liboracle.so")
+REF_SO = os.path.join(HERE, "_ref", "libscaphref.so")
+REF_PAGEGEN = os.path.join(HERE, "_ref", "pagegencsr")
+
+_o = None
+_r = None
+
+
+def _p(a):
+    return None if a is None else C.c_void_p(a.ctypes.data)
+
+
+def olib() -> C.CDLL:
+    global _o
+    if _o is None:
+        if not os.path.exists(ORACLE_SO):
+            raise RuntimeError(f"{ORACLE_SO} missing: run `make -C oracle`")
+        L = C.CDLL(ORACLE_SO)
+        vp, u32, i64, i32 = C.c_void_p, C.c_uint32, C.c_int64, C.c_int
+        L.oracle_bfs.argtypes = [u32, vp, vp, u32, u32, vp]
+        L.oracle_bfs.restype = i64
+        L.oracle_bfs_omp.argtypes = [u32, vp, vp, u32, u32, vp, i32]
+        L.oracle_bfs_omp.restype = i64
+        L.oracle_bfs_paged.argtypes = [u32, i64, vp, vp, i32, u32, u32, vp]
+        L.oracle_bfs_paged.restype = i64
+        L.oracle_validate_tree.argtypes = [u32, vp, vp, u32, u32, vp, vp, C.POINTER(u32)]
+        L.oracle_validate_tree.restype = i32
+        L.oracle_page_stats.argtypes = [i64, vp, vp, vp, i32, vp, vp, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
+        L.oracle_page_stats.restype = None
+        L.oracle_compact_page.argtypes = [vp, vp, vp, u32, u32, u32, i32]
+        L.oracle_compact_page.restype = u32
+        L.oracle_max_zero_run.argtypes = [u32]
+        L.oracle_max_zero_run.restype = i32
+        L.oracle_fit_zero_run.argtypes = [u32, i32]
+        L.oracle_fit_zero_run.restype = i32
+        L.oracle_set_run.argtypes = [u32, i32, i32, i32]
+        L.oracle_set_run.restype = u32
+        _o = L
+    return _o
+
+
+def ref_available() -> bool:
+    return os.path.exists(REF_SO)
+
+
+def rlib() -> C.CDLL:
+    global _r
+    if _r is None:
+        L = C.CDLL(REF_SO)
+        vp, u32, i32 = C.c_void_p, C.c_uint, C.c_int
+        L.ref_bfs_check.argtypes = [u32, vp, vp, u32, vp, C.POINTER(C.c_longlong), C.POINTER(C.c_double)]
+        L.ref_bfs_check.restype = i32
+        L.ref_compress_stat.argtypes = [vp, vp, vp, u32, u32, u32]
+        L.ref_compress_stat.restype = u32
+        L.ref_max_zero_run.argtypes = [i32]
+        L.ref_max_zero_run.restype = i32
+        L.ref_fit_zero_run.argtypes = [i32, i32]
+        L.ref_fit_zero_run.restype = i32
+        L.ref_set_run.argtypes = [i32, i32, i32, i32]
+        L.ref_set_run.restype = i32
+        _r = L
+    return _r
+
+
+def _csr(idx, ngh):
+    return np.ascontiguousarray(idx, np.uint64), np.ascontiguousarray(ngh, np.uint32)
+
+
+def bfs(idx, ngh, src: int, unreached: int = 0xFFFFFFFF) -> np.ndarray:
+    """Single-threaded level-synchronous BFS (app/bfs.cu:70-101)."""
+    idx, ngh = _csr(idx, ngh)
+    V = len(idx) - 1
+    d = np.empty(V, np.uint32)
+    if olib().oracle_bfs(V, _p(idx), _p(ngh), src, unreached, _p(d)) < 0:
+        raise ValueError("oracle_bfs: bad input")
+    return d
+
+
+def bfs_omp(idx, ngh, src: int, unreached: int = 0xFFFFFFFF, threads: int = 0) -> np.ndarray:
+    idx, ngh = _csr(idx, ngh)
+    V = len(idx) - 1
+    d = np.empty(V, np.uint32)
+    if olib().oracle_bfs_omp(V, _p(idx), _p(ngh), src, unreached, _p(d), threads) < 0:
+        raise ValueError("oracle_bfs_omp: bad input")
+    return d
+
+
+def bfs_paged(V: int, page_list: np.ndarray, pages: list, src: int, unreached: int = 0xFFFFFFFF,
+              weighted: bool = False) -> np.ndarray:
+    pl = np.ascontiguousarray(page_list, np.uint32)
+    ptrs = (C.c_void_p * len(pages))(*[p.ctypes.data for p in pages])
+    d = np.empty(V, np.uint32)
+    if olib().oracle_bfs_paged(V, len(pages), _p(pl), ptrs, int(weighted), src, unreached, _p(d)) < 0:
+        raise ValueError("oracle_bfs_paged: bad input")
+    return d
+
+
+def validate_tree(idx, ngh, src: int, depth: np.ndarray, parent: np.ndarray, unreached: int = 0xFFFFFFFF):
+    """Returns (code, vertex): code 0 = valid BFS tree."""
+    idx, ngh = _csr(idx, ngh)
+    depth = np.ascontiguousarray(depth, np.uint32)
+    parent = np.ascontiguousarray(parent, np.uint32)
+    bad = C.c_uint32(0)
+    rc = olib().oracle_validate_tree(len(idx) - 1, _p(idx), _p(ngh), src, unreached, _p(depth), _p(parent),
+                                     C.byref(bad))
+    return rc, bad.value
+
+
+def page_stats(page_list, stat, degree, weighted=False):
+    pl = np.ascontiguousarray(page_list, np.uint32)
+    stat = np.ascontiguousarray(stat, np.uint8)
+    degree = np.ascontiguousarray(degree, np.uint32)
+    n = len(pl)
+    nodes = np.zeros(n, np.uint32)
+    datas = np.zeros(n, np.uint32)
+    tn, td = C.c_int64(), C.c_int64()
+    olib().oracle_page_stats(n, _p(pl), _p(stat), _p(degree), int(weighted), _p(nodes), _p(datas),
+                             C.byref(tn), C.byref(td))
+    return nodes, datas, tn.value, td.value
+
+
+def compact_page(page_src, stat, left, srcnodenum, dstnodenum, weighted=False, out_words=None):
+    src = np.ascontiguousarray(page_src, np.uint32)
+    stat = np.ascontiguousarray(stat, np.uint8)
+    dst = np.zeros(out_words or len(src), np.uint32)
+    n = olib().oracle_compact_page(_p(src), _p(dst), _p(stat), left, srcnodenum, dstnodenum, int(weighted))
+    return dst, n
+
+
+def ref_bfs_check(idx32, ngh, src: int, values: np.ndarray):
+    """Runs the reference's own bfs::check; returns (mismatches, seconds)."""
+    idx32 = np.ascontiguousarray(idx32, np.uint32)
+    ngh = np.ascontiguousarray(ngh, np.uint32)
+    values = np.ascontiguousarray(values, np.uint32).copy()
+    err, sec = C.c_longlong(), C.c_double()
+    rc = rlib().ref_bfs_check(len(idx32) - 1, _p(idx32), _p(ngh), src, _p(values), C.byref(err), C.byref(sec))
+    if rc != 0:
+        raise RuntimeError("ref_bfs_check: could not parse the reference output")
+    return err.value, sec.value

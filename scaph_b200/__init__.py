@@ -1,0 +1,341 @@
+"""scaph_b200 - the Scaph BFS hot path rebuilt for B200 (sm_100a).
+
+Python mirror of the C ABI in include/scaph/scaph.h (libscaph.so, built
+in-tree by scaph_b200/Makefile).  The engine itself is C++/CUDA; this module
+only marshals arguments with ctypes and numpy.  There is no CPU fallback: if
+libscaph.so is missing, importing the engine raises ScaphError.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libscaph.so")
+
+# status codes (include/scaph/scaph.h)
+OK, EINVAL, EIO, ENOMEM, ECUDA, EFORMAT, ETIMEOUT, EUNSUPPORTED, EDEVICE = 0, -1, -2, -3, -4, -5, -6, -7, -8
+DIR_ALPHABETA, DIR_PUSH, DIR_PULL, DIR_LEARNED = 0, 1, 2, 3
+UNREACHED = 0xFFFFFFFF
+REF_UNREACHED = 63  # MAXDEPTH of the reference BFS app (app/bfs.cu:18)
+
+
+class ScaphError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"scaph error {code}: {msg}")
+        self.code = code
+
+
+class _Csr(C.Structure):
+    _fields_ = [("V", C.c_uint32), ("E", C.c_uint64), ("idx", C.POINTER(C.c_uint64)),
+                ("ngh", C.POINTER(C.c_uint32)), ("wgh", C.POINTER(C.c_uint32))]
+
+
+class _GraphInfo(C.Structure):
+    _fields_ = [("pagesize", C.c_uint32), ("V", C.c_uint32), ("E", C.c_uint64),
+                ("npages", C.c_int32), ("weighted", C.c_int32)]
+
+
+class _Config(C.Structure):
+    _fields_ = [("pool_bytes", C.c_int64), ("unreached", C.c_uint32), ("direction", C.c_int32),
+                ("alpha", C.c_float), ("beta", C.c_float), ("block_size", C.c_int32),
+                ("ctas_per_sm", C.c_int32), ("copy_streams", C.c_int32), ("prefetch", C.c_int32),
+                ("compact_threshold", C.c_int32), ("use_graph", C.c_int32), ("device", C.c_int32),
+                ("stream", C.c_void_p)]
+
+
+class _Stats(C.Structure):
+    _fields_ = [("levels", C.c_int32), ("push_levels", C.c_int32), ("pull_levels", C.c_int32),
+                ("_pad", C.c_int32), ("reached", C.c_uint64), ("reached_edges", C.c_uint64),
+                ("edges_inspected", C.c_uint64), ("alg_bytes", C.c_uint64), ("h2d_bytes", C.c_uint64),
+                ("zc_bytes", C.c_uint64), ("page_faults", C.c_uint64), ("prefetched", C.c_uint64),
+                ("ms", C.c_double)]
+
+
+class _Trace(C.Structure):
+    _fields_ = [("level", C.c_int32), ("direction", C.c_int32), ("frontier", C.c_uint64),
+                ("frontier_edges", C.c_uint64), ("unvisited", C.c_uint64), ("unvisited_edges", C.c_uint64),
+                ("next", C.c_uint64), ("edges_inspected", C.c_uint64), ("h2d_bytes", C.c_uint64),
+                ("ms", C.c_double)]
+
+
+_lib = None
+
+
+def lib() -> C.CDLL:
+    """Loads libscaph.so (once).  Raises ScaphError if it has not been built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ScaphError(EUNSUPPORTED, f"{LIB_PATH} not built (run __graft_entry__.build())")
+    L = C.CDLL(LIB_PATH)
+    P, u32, u64, i32, vp = C.POINTER, C.c_uint32, C.c_uint64, C.c_int, C.c_void_p
+    sig = {
+        "scaph_last_error": ([], C.c_char_p),
+        "scaph_version": ([], C.c_char_p),
+        "scaph_gen_rmat": ([i32, C.c_double, C.c_double, C.c_double, C.c_double, u64, i32, P(_Csr)], i32),
+        "scaph_gen_powerlaw": ([u32, u64, C.c_double, u32, u64, P(_Csr)], i32),
+        "scaph_gen_web": ([u32, u64, C.c_double, u32, u32, C.c_double, u64, P(_Csr)], i32),
+        "scaph_csr_transpose": ([P(_Csr), P(_Csr)], i32),
+        "scaph_csr_from_arrays": ([u32, u64, vp, vp, vp, P(_Csr)], i32),
+        "scaph_csr_free": ([P(_Csr)], None),
+        "scaph_csr_write": ([C.c_char_p, P(_Csr)], i32),
+        "scaph_csr_read": ([C.c_char_p, i32, P(_Csr)], i32),
+        "scaph_pages_write": ([C.c_char_p, P(_Csr), u32, i32], i32),
+        "scaph_graph_open": ([C.c_char_p, i32, P(vp)], i32),
+        "scaph_graph_from_csr": ([P(_Csr), u32, i32, P(vp)], i32),
+        "scaph_graph_get_info": ([vp, P(_GraphInfo)], i32),
+        "scaph_graph_page": ([vp, i32], P(u32)),
+        "scaph_graph_page_list": ([vp], P(u32)),
+        "scaph_graph_degree": ([vp], P(u32)),
+        "scaph_graph_close": ([vp], None),
+        "scaph_engine_create": ([vp, vp, P(_Config), P(vp)], i32),
+        "scaph_engine_destroy": ([vp], i32),
+        "scaph_bfs": ([vp, u32, vp, vp, i32, P(_Stats)], i32),
+        "scaph_bfs_trace": ([vp, P(_Trace), i32], i32),
+        "scaph_bfs_page_hist": ([vp, i32, vp, vp, i32], i32),
+        "scaph_host_alloc": ([C.c_size_t], vp),
+        "scaph_host_free": ([vp], None),
+        "scaph_device_count": ([], i32),
+    }
+    for name, (args, res) in sig.items():
+        f = getattr(L, name)
+        f.argtypes = args
+        f.restype = res
+    _lib = L
+    return L
+
+
+def _check(rc: int) -> int:
+    if rc < 0:
+        raise ScaphError(rc, lib().scaph_last_error().decode())
+    return rc
+
+
+def _ptr(a: np.ndarray | None) -> C.c_void_p | None:
+    return None if a is None else C.c_void_p(a.ctypes.data)
+
+
+def device_count() -> int:
+    return lib().scaph_device_count()
+
+
+# ---------------------------------------------------------------------------
+# flat CSR
+# ---------------------------------------------------------------------------
+class Csr:
+    """Library-owned flat CSR (64-bit offsets, 32-bit neighbour ids)."""
+
+    def __init__(self):
+        self._c = _Csr()
+
+    def __del__(self):
+        if getattr(self, "_c", None) is not None and lib is not None:
+            try:
+                lib().scaph_csr_free(C.byref(self._c))
+            except Exception:
+                pass
+
+    @property
+    def V(self) -> int:
+        return int(self._c.V)
+
+    @property
+    def E(self) -> int:
+        return int(self._c.E)
+
+    @property
+    def idx(self) -> np.ndarray:
+        return np.ctypeslib.as_array(self._c.idx, shape=(self.V + 1,))
+
+    @property
+    def ngh(self) -> np.ndarray:
+        if self.E == 0:
+            return np.zeros(0, np.uint32)
+        return np.ctypeslib.as_array(self._c.ngh, shape=(self.E,))
+
+    @property
+    def wgh(self) -> np.ndarray | None:
+        if not self._c.wgh or self.E == 0:
+            return None
+        return np.ctypeslib.as_array(self._c.wgh, shape=(self.E,))
+
+    def degree(self) -> np.ndarray:
+        return np.diff(self.idx).astype(np.uint32)
+
+    @classmethod
+    def rmat(cls, scale: int, edgefactor: float = 16.0, a=0.57, b=0.19, c=0.19, seed: int = 1,
+             scramble: bool = True) -> "Csr":
+        g = cls()
+        _check(lib().scaph_gen_rmat(scale, edgefactor, a, b, c, seed, int(scramble), C.byref(g._c)))
+        return g
+
+    @classmethod
+    def powerlaw(cls, V: int, E: int, zipf_s: float = 1.9, max_degree: int = 0, seed: int = 1) -> "Csr":
+        g = cls()
+        _check(lib().scaph_gen_powerlaw(V, E, zipf_s, max_degree, seed, C.byref(g._c)))
+        return g
+
+    @classmethod
+    def web(cls, V: int, E: int, s: float = 2.1, max_degree: int = 0, block: int = 4096,
+            local_frac: float = 0.9, seed: int = 1) -> "Csr":
+        g = cls()
+        _check(lib().scaph_gen_web(V, E, s, max_degree, block, local_frac, seed, C.byref(g._c)))
+        return g
+
+    @classmethod
+    def from_arrays(cls, idx, ngh, wgh=None) -> "Csr":
+        idx = np.ascontiguousarray(idx, dtype=np.uint64)
+        ngh = np.ascontiguousarray(ngh, dtype=np.uint32)
+        w = None if wgh is None else np.ascontiguousarray(wgh, dtype=np.uint32)
+        g = cls()
+        _check(lib().scaph_csr_from_arrays(len(idx) - 1, len(ngh), _ptr(idx), _ptr(ngh), _ptr(w), C.byref(g._c)))
+        return g
+
+    @classmethod
+    def read(cls, prefix: str, with_weights: bool = False) -> "Csr":
+        g = cls()
+        _check(lib().scaph_csr_read(prefix.encode(), int(with_weights), C.byref(g._c)))
+        return g
+
+    def transpose(self) -> "Csr":
+        t = Csr()
+        _check(lib().scaph_csr_transpose(C.byref(self._c), C.byref(t._c)))
+        return t
+
+    def write(self, prefix: str) -> None:
+        _check(lib().scaph_csr_write(prefix.encode(), C.byref(self._c)))
+
+    def write_pages(self, prefix: str, pagesize_words: int, weighted: bool = False) -> None:
+        _check(lib().scaph_pages_write(prefix.encode(), C.byref(self._c), pagesize_words, int(weighted)))
+
+
+# ---------------------------------------------------------------------------
+# paged CSR
+# ---------------------------------------------------------------------------
+class PagedGraph:
+    """Host copy of a paged CSR (the reference's h_page / h_page_list)."""
+
+    def __init__(self, handle: C.c_void_p, keep=None):
+        self._h = handle
+        self._keep = keep
+        info = _GraphInfo()
+        _check(lib().scaph_graph_get_info(self._h, C.byref(info)))
+        self.pagesize, self.V, self.E = int(info.pagesize), int(info.V), int(info.E)
+        self.npages, self.weighted = int(info.npages), bool(info.weighted)
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            try:
+                lib().scaph_graph_close(h)
+            except Exception:
+                pass
+            self._h = None
+
+    @classmethod
+    def open(cls, prefix: str, weighted: bool = False) -> "PagedGraph":
+        h = C.c_void_p()
+        _check(lib().scaph_graph_open(prefix.encode(), int(weighted), C.byref(h)))
+        return cls(h)
+
+    @classmethod
+    def from_csr(cls, csr: Csr, pagesize_words: int = 10 * 1024 * 1024, weighted: bool = False) -> "PagedGraph":
+        h = C.c_void_p()
+        _check(lib().scaph_graph_from_csr(C.byref(csr._c), pagesize_words, int(weighted), C.byref(h)))
+        return cls(h)
+
+    def page(self, p: int) -> np.ndarray:
+        ptr = lib().scaph_graph_page(self._h, p)
+        if not ptr:
+            raise ScaphError(EINVAL, f"page {p} out of range")
+        return np.ctypeslib.as_array(ptr, shape=(self.pagesize,))
+
+    def page_list(self) -> np.ndarray:
+        """Page{left,right,nodenum,edgenum}[npages] as an (npages, 4) uint32 array."""
+        ptr = lib().scaph_graph_page_list(self._h)
+        return np.ctypeslib.as_array(ptr, shape=(self.npages, 4))
+
+    def degree(self) -> np.ndarray:
+        return np.ctypeslib.as_array(lib().scaph_graph_degree(self._h), shape=(self.V,))
+
+
+@dataclass
+class BfsStats:
+    levels: int
+    push_levels: int
+    pull_levels: int
+    reached: int
+    reached_edges: int
+    edges_inspected: int
+    alg_bytes: int
+    h2d_bytes: int
+    zc_bytes: int
+    page_faults: int
+    prefetched: int
+    ms: float
+
+
+def _stats(s: _Stats) -> BfsStats:
+    return BfsStats(s.levels, s.push_levels, s.pull_levels, s.reached, s.reached_edges, s.edges_inspected,
+                    s.alg_bytes, s.h2d_bytes, s.zc_bytes, s.page_faults, s.prefetched, s.ms)
+
+
+class Engine:
+    """Device BFS engine over a paged graph (scaph_engine_create)."""
+
+    def __init__(self, graph: PagedGraph, transposed: PagedGraph | None = None, *, pool_bytes: int = 0,
+                 unreached: int = UNREACHED, direction: int = DIR_ALPHABETA, alpha: float = 14.0,
+                 beta: float = 24.0, block_size: int = 256, ctas_per_sm: int = 0, copy_streams: int = 2,
+                 prefetch: int = 0, compact_threshold: int = 3, use_graph: int = 0, device: int = 0,
+                 stream: int | None = None):
+        self.graph, self.transposed = graph, transposed
+        cfg = _Config(pool_bytes, unreached, direction, alpha, beta, block_size, ctas_per_sm, copy_streams,
+                      prefetch, compact_threshold, use_graph, device, stream)
+        self._cfg = cfg
+        h = C.c_void_p()
+        _check(lib().scaph_engine_create(graph._h, transposed._h if transposed else None, C.byref(cfg), C.byref(h)))
+        self._h = h
+        self.V = graph.V
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().scaph_engine_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def bfs(self, src: int, parents: bool = False, depth_out: np.ndarray | None = None,
+            parent_out: np.ndarray | None = None):
+        """Runs one BFS; returns (depth, parent or None, BfsStats) as host arrays."""
+        d = depth_out if depth_out is not None else np.empty(self.V, np.uint32)
+        p = parent_out if parent_out is not None else (np.empty(self.V, np.uint32) if parents else None)
+        st = _Stats()
+        _check(lib().scaph_bfs(self._h, src, _ptr(d), _ptr(p), 0, C.byref(st)))
+        return d, p, _stats(st)
+
+    def bfs_device(self, src: int, depth_ptr: int, parent_ptr: int | None = None) -> BfsStats:
+        """Runs one BFS writing into device buffers (raw CUDA pointers)."""
+        st = _Stats()
+        _check(lib().scaph_bfs(self._h, src, C.c_void_p(depth_ptr), C.c_void_p(parent_ptr) if parent_ptr else None,
+                               1, C.byref(st)))
+        return _stats(st)
+
+    def trace(self) -> list[dict]:
+        buf = (_Trace * 4096)()
+        n = _check(lib().scaph_bfs_trace(self._h, buf, 4096))
+        return [{f: getattr(buf[i], f) for f, _ in _Trace._fields_} for i in range(n)]
+
+    def page_hist(self, level: int):
+        n = np.zeros(self.graph.npages, np.uint32)
+        d = np.zeros(self.graph.npages, np.uint32)
+        _check(lib().scaph_bfs_page_hist(self._h, level, _ptr(n), _ptr(d), self.graph.npages))
+        return n, d

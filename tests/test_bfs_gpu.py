@@ -1,0 +1,154 @@
+"""Parity of the sm_100a BFS engine with the CPU oracle, through the C ABI.
+
+Depths must be bit-exact (integer work); parents must form a valid BFS tree.
+"""
+import numpy as np
+import pytest
+
+import scaph_b200 as S
+from oracle import oracle as O
+from tests import graphs as G
+
+pytestmark = pytest.mark.gpu
+
+DIRS = [S.DIR_ALPHABETA, S.DIR_PUSH, S.DIR_PULL]
+
+
+def check_run(csr, g, src, gt=None, direction=S.DIR_ALPHABETA, unreached=S.UNREACHED, tcsr=None, **kw):
+    eng = S.Engine(g, gt, direction=direction, unreached=unreached, **kw)
+    depth, parent, st = eng.bfs(src, parents=True)
+    ref = O.bfs(csr.idx, csr.ngh, src, unreached)
+    mism = np.flatnonzero(depth != ref)
+    assert mism.size == 0, f"src {src} dir {direction}: {mism.size} mismatches, first v={mism[0]} " \
+                           f"gpu={depth[mism[0]]} cpu={ref[mism[0]]}"
+    rc, bad = O.validate_tree(csr.idx, csr.ngh, src, depth, parent, unreached)
+    assert rc == 0, f"invalid tree code {rc} at {bad}"
+    assert st.reached == int((ref != unreached).sum())
+    trace = eng.trace()
+    eng.close()
+    return depth, st, trace
+
+
+@pytest.fixture(scope="module")
+def rmat16():
+    csr = S.Csr.rmat(16, 16, seed=G.SEED + 0)
+    return csr, S.PagedGraph.from_csr(csr)  # 10 Mi-word pages, like the reference default
+
+
+@pytest.mark.parametrize("direction", DIRS)
+def test_rmat16_max_degree_source(rmat16, direction):
+    csr, g = rmat16
+    src = int(np.argmax(csr.degree()))
+    check_run(csr, g, src, direction=direction)
+
+
+def test_rmat16_reference_sentinel(rmat16):
+    """Reference convention: unreached = 63 (app/bfs.cu:18), bit-exact with bfs::check's rule."""
+    csr, g = rmat16
+    src = int(np.argmax(csr.degree()))
+    check_run(csr, g, src, unreached=S.REF_UNREACHED)
+
+
+def test_rmat_multipage_random_sources():
+    csr = S.Csr.rmat(14, 16, seed=G.SEED + 1)
+    g = S.PagedGraph.from_csr(csr, pagesize_words=1 << 13)
+    assert g.npages > 10
+    for i, src in enumerate(G.sources(csr, 6, 1)):
+        check_run(csr, g, src, direction=DIRS[i % 3])
+
+
+@pytest.mark.parametrize("block", [128, 256, 512])
+def test_block_sizes(block):
+    csr = S.Csr.rmat(13, 8, seed=G.SEED + 2)
+    g = S.PagedGraph.from_csr(csr, pagesize_words=1 << 12)
+    for src in G.sources(csr, 2, 2):
+        check_run(csr, g, src, block_size=block)
+
+
+def test_deep_path_and_cap():
+    """A 300-vertex path: native depths go to 299; with the reference sentinel
+    63 the reference semantics cap reachability at depth 62."""
+    csr = G.path(300)
+    g = S.PagedGraph.from_csr(csr, pagesize_words=256)
+    check_run(csr, g, 0, direction=S.DIR_PUSH)
+    check_run(csr, g, 150, direction=S.DIR_PULL)
+    d, _, _ = check_run(csr, g, 0, unreached=S.REF_UNREACHED)
+    assert d.max() == 63 and (d == 62).sum() == 1
+
+
+def test_isolated_source_and_ragged_V():
+    csr = G.random_graph(1001, 900, seed=3)  # V not a multiple of 32, isolated vertices
+    g = S.PagedGraph.from_csr(csr, pagesize_words=512)
+    iso = [int(v) for v in np.flatnonzero(csr.degree() == 0)[:2]]
+    for src in iso + G.sources(csr, 3, 3) + [1000]:
+        check_run(csr, g, src)
+
+
+def test_giant_vertex_chunks():
+    """A hub of degree > 4096 goes through the giant-chunk kernel."""
+    csr = G.star(20000, center=77)
+    g = S.PagedGraph.from_csr(csr, pagesize_words=1 << 16)
+    check_run(csr, g, 77, direction=S.DIR_PUSH)
+    check_run(csr, g, 5, direction=S.DIR_PUSH)
+    check_run(csr, g, 5)
+
+
+@pytest.mark.parametrize("direction", DIRS)
+def test_directed_powerlaw_with_transpose(direction):
+    csr = S.Csr.powerlaw(20000, 300000, 1.9, 2000, seed=G.SEED + 3)
+    t = csr.transpose()
+    g = S.PagedGraph.from_csr(csr, pagesize_words=1 << 14)
+    gt = S.PagedGraph.from_csr(t, pagesize_words=1 << 14)
+    for src in G.sources(csr, 3, 4):
+        check_run(csr, g, src, gt=gt, direction=direction)
+
+
+def test_web_graph():
+    csr = S.Csr.web(50000, 600000, 2.1, 5000, 4096, 0.9, seed=G.SEED + 5)
+    t = csr.transpose()
+    g = S.PagedGraph.from_csr(csr, pagesize_words=1 << 15)
+    gt = S.PagedGraph.from_csr(t, pagesize_words=1 << 15)
+    for src in G.sources(csr, 3, 5):
+        check_run(csr, g, src, gt=gt)
+
+
+def test_trace_and_page_histogram():
+    """Per-level trace adds up, and the fused per-page frontier histogram equals
+    get_page_info's (src/gpu_engine.cuh:397-441) restated in the oracle."""
+    csr = S.Csr.rmat(14, 16, seed=G.SEED + 6)
+    g = S.PagedGraph.from_csr(csr, pagesize_words=1 << 14)
+    src = G.sources(csr, 1, 6)[0]
+    eng = S.Engine(g)
+    depth, _, st = eng.bfs(src)
+    tr = eng.trace()
+    assert len(tr) == st.levels
+    assert 1 + sum(t["next"] for t in tr) == st.reached
+    deg = csr.degree()
+    for lvl in range(1, st.levels + 1):
+        stat = (depth == lvl).astype(np.uint8)
+        nodes, datas, _, _ = O.page_stats(g.page_list(), stat, deg)
+        hn, hd = eng.page_hist(lvl)
+        assert np.array_equal(hn, nodes) and np.array_equal(hd, datas), f"level {lvl}"
+        if lvl < st.levels:
+            assert tr[lvl]["frontier"] == stat.sum()
+    eng.close()
+
+
+def test_pages_from_files(tmp_path):
+    """Engine over pages read back from disk (the pagegencsr file set)."""
+    csr = S.Csr.rmat(13, 16, seed=G.SEED + 7)
+    prefix = str(tmp_path / "g")
+    csr.write(prefix)
+    csr.write_pages(prefix, 1 << 13)
+    g = S.PagedGraph.open(prefix)
+    for src in G.sources(csr, 2, 7):
+        check_run(csr, g, src)
+
+
+def test_bad_source_is_an_error(rmat16):
+    csr, g = rmat16
+    eng = S.Engine(g)
+    with pytest.raises(S.ScaphError) as ei:
+        eng.bfs(csr.V)
+    assert ei.value.code == S.EINVAL
+    eng.close()
