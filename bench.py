@@ -1,0 +1,355 @@
+#!/usr/bin/env python3
+"""BFS benchmark of the sm_100a Scaph engine.
+
+Workload (default): RMAT scale 24, edge factor 16, a/b/c/d = .57/.19/.19/.05,
+seeded, symmetrised, deduplicated, uint32 ids, paged CSR with 10 Mi-word
+pages, fully resident in HBM; 64 seeded random sources with nonzero degree,
+each run separately; Beamer alpha/beta direction switch (alpha 14, beta 24).
+One step = one single-source BFS.  GTEPS follows the reference's formula,
+edge_count / traversal time (src/app.cuh:252).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+Multi-GPU runs are replicas: each rank runs its own BFS sources on its own
+copy of the graph (no collective on the data path); value = all ranks'
+traversed edges / max-over-ranks time.
+
+--impl reference times the reference's own CPU BFS (bfs::check,
+app/bfs.cu:67-117, compiled from the reference sources into oracle/_ref) on
+the host cores, one process per core, on the same graph and sources.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "BFS GTEPS (edge_count / traversal time), plain direction-optimizing engine, RMAT-24 in HBM"
+PEAKS_FILE = os.path.join(ROOT, "MEASURED_PEAKS.json")
+FALLBACK_HBM_GBS = 6650.0
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=64)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--scale", type=int, default=24)
+    ap.add_argument("--sources", type=int, default=64)
+    ap.add_argument("--cpu-seconds", type=float, default=15.0, help="bounded CPU-baseline sample")
+    ap.add_argument("--no-cpu", action="store_true")
+    return ap.parse_args()
+
+
+def hbm_peak():
+    try:
+        with open(PEAKS_FILE) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.idx = gpu_index
+        self.proc = None
+        self.out = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.idx), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.out, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        self.proc.wait(timeout=10)
+        self.out.flush()
+        self.out.seek(0)
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.out.read().splitlines():
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        os.unlink(self.out.name)
+        load = [x for x in sm if smax and x > 0.3 * smax] or sm
+        return {"sm_mhz": statistics.median(load) if load else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def gpu_index(local_rank: int) -> int:
+    vis = os.environ.get("CUDA_VISIBLE_DEVICES")
+    if vis:
+        ids = [x.strip() for x in vis.split(",") if x.strip()]
+        if local_rank < len(ids) and ids[local_rank].isdigit():
+            return int(ids[local_rank])
+    return local_rank
+
+
+def config_dict(csr, scale, nsrc, extra=None):
+    d = {"workload": f"rmat{scale}-ef16 single-source BFS, {nsrc} seeded sources, alpha/beta 14/24, in HBM",
+         "graph": f"RMAT scale {scale}, ef 16, a/b/c/d .57/.19/.19/.05, symmetrised, dedup",
+         "V": csr.V, "E": csr.E, "sources": nsrc, "pagesize_words": 10 * 1024 * 1024,
+         "l2": "inputs larger than L2 (paged graph %.2f GB > 126 MB)" % (4 * (3 * csr.V + csr.E) / 1e9)}
+    if extra:
+        d.update(extra)
+    return d
+
+
+# ---------------------------------------------------------------------------
+# reference CPU arm
+# ---------------------------------------------------------------------------
+_W = {}
+
+
+def _ref_worker_init(idx_path, ngh_path):
+    import numpy as np
+
+    from oracle import oracle as O
+
+    _W["idx"] = np.load(idx_path, mmap_mode="r")
+    _W["ngh"] = np.load(ngh_path, mmap_mode="r")
+    _W["O"] = O
+    _W["vals"] = np.zeros(len(_W["idx"]) - 1, np.uint32)
+
+
+def _ref_worker_bfs(src):
+    O = _W["O"]
+    if O.ref_available():
+        _, sec = O.ref_bfs_check(_W["idx"], _W["ngh"], src, _W["vals"])
+        return sec
+    t = time.perf_counter()
+    O.bfs(_W["idx"].astype("uint64"), _W["ngh"], src, 63)
+    return time.perf_counter() - t
+
+
+def run_reference(args, world):
+    import multiprocessing as mp
+
+    import numpy as np
+
+    from oracle import oracle as O
+    from scaph_b200 import workloads
+
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    csr, srcs = workloads.config2(args.scale, args.sources)
+    kind = "reference" if O.ref_available() else "port"
+    tmp = tempfile.mkdtemp(dir="/dev/shm" if os.path.isdir("/dev/shm") else None)
+    idx_path, ngh_path = os.path.join(tmp, "idx.npy"), os.path.join(tmp, "ngh.npy")
+    np.save(idx_path, csr.idx.astype(np.uint32))
+    np.save(ngh_path, csr.ngh)
+    E = csr.E
+    cores = os.cpu_count() or 1
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(cores, initializer=_ref_worker_init, initargs=(idx_path, ngh_path)) as pool:
+        pool.map(_ref_worker_bfs, [srcs[i % len(srcs)] for i in range(max(args.warmup, cores))])
+        order = [srcs[i % len(srcs)] for i in range(args.steps)]
+        t0 = time.perf_counter()
+        secs = pool.map(_ref_worker_bfs, order, chunksize=1)
+        wall = time.perf_counter() - t0
+    for p in (idx_path, ngh_path):
+        os.unlink(p)
+    os.rmdir(tmp)
+    value = args.steps * E / wall / 1e9
+    sample = (f"{args.steps} single-source BFS of bfs::check over the flat CSR, {cores} processes "
+              f"(one source each), mean {statistics.mean(secs):.3f} s per source")
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "GTEPS", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * wall / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
+            "data": "synthetic (seeded RMAT)", "config": config_dict(csr, args.scale, len(srcs)),
+            "cpu_baseline": {"value": value, "unit": "GTEPS", "cores": cores, "kind": kind, "sample": sample},
+            "e2e": {"value": value, "unit": "GTEPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
+# CPU baseline beside our own arm (rank 0, N = 1)
+# ---------------------------------------------------------------------------
+def cpu_baseline(csr, srcs, budget_s):
+    import numpy as np
+
+    from oracle import oracle as O
+
+    kind = "reference" if O.ref_available() else "port"
+    idx32 = csr.idx.astype(np.uint32) if kind == "reference" else None
+    vals = np.zeros(csr.V, np.uint32)
+    n, tot = 0, 0.0
+    for s in srcs:
+        if kind == "reference":
+            _, sec = O.ref_bfs_check(idx32, csr.ngh, s, vals)
+        else:
+            t = time.perf_counter()
+            O.bfs(csr.idx, csr.ngh, s, 63)
+            sec = time.perf_counter() - t
+        n += 1
+        tot += sec
+        if tot >= budget_s:
+            break
+    return {"value": n * csr.E / tot / 1e9, "unit": "GTEPS", "cores": 1, "kind": kind,
+            "sample": f"{n} of the {len(srcs)} sources, single-threaded bfs::check "
+                      f"({'reference code' if kind == 'reference' else 'oracle restatement'}), "
+                      f"{tot:.1f} s total"}
+
+
+# ---------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------
+def run_ours(args, world):
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+
+    import scaph_b200 as S
+    from scaph_b200 import workloads
+
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local_rank)
+    if world > 1:
+        import datetime
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local_rank))
+
+    t0 = time.time()
+    csr, srcs = workloads.config2(args.scale, args.sources)
+    g = workloads.paged(csr)
+    gen_s = time.time() - t0
+    V, E = csr.V, csr.E
+    stream = torch.cuda.current_stream()
+    eng = S.Engine(g, device=local_rank, stream=stream.cuda_stream)
+    depth = torch.empty(V, dtype=torch.int32, device="cuda")
+
+    def src_of(i):
+        return srcs[(rank * 7 + i) % len(srcs)]
+
+    for i in range(args.warmup):
+        eng.bfs_device(src_of(i), depth.data_ptr())
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    clocks = ClockSampler(gpu_index(local_rank))
+    clocks.start()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    launches = 0
+    torch.cuda.synchronize()
+    ev0.record(stream)
+    for i in range(args.steps):
+        st = eng.bfs_device(src_of(i), depth.data_ptr())
+        launches += st.launches
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    ms = ev0.elapsed_time(ev1)
+    if world > 1:
+        t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+        dist.barrier()
+    value = world * args.steps * E / (ms / 1e3) / 1e9
+
+    # end to end through the public API: host output buffer (pinned), the
+    # source id in, depths copied back every step
+    L = S.lib()
+    ptr = L.scaph_host_alloc(V * 4)
+    host_depth = np.ctypeslib.as_array((S.C.c_uint32 * V).from_address(ptr))
+    n_e2e = args.steps
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    ev2, ev3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev2.record(stream)
+    for i in range(n_e2e):
+        eng.bfs(src_of(i), depth_out=host_depth)
+    ev3.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = ev2.elapsed_time(ev3)
+    if world > 1:
+        t = torch.tensor([e2e_ms], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    e2e_value = world * n_e2e * E / (e2e_ms / 1e3) / 1e9
+
+    # roofline of the dominant kernel from per-level device times over every
+    # source (separate, untimed pass)
+    per_dir = {0: [0, 0.0, 0], 1: [0, 0.0, 0]}  # alg bytes, ms, launches
+    g500 = []
+    for s in srcs:
+        _, _, st = eng.bfs(s)
+        g500.append(st.reached_edges / 2 / (st.ms / 1e3) / 1e9)
+        for t in eng.trace():
+            a = per_dir[t["direction"]]
+            a[0] += t["alg_bytes"]
+            a[1] += t["ms"]
+            a[2] += 1
+    dom = max(per_dir, key=lambda d: per_dir[d][1])
+    alg, dms, nl = per_dir[dom]
+    peak, peak_kind = hbm_peak()
+    achieved = (alg / nl) / (dms / nl / 1e3) / 1e9 if nl and dms > 0 else None
+    roof = {"bound": "hbm", "kernel": "k_pull" if dom == 1 else "k_push(+k_push_giant)",
+            "achieved": achieved, "peak": peak, "unit": "GB/s",
+            "frac": achieved / peak if achieved else None, "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)",
+            "traffic": None, "launches_sampled": nl, "alg_bytes_per_launch": alg / nl if nl else None,
+            "share_of_level_time": dms / (per_dir[0][1] + per_dir[1][1])}
+
+    line = {"metric": METRIC, "value": value, "unit": "GTEPS", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "u32", "data": "synthetic (seeded RMAT, generated on the host)",
+            "config": config_dict(csr, args.scale, len(srcs), {"parallelism": f"replicas x{world}",
+                                                                "graph_gen_s": round(gen_s, 1)}),
+            "e2e": {"value": e2e_value, "unit": "GTEPS", "h2d_bytes_per_step": 4, "d2h_bytes_per_step": V * 4},
+            "gpu_launches": launches, "roofline": roof, "clocks": clk,
+            "graph500_gteps_median": statistics.median(g500)}
+    if rank == 0 and world == 1 and not args.no_cpu:
+        line["cpu_baseline"] = cpu_baseline(csr, srcs, args.cpu_seconds)
+    L.scaph_host_free(ptr)
+    eng.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    if args.impl == "reference":
+        run_reference(args, world)
+    else:
+        run_ours(args, world)
+
+
+if __name__ == "__main__":
+    main()

@@ -192,6 +192,7 @@ typedef struct scaph_bfs_stats {
     uint64_t zc_bytes;          /* page bytes read zero-copy over PCIe      */
     uint64_t page_faults;       /* page loads on demand                     */
     uint64_t prefetched;        /* page loads issued ahead by the scheduler */
+    uint64_t launches;          /* kernels this library launched            */
     double   ms;                /* device time of the traversal (events)    */
 } scaph_bfs_stats;
 
@@ -215,8 +216,9 @@ typedef struct scaph_level_trace {
     uint64_t unvisited_edges;   /* their out-degree sum                     */
     uint64_t next;              /* vertices discovered by this level        */
     uint64_t edges_inspected;
+    uint64_t alg_bytes;         /* algorithmic HBM bytes of this level      */
     uint64_t h2d_bytes;
-    double   ms;
+    double   ms;                /* device time of this level's kernels      */
 } scaph_level_trace;
 int scaph_bfs_trace(const scaph_engine *e, scaph_level_trace *out, int cap);
 /* Active-vertex histogram of the frontier at `level` of the last run:

@@ -52,14 +52,14 @@ class _Stats(C.Structure):
                 ("_pad", C.c_int32), ("reached", C.c_uint64), ("reached_edges", C.c_uint64),
                 ("edges_inspected", C.c_uint64), ("alg_bytes", C.c_uint64), ("h2d_bytes", C.c_uint64),
                 ("zc_bytes", C.c_uint64), ("page_faults", C.c_uint64), ("prefetched", C.c_uint64),
-                ("ms", C.c_double)]
+                ("launches", C.c_uint64), ("ms", C.c_double)]
 
 
 class _Trace(C.Structure):
     _fields_ = [("level", C.c_int32), ("direction", C.c_int32), ("frontier", C.c_uint64),
                 ("frontier_edges", C.c_uint64), ("unvisited", C.c_uint64), ("unvisited_edges", C.c_uint64),
-                ("next", C.c_uint64), ("edges_inspected", C.c_uint64), ("h2d_bytes", C.c_uint64),
-                ("ms", C.c_double)]
+                ("next", C.c_uint64), ("edges_inspected", C.c_uint64), ("alg_bytes", C.c_uint64),
+                ("h2d_bytes", C.c_uint64), ("ms", C.c_double)]
 
 
 _lib = None
@@ -277,12 +277,13 @@ class BfsStats:
     zc_bytes: int
     page_faults: int
     prefetched: int
+    launches: int
     ms: float
 
 
 def _stats(s: _Stats) -> BfsStats:
     return BfsStats(s.levels, s.push_levels, s.pull_levels, s.reached, s.reached_edges, s.edges_inspected,
-                    s.alg_bytes, s.h2d_bytes, s.zc_bytes, s.page_faults, s.prefetched, s.ms)
+                    s.alg_bytes, s.h2d_bytes, s.zc_bytes, s.page_faults, s.prefetched, s.launches, s.ms)
 
 
 class Engine:

@@ -245,6 +245,7 @@ int scaph_engine::bfs(uint32_t src, uint32_t *depths, uint32_t *parents, int out
     uint64_t nf = 1, prev_nf = 0, mf = g->degree[src];
     uint64_t vis_n = 1, vis_e = mf;
     uint64_t insp_total = 0, alg_total = 0;
+    uint64_t launches = dp ? 3 : 2;  // fills + set_source
     int dir = 0, cur = 0, level = 0, npush = 0, npull = 0;
     uint32_t err = 0;
     while (nf > 0 && level < kMaxLevels && (uint64_t)level + 1 < unreached) {
@@ -288,12 +289,15 @@ int scaph_engine::bfs(uint32_t src, uint32_t *depths, uint32_t *parents, int out
         // pull: headers of unvisited vertices + in-edges up to the first
         // frontier hit; both: a V/8 bitmap pass and depth+parent writes)
         const uint64_t state_w = lc.next * (dp ? 8 : 4) + (uint64_t)nwords * 4;
+        const uint64_t alg = dir == 0 ? nf * 12 + mf * 4 + state_w : (V - vis_n) * 12 + lc.inspected * 4 + state_w;
+        trace.back().alg_bytes = alg;
+        alg_total += alg;
         if (dir == 0) {
-            alg_total += nf * 12 + mf * 4 + state_w;
             npush++;
+            launches += 2;
         } else {
-            alg_total += (V - vis_n) * 12 + lc.inspected * 4 + state_w;
             npull++;
+            launches += 1;
         }
         insp_total += lc.inspected;
         prev_nf = nf;
@@ -331,6 +335,7 @@ int scaph_engine::bfs(uint32_t src, uint32_t *depths, uint32_t *parents, int out
         stats->reached_edges = vis_e;
         stats->edges_inspected = insp_total;
         stats->alg_bytes = alg_total;
+        stats->launches = launches;
     }
     return SCAPH_OK;
 }

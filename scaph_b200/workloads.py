@@ -1,0 +1,44 @@
+"""Seeded synthetic workloads of the five benchmark configurations.
+
+Inputs are generated, never downloaded: RMAT graphs (Chakrabarti et al.),
+a directed power-law graph with preferential-attachment destinations, and a
+block-local web-crawl-like graph.  Seeds are 0x5CA90000 + configuration
+index, so every run of a configuration sees the same graph and sources.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+from . import Csr, PagedGraph
+
+SEED_BASE = 0x5CA90000
+PAGESIZE_WORDS = 10 * 1024 * 1024  # FLAGS_pagesize = 10 Mi words (src/app.cuh:38,149)
+RMAT_ABC = (0.57, 0.19, 0.19)
+
+
+def rmat(scale: int, edgefactor: float, config_index: int) -> Csr:
+    a, b, c = RMAT_ABC
+    return Csr.rmat(scale, edgefactor, a, b, c, seed=SEED_BASE + config_index, scramble=True)
+
+
+def random_sources(csr: Csr, n: int, seed: int) -> list[int]:
+    """n distinct seeded random sources with nonzero out-degree."""
+    cand = np.flatnonzero(csr.degree() > 0)
+    rng = np.random.default_rng(seed)
+    return [int(x) for x in rng.choice(cand, size=min(n, len(cand)), replace=False)]
+
+
+def config1():
+    """RMAT scale 16, ef 16; source = max-degree vertex."""
+    csr = rmat(16, 16, 0)
+    return csr, [int(np.argmax(csr.degree()))]
+
+
+def config2(scale: int = 24, nsrc: int = 64):
+    """RMAT scale 24, ef 16; 64 seeded random sources with nonzero degree."""
+    csr = rmat(scale, 16, 1)
+    return csr, random_sources(csr, nsrc, SEED_BASE + 1)
+
+
+def paged(csr: Csr, pagesize_words: int = PAGESIZE_WORDS) -> PagedGraph:
+    return PagedGraph.from_csr(csr, pagesize_words)
