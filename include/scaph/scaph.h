@@ -226,6 +226,33 @@ int scaph_bfs_trace(const scaph_engine *e, scaph_level_trace *out, int cap);
 int scaph_bfs_page_hist(const scaph_engine *e, int level, uint32_t *nodes,
                         uint32_t *datas, int npages);
 
+/* ---- BFS without device allocation -------------------------------------- */
+
+/* No counterpart in the reference.  For callers that must not have the
+ * library allocate device memory: hosts that pre-reserve the GPU's memory in
+ * their own pool, and latency-critical paths where cudaMalloc/cudaFree would
+ * synchronise the device.  Runs the same level kernels as scaph_bfs over ONE
+ * paged-CSR page that the caller already holds in device memory (the page
+ * must hold vertices 0..nodenum-1, i.e. the whole graph; the layout of
+ * <p>page0, tools/pagegencsr.cpp:221-242), writing depths (and parents, if
+ * d_parent is not NULL) into the caller's device arrays.
+ *   d_page   16-byte aligned, at least round_up(3*nodenum + edgenum, 4) words
+ *   limits   nodenum <= SCAPH_NOALLOC_MAX_V, edgenum <= SCAPH_NOALLOC_MAX_E,
+ *            larger inputs return SCAPH_EINVAL before any GPU work
+ * Its scratch state is a fixed ~1.2 MB __device__ array inside the library,
+ * held on every GPU that loads it until the process exits.  All calls share
+ * it and leave their contents in it; each call clears what it needs, but
+ * calls whose GPU work overlaps race on it.  The first call on a device
+ * looks up the array's address (cudaGetSymbolAddress, with that device
+ * current); make that first call before any stream capture.  The call
+ * synchronises `stream` (a cudaStream_t; NULL = default stream) once per
+ * level. */
+#define SCAPH_NOALLOC_MAX_V (1u << 18)
+#define SCAPH_NOALLOC_MAX_E (1u << 22)
+int scaph_bfs_page_noalloc(const uint32_t *d_page, uint32_t nodenum, uint32_t edgenum,
+                           uint32_t src, uint32_t unreached, uint32_t *d_depth,
+                           uint32_t *d_parent, void *stream);
+
 /* ---- host helpers ------------------------------------------------------ */
 
 /* Page-locked host memory for outputs copied back by scaph_bfs (faster
