@@ -231,7 +231,7 @@ def run_ours(args, world):
     import torch.distributed as dist
 
     import scaph_b200 as S
-    from scaph_b200 import workloads
+    from scaph_b200 import replicas, workloads
 
     rank = int(os.environ.get("RANK", "0"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
@@ -251,8 +251,10 @@ def run_ours(args, world):
     eng = S.Engine(g, device=local_rank, stream=stream.cuda_stream)
     depth = torch.empty(V, dtype=torch.int32, device="cuda")
 
+    order = replicas.rank_sources(srcs, rank, max(args.steps, args.warmup))
+
     def src_of(i):
-        return srcs[(rank * 7 + i) % len(srcs)]
+        return order[i % len(order)]
 
     for i in range(args.warmup):
         eng.bfs_device(src_of(i), depth.data_ptr())
@@ -271,13 +273,10 @@ def run_ours(args, world):
     ev1.record(stream)
     torch.cuda.synchronize()
     clk = clocks.stop()
-    ms = ev0.elapsed_time(ev1)
+    ms = replicas.max_over_ranks(ev0.elapsed_time(ev1), world, "cuda")
     if world > 1:
-        t = torch.tensor([ms], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
         dist.barrier()
-    value = world * args.steps * E / (ms / 1e3) / 1e9
+    value = replicas.aggregate_gteps(world, args.steps, E, ms)
 
     # end to end through the public API: host output buffer (pinned), the
     # source id in, depths copied back every step
@@ -294,12 +293,8 @@ def run_ours(args, world):
         eng.bfs(src_of(i), depth_out=host_depth)
     ev3.record(stream)
     torch.cuda.synchronize()
-    e2e_ms = ev2.elapsed_time(ev3)
-    if world > 1:
-        t = torch.tensor([e2e_ms], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
-    e2e_value = world * n_e2e * E / (e2e_ms / 1e3) / 1e9
+    e2e_ms = replicas.max_over_ranks(ev2.elapsed_time(ev3), world, "cuda")
+    e2e_value = replicas.aggregate_gteps(world, n_e2e, E, e2e_ms)
 
     # roofline of the dominant kernel from per-level device times over every
     # source (separate, untimed pass)
