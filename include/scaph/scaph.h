@@ -163,7 +163,9 @@ typedef struct scaph_config {
                                   threshold/32 of a page are read zero-copy
                                   instead of copied (FLAGS_threshold,
                                   src/app.cuh:45,151); 0 = 3                */
-    int32_t  use_graph;        /* 1 = run each BFS as one CUDA-graph launch */
+    int32_t  use_graph;        /* 0/1: each BFS is one CUDA-graph launch whose
+                                  level loop runs on the device; 2: host loop
+                                  (one launch per level, per-level events)  */
     int32_t  device;           /* CUDA device ordinal                       */
     void    *stream;           /* cudaStream_t to run on; NULL = own stream */
 } scaph_config;
@@ -204,6 +206,10 @@ typedef struct scaph_bfs_stats {
  * stats may be NULL. */
 int scaph_bfs(scaph_engine *e, uint32_t src, uint32_t *depths, uint32_t *parents,
               int out_on_device, scaph_bfs_stats *stats);
+/* With out_on_device != 0 and stats == NULL, scaph_bfs only enqueues the
+ * traversal on the engine's stream and returns; scaph_engine_sync waits,
+ * and scaph_bfs_trace / scaph_bfs_page_hist wait for the last run. */
+int scaph_engine_sync(scaph_engine *e);
 
 /* Per-level trace of the last scaph_bfs (direction, frontier, edges, time,
  * per-page histogram).  Writes up to `cap` records, returns the count. */
@@ -220,10 +226,10 @@ typedef struct scaph_level_trace {
     uint64_t h2d_bytes;
     double   ms;                /* device time of this level's kernels      */
 } scaph_level_trace;
-int scaph_bfs_trace(const scaph_engine *e, scaph_level_trace *out, int cap);
+int scaph_bfs_trace(scaph_engine *e, scaph_level_trace *out, int cap);
 /* Active-vertex histogram of the frontier at `level` of the last run:
  * nodes[p] / datas[p] as get_page_info computes them (src/gpu_engine.cuh:397-441). */
-int scaph_bfs_page_hist(const scaph_engine *e, int level, uint32_t *nodes,
+int scaph_bfs_page_hist(scaph_engine *e, int level, uint32_t *nodes,
                         uint32_t *datas, int npages);
 
 /* ---- BFS without device allocation -------------------------------------- */
@@ -239,7 +245,7 @@ int scaph_bfs_page_hist(const scaph_engine *e, int level, uint32_t *nodes,
  *   d_page   16-byte aligned, at least round_up(3*nodenum + edgenum, 4) words
  *   limits   nodenum <= SCAPH_NOALLOC_MAX_V, edgenum <= SCAPH_NOALLOC_MAX_E,
  *            larger inputs return SCAPH_EINVAL before any GPU work
- * Its scratch state is a fixed ~1.2 MB __device__ array inside the library,
+ * Its scratch state is a fixed ~1.3 MB __device__ array inside the library,
  * held on every GPU that loads it until the process exits.  All calls share
  * it and leave their contents in it; each call clears what it needs, but
  * calls whose GPU work overlaps race on it.  The first call on a device

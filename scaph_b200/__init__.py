@@ -14,7 +14,9 @@ from dataclasses import dataclass
 import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_HERE, "libscaph.so")
+# SCAPH_LIB may point at another build of the same library (e.g. a variant
+# compiled with different tile parameters).
+LIB_PATH = os.environ.get("SCAPH_LIB", os.path.join(_HERE, "libscaph.so"))
 
 # status codes (include/scaph/scaph.h)
 OK, EINVAL, EIO, ENOMEM, ECUDA, EFORMAT, ETIMEOUT, EUNSUPPORTED, EDEVICE = 0, -1, -2, -3, -4, -5, -6, -7, -8
@@ -97,6 +99,7 @@ def lib() -> C.CDLL:
         "scaph_engine_destroy": ([vp], i32),
         "scaph_bfs": ([vp, u32, vp, vp, i32, P(_Stats)], i32),
         "scaph_bfs_trace": ([vp, P(_Trace), i32], i32),
+        "scaph_engine_sync": ([vp], i32),
         "scaph_bfs_page_hist": ([vp, i32, vp, vp, i32], i32),
         "scaph_host_alloc": ([C.c_size_t], vp),
         "scaph_host_free": ([vp], None),
@@ -329,6 +332,14 @@ class Engine:
         _check(lib().scaph_bfs(self._h, src, C.c_void_p(depth_ptr), C.c_void_p(parent_ptr) if parent_ptr else None,
                                1, C.byref(st)))
         return _stats(st)
+
+    def bfs_async(self, src: int, depth_ptr: int, parent_ptr: int | None = None) -> None:
+        """Enqueues one BFS writing into device buffers; returns at once."""
+        _check(lib().scaph_bfs(self._h, src, C.c_void_p(depth_ptr), C.c_void_p(parent_ptr) if parent_ptr else None,
+                               1, None))
+
+    def sync(self) -> None:
+        _check(lib().scaph_engine_sync(self._h))
 
     def trace(self) -> list[dict]:
         buf = (_Trace * 4096)()

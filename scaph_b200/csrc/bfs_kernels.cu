@@ -12,13 +12,20 @@
 //   second kernel spreads over the whole GPU.
 // pull (bottom-up): has no reference counterpart (gpu_pull_iteration is a
 //   stub, src/app.cuh:365-369).  A warp owns one word (32 vertices) of the
-//   visited bitmap, so visited/next words are written without atomics; each
-//   unvisited vertex scans its in-edges against the frontier bitmap and
-//   stops at the first hit (thread-per-vertex for the first few edges, then
-//   warp-cooperative with ballot).
-// Both fold the per-page frontier statistics of get_page_info
-// (src/gpu_engine.cuh:397-441) into their epilogue: a shared-memory
-// histogram of the next frontier by page, flushed once per CTA.
+//   visited bitmap, so visited/next words are written without atomics.  Each
+//   unvisited vertex issues its first four in-edge loads and frontier probes
+//   at once; longer lists are then scanned by the whole warp, 128 edges per
+//   step with 128-bit loads, stopping at the first frontier hit.  Warps take
+//   words from a per-CTA shared counter, so heavy words do not stall a CTA.
+// Both stage the page table and coarse index in shared memory, and fold the
+// per-page frontier statistics of get_page_info (src/gpu_engine.cuh:397-441)
+// into their epilogue: a shared-memory histogram of the next frontier by
+// page, flushed once per CTA.
+//
+// Two entry points per level kernel: one takes the level's state as kernel
+// arguments (host-driven loop, out-of-core page batches), the other reads it
+// from a device control block (graph mode: a whole BFS is one CUDA-graph
+// launch whose level loop is a conditional WHILE node, see engine.cu).
 #include <cuda_runtime.h>
 
 #include "device.cuh"
@@ -27,6 +34,13 @@
 namespace scaph {
 
 namespace {
+
+#ifndef SCAPH_PULL_SERIAL
+#define SCAPH_PULL_SERIAL 4
+#endif
+constexpr int kPushTileWords = 128;                  // frontier-bitmap words per push tile
+constexpr int kPullTileWords = 128;                  // visited-bitmap words per pull tile
+constexpr uint32_t kPullSerial = SCAPH_PULL_SERIAL;  // in-edges each lane probes before the warp helps
 
 template <int BLOCK>
 __device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t x, uint32_t *wsum, uint32_t &total)
@@ -69,20 +83,22 @@ struct CtaAcc {
     unsigned long long next, next_edges, inspected, headers;
 };
 
+// per-thread counts stay below 2^32: a level touches each vertex once and
+// each of the < 2^32 edges of a paged graph at most once
+struct ThreadAcc {
+    uint32_t next = 0, next_edges = 0, inspected = 0, headers = 0;
+};
+
 template <int BLOCK>
-__device__ __forceinline__ void flush_acc(CtaAcc *acc, unsigned long long next, unsigned long long next_edges,
-                                          unsigned long long inspected, unsigned long long headers,
-                                          LevelCounters *ctr)
+__device__ __forceinline__ void flush_acc(CtaAcc *acc, ThreadAcc t, LevelCounters *ctr)
 {
-    next = warp_sum64(next);
-    next_edges = warp_sum64(next_edges);
-    inspected = warp_sum64(inspected);
-    headers = warp_sum64(headers);
+    const unsigned long long n = warp_sum64(t.next), ne = warp_sum64(t.next_edges);
+    const unsigned long long in = warp_sum64(t.inspected), h = warp_sum64(t.headers);
     if ((threadIdx.x & 31) == 0) {
-        atomicAdd(&acc->next, next);
-        atomicAdd(&acc->next_edges, next_edges);
-        atomicAdd(&acc->inspected, inspected);
-        atomicAdd(&acc->headers, headers);
+        atomicAdd(&acc->next, n);
+        atomicAdd(&acc->next_edges, ne);
+        atomicAdd(&acc->inspected, in);
+        atomicAdd(&acc->headers, h);
     }
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -93,39 +109,66 @@ __device__ __forceinline__ void flush_acc(CtaAcc *acc, unsigned long long next, 
     }
 }
 
-// Adds vertex u (out-degree + 3 words, the reference's `datas` unit) to the
-// next-frontier histogram over the pages of the out-edge graph s.hg.
-__device__ __forceinline__ void hist_add(uint32_t *hn, uint32_t *hd, const BfsDev &s, uint32_t u, uint32_t datas)
+// Shared-memory working set common to the level kernels.
+struct LevelSmem {
+    uint32_t hn[kHistCap], hd[kHistCap];
+    PageDev lut_pages[kLutPages];
+    uint32_t lut_coarse[kLutCoarse];
+    CtaAcc acc;
+};
+
+// Stages g's page table + coarse index in shared memory when they fit.
+template <int BLOCK>
+__device__ __forceinline__ PageLut stage_lut(const GraphDev &g, LevelSmem &sm)
 {
-    if (!s.page_nodes) return;
-    const int p = page_of(s.hg, u);
-    if (p < kHistCap) {
-        atomicAdd(&hn[p], 1u);
-        atomicAdd(&hd[p], datas);
-    } else {
-        atomicAdd(&s.page_nodes[p], 1u);
-        atomicAdd(&s.page_datas[p], datas);
+    const uint32_t ncoarse = (g.V >> g.cshift) + 1;
+    if (g.npages + 1 <= (uint32_t)kLutPages && ncoarse <= (uint32_t)kLutCoarse) {
+        for (uint32_t i = threadIdx.x; i <= g.npages; i += BLOCK) sm.lut_pages[i] = g.pages[i];
+        for (uint32_t i = threadIdx.x; i < ncoarse; i += BLOCK) sm.lut_coarse[i] = g.coarse[i];
+        return PageLut{sm.lut_pages, sm.lut_coarse, g.cshift};
+    }
+    return PageLut{g.pages, g.coarse, g.cshift};
+}
+
+template <int BLOCK>
+__device__ __forceinline__ void level_prologue(LevelSmem &sm, const BfsDev &s)
+{
+    if (threadIdx.x == 0) sm.acc = CtaAcc{0, 0, 0, 0};
+    if (s.page_nodes) {
+        const int n = s.hg.npages < (uint32_t)kHistCap ? (int)s.hg.npages : kHistCap;
+        for (int i = threadIdx.x; i < n; i += BLOCK) {
+            sm.hn[i] = 0;
+            sm.hd[i] = 0;
+        }
     }
 }
 
 template <int BLOCK>
-__device__ __forceinline__ void hist_init(uint32_t *hn, uint32_t *hd, const BfsDev &s)
+__device__ __forceinline__ void level_epilogue(LevelSmem &sm, const BfsDev &s, const ThreadAcc &t)
 {
-    if (!s.page_nodes) return;
-    const int n = s.hg.npages < (uint32_t)kHistCap ? (int)s.hg.npages : kHistCap;
-    for (int i = threadIdx.x; i < n; i += BLOCK) { hn[i] = 0; hd[i] = 0; }
+    __syncthreads();
+    flush_acc<BLOCK>(&sm.acc, t, s.ctr);
+    if (s.page_nodes) {
+        const int n = s.hg.npages < (uint32_t)kHistCap ? (int)s.hg.npages : kHistCap;
+        for (int i = threadIdx.x; i < n; i += BLOCK) {
+            if (sm.hn[i]) {
+                atomicAdd(&s.page_nodes[i], sm.hn[i]);
+                atomicAdd(&s.page_datas[i], sm.hd[i]);
+            }
+        }
+    }
 }
 
-template <int BLOCK>
-__device__ __forceinline__ void hist_flush(const uint32_t *hn, const uint32_t *hd, const BfsDev &s)
+// Adds a discovered vertex (page p of the histogram graph; out-degree + 3
+// words, the reference's `datas` unit) to the next-frontier histogram.
+__device__ __forceinline__ void hist_add(LevelSmem &sm, const BfsDev &s, int p, uint32_t datas)
 {
-    if (!s.page_nodes) return;
-    const int n = s.hg.npages < (uint32_t)kHistCap ? (int)s.hg.npages : kHistCap;
-    for (int i = threadIdx.x; i < n; i += BLOCK) {
-        if (hn[i]) {
-            atomicAdd(&s.page_nodes[i], hn[i]);
-            atomicAdd(&s.page_datas[i], hd[i]);
-        }
+    if (p < kHistCap) {
+        atomicAdd(&sm.hn[p], 1u);
+        atomicAdd(&sm.hd[p], datas);
+    } else {
+        atomicAdd(&s.page_nodes[p], 1u);
+        atomicAdd(&s.page_datas[p], datas);
     }
 }
 
@@ -143,36 +186,47 @@ __device__ __forceinline__ bool claim(const BfsDev &s, uint32_t u, uint32_t src)
     return true;
 }
 
-}  // namespace
+__device__ __forceinline__ void visit(LevelSmem &sm, const BfsDev &s, ThreadAcc &t, uint32_t u, uint32_t src,
+                                      bool hist_same, const PageLut &lut)
+{
+    if (u >= s.V) {
+        atomicOr(&s.ctr->error, 1u);
+        return;
+    }
+    if (!claim(s, u, src)) return;
+    t.next++;
+    const uint32_t du = __ldg(&s.degree[u]);
+    t.next_edges += du;
+    if (s.page_nodes) hist_add(sm, s, hist_same ? lut.of(u) : page_of(s.hg, u), du + 3);
+}
 
 // ---------------------------------------------------------------------------
-// push level
+// bodies
 // ---------------------------------------------------------------------------
 template <int BLOCK>
-__global__ void __launch_bounds__(BLOCK) k_push(GraphDev g, BfsDev s, uint32_t vlo, uint32_t vhi)
+__device__ __forceinline__ void push_body(const GraphDev &g, const BfsDev &s, uint32_t vlo, uint32_t vhi)
 {
-    constexpr int TW = BLOCK < 256 ? BLOCK : 256;  // bitmap words per tile
-    __shared__ uint32_t q[TW * 32];
+    __shared__ LevelSmem sm;
+    __shared__ uint32_t q[kPushTileWords * 32];
     __shared__ unsigned long long ebase[BLOCK];
     __shared__ uint32_t elen[BLOCK];
     __shared__ uint32_t qoff[BLOCK];
     __shared__ uint32_t wsum[BLOCK / 32];
-    __shared__ uint32_t hn[kHistCap], hd[kHistCap];
-    __shared__ CtaAcc acc;
 
-    if (threadIdx.x == 0) acc = CtaAcc{0, 0, 0, 0};
-    hist_init<BLOCK>(hn, hd, s);
+    level_prologue<BLOCK>(sm, s);
+    const PageLut lut = stage_lut<BLOCK>(g, sm);
+    const bool hist_same = s.hg.pages == g.pages;
     __syncthreads();
 
-    unsigned long long my_next = 0, my_edges = 0, my_insp = 0, my_hdr = 0;
-    const uint32_t ew = s.weighted_edges ? 2u : 1u;
+    ThreadAcc t;
     const uint32_t wlo = vlo >> 5, whi = (uint32_t)(((unsigned long long)vhi + 31) >> 5);
-    const uint32_t ntiles = (whi - wlo + TW - 1) / TW;
+    const uint32_t ntiles = (whi - wlo + kPushTileWords - 1) / kPushTileWords;
 
     for (uint32_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-        const uint32_t w = wlo + tile * TW + threadIdx.x;
+        const uint32_t w = wlo + tile * kPushTileWords + threadIdx.x;
         uint32_t f = 0;
-        if (threadIdx.x < TW && w < whi) f = s.front[w] & range_mask(w, vlo, vhi);
+        if (threadIdx.x < kPushTileWords && w < whi) f = s.front[w] & range_mask(w, vlo, vhi);
+        if (!__syncthreads_or(f != 0)) continue;
         uint32_t total;
         uint32_t off = block_exclusive_scan<BLOCK>(__popc(f), wsum, total);
         if (total == 0) continue;
@@ -186,18 +240,18 @@ __global__ void __launch_bounds__(BLOCK) k_push(GraphDev g, BfsDev s, uint32_t v
             uint32_t nq = 0;
             if (k < total) {
                 const uint32_t v = q[k];
-                const int p = page_of(g, v);
-                const PageDev pd = g.pages[p];
+                const int p = lut.of(v);
+                const PageDev pd = lut.pages[p];
                 uint32_t len = 0;
                 unsigned long long st = 0;
                 if (pd.base != kNotResident) {
                     const uint32_t *node = g.pool + pd.base + 3ull * (v - pd.left);
                     const uint32_t pos = node[1];
                     len = node[2];
-                    st = pd.base + 3ull * pd.nodenum + (unsigned long long)pos * ew;
-                    my_hdr++;
-                    my_insp += len;
-                    if (len > kGiantEdges && ew == 1) {
+                    st = pd.base + 3ull * pd.nodenum + pos;
+                    t.headers++;
+                    t.inspected += len;
+                    if (len > kGiantEdges) {
                         const uint32_t nch = (len + kGiantEdges - 1) / kGiantEdges;
                         const uint32_t at = atomicAdd(&s.ctr->giant, nch);
                         if (at + nch <= s.giant_cap) {
@@ -210,15 +264,15 @@ __global__ void __launch_bounds__(BLOCK) k_push(GraphDev g, BfsDev s, uint32_t v
                             }
                             len = 0;
                         } else {
-                            atomicOr(&s.ctr->error, 2u);  // giant queue overflow: expand here
+                            atomicOr(&s.ctr->error, 2u);  // cannot happen: the queue holds 2E/4096+1024
                         }
                     }
                 } else {
                     atomicOr(&s.ctr->error, 4u);  // frontier vertex on a non-resident page
                 }
                 ebase[threadIdx.x] = st;
-                elen[threadIdx.x] = len * ew;
-                nq = len ? (uint32_t)(((st + (unsigned long long)len * ew + 3) >> 2) - (st >> 2)) : 0u;
+                elen[threadIdx.x] = len;
+                nq = len ? (uint32_t)(((st + len + 3) >> 2) - (st >> 2)) : 0u;
             }
             uint32_t tq;
             const uint32_t qo = block_exclusive_scan<BLOCK>(nq, wsum, tq);
@@ -239,38 +293,25 @@ __global__ void __launch_bounds__(BLOCK) k_push(GraphDev g, BfsDev s, uint32_t v
 #pragma unroll
                 for (int j = 0; j < 4; j++) {
                     const unsigned long long word = quad * 4 + j;
-                    if (word >= st && word < en && ((word - st) % ew) == 0) {
-                        const uint32_t u = vals[j];
-                        if (u < s.V && claim(s, u, src)) {
-                            my_next++;
-                            const uint32_t du = __ldg(&s.degree[u]);
-                            my_edges += du;
-                            hist_add(hn, hd, s, u, du + 3);
-                        } else if (u >= s.V) {
-                            atomicOr(&s.ctr->error, 1u);
-                        }
-                    }
+                    if (word >= st && word < en) visit(sm, s, t, vals[j], src, hist_same, lut);
                 }
             }
             __syncthreads();
         }
     }
-    __syncthreads();
-    flush_acc<BLOCK>(&acc, my_next, my_edges, my_insp, my_hdr, s.ctr);
-    hist_flush<BLOCK>(hn, hd, s);
+    level_epilogue<BLOCK>(sm, s, t);
 }
 
-// Giant adjacency chunks queued by k_push: one CTA per chunk, grid-stride.
 template <int BLOCK>
-__global__ void __launch_bounds__(BLOCK) k_push_giant(GraphDev g, BfsDev s)
+__device__ __forceinline__ void giant_body(const GraphDev &g, const BfsDev &s)
 {
-    __shared__ uint32_t hn[kHistCap], hd[kHistCap];
-    __shared__ CtaAcc acc;
-    if (threadIdx.x == 0) acc = CtaAcc{0, 0, 0, 0};
-    hist_init<BLOCK>(hn, hd, s);
-    __syncthreads();
-    unsigned long long my_next = 0, my_edges = 0;
+    __shared__ LevelSmem sm;
     const uint32_t n = min(*((volatile uint32_t *)&s.ctr->giant), s.giant_cap);
+    if (blockIdx.x >= n) return;  // whole CTA: no chunk for it
+    level_prologue<BLOCK>(sm, s);
+    const PageLut lut = stage_lut<BLOCK>(s.hg, sm);
+    __syncthreads();
+    ThreadAcc t;
     for (uint32_t c = blockIdx.x; c < n; c += gridDim.x) {
         const GiantChunk gc = s.giant[c];
         if (gc.len > kGiantEdges || gc.start + gc.len > g.pool_words || gc.src >= s.V) {
@@ -285,128 +326,364 @@ __global__ void __launch_bounds__(BLOCK) k_push_giant(GraphDev g, BfsDev s)
 #pragma unroll
             for (int j = 0; j < 4; j++) {
                 const unsigned long long word = qd * 4 + j;
-                if (word >= st && word < en) {
-                    const uint32_t u = vals[j];
-                    if (u < s.V && claim(s, u, gc.src)) {
-                        my_next++;
-                        const uint32_t du = __ldg(&s.degree[u]);
-                        my_edges += du;
-                        hist_add(hn, hd, s, u, du + 3);
-                    } else if (u >= s.V) {
-                        atomicOr(&s.ctr->error, 1u);
-                    }
-                }
+                if (word >= st && word < en) visit(sm, s, t, vals[j], gc.src, true, lut);
             }
         }
     }
-    __syncthreads();
-    flush_acc<BLOCK>(&acc, my_next, my_edges, 0, 0, s.ctr);
-    hist_flush<BLOCK>(hn, hd, s);
+    level_epilogue<BLOCK>(sm, s, t);
 }
-
-// ---------------------------------------------------------------------------
-// pull level (g = in-edge graph)
-// ---------------------------------------------------------------------------
-constexpr uint32_t kPullSerial = 4;  // edges each lane tries alone before the warp helps
 
 template <int BLOCK>
-__global__ void __launch_bounds__(BLOCK) k_pull(GraphDev g, BfsDev s, uint32_t vlo, uint32_t vhi)
+__device__ __forceinline__ void pull_body(const GraphDev &g, const BfsDev &s, uint32_t vlo, uint32_t vhi)
 {
-    __shared__ uint32_t hn[kHistCap], hd[kHistCap];
-    __shared__ CtaAcc acc;
-    if (threadIdx.x == 0) acc = CtaAcc{0, 0, 0, 0};
-    hist_init<BLOCK>(hn, hd, s);
+    // A CTA takes a tile of kPullTileWords visited-bitmap words, compacts the
+    // tile's unvisited vertices into q, and runs them one per thread (phase
+    // A: header, the first kPullSerial in-edges and their frontier probes, all
+    // issued back to back).  Vertices still unresolved go to bq and are
+    // scanned by groups of kGroup lanes, 4*kGroup in-edges per step with
+    // 128-bit loads, up to the first frontier hit (phase B).  Found vertices
+    // are collected in a shared bitmap and the tile's visited/next words are
+    // then written once, without global atomics.
+    constexpr int kGroup = 8;
+    constexpr int kGroups = BLOCK / kGroup;
+    __shared__ LevelSmem sm;
+    __shared__ uint32_t q[kPullTileWords * 32];
+    __shared__ uint32_t fnd[kPullTileWords];
+    __shared__ uint32_t bq_v[BLOCK], bq_len[BLOCK];
+    __shared__ unsigned long long bq_st[BLOCK];
+    __shared__ int bq_p[BLOCK];
+    __shared__ uint32_t wsum[BLOCK / 32];
+
+    level_prologue<BLOCK>(sm, s);
+    const PageLut lut = stage_lut<BLOCK>(g, sm);
+    const bool hist_same = s.hg.pages == g.pages;
+    const int lane = threadIdx.x & 31;
+    const int grp = threadIdx.x / kGroup, glane = threadIdx.x % kGroup;
+    const int gshift = (lane / kGroup) * kGroup;  // bit offset of this group in a warp ballot
     __syncthreads();
 
-    unsigned long long my_next = 0, my_edges = 0, my_insp = 0, my_hdr = 0;
-    const int lane = threadIdx.x & 31;
-    const uint32_t ew = s.weighted_edges ? 2u : 1u;
+    ThreadAcc t;
     const uint32_t wlo = vlo >> 5, whi = (uint32_t)(((unsigned long long)vhi + 31) >> 5);
-    const uint32_t wstride = (gridDim.x * BLOCK) >> 5;
+    const uint32_t ntiles = (whi - wlo + kPullTileWords - 1) / kPullTileWords;
 
-    for (uint32_t w = wlo + ((blockIdx.x * BLOCK + threadIdx.x) >> 5); w < whi; w += wstride) {
-        const uint32_t vis = s.visited[w];
-        const uint32_t unv = ~vis & range_mask(w, vlo, vhi);
-        if (!unv) continue;
-        const uint32_t v = (w << 5) + lane;
-        const bool mine = (unv >> lane) & 1u;
-        uint32_t len = 0, found = 0, par = kNoParent, k = 0;
-        unsigned long long st = 0;
-        if (mine) {
-            const int p = page_of(g, v);
-            const PageDev pd = g.pages[p];
-            if (pd.base != kNotResident) {
-                const uint32_t *node = g.pool + pd.base + 3ull * (v - pd.left);
-                const uint32_t pos = node[1];
-                len = node[2];
-                st = pd.base + 3ull * pd.nodenum + (unsigned long long)pos * ew;
-                my_hdr++;
-                const uint32_t lim = min(len, kPullSerial);
-                for (; k < lim; k++) {
-                    const uint32_t u = __ldg(&g.pool[st + (unsigned long long)k * ew]);
-                    if (u < s.V && test_bit(s.front, u)) {
-                        found = 1;
-                        par = u;
-                        k++;
-                        break;
+    for (uint32_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        const uint32_t w = wlo + tile * kPullTileWords + threadIdx.x;
+        uint32_t unv = 0;
+        if (threadIdx.x < kPullTileWords) {
+            fnd[threadIdx.x] = 0;
+            if (w < whi) unv = ~s.visited[w] & range_mask(w, vlo, vhi);
+        }
+        if (!__syncthreads_or(unv != 0)) continue;
+        uint32_t total;
+        uint32_t off = block_exclusive_scan<BLOCK>(__popc(unv), wsum, total);
+        if (total == 0) continue;
+        {
+            uint32_t m = unv;
+            while (m) {
+                q[off++] = (w << 5) + (__ffs(m) - 1);
+                m &= m - 1;
+            }
+        }
+        __syncthreads();
+        for (uint32_t c0 = 0; c0 < total; c0 += BLOCK) {
+            // ---- phase A: one unvisited vertex per thread
+            const uint32_t k = c0 + threadIdx.x;
+            uint32_t v = 0, len = 0, need = 0;
+            unsigned long long st = 0;
+            int p = 0;
+            if (k < total) {
+                v = q[k];
+                p = lut.of(v);
+                const PageDev pd = lut.pages[p];
+                if (pd.base != kNotResident) {
+                    const uint32_t *node = g.pool + pd.base + 3ull * (v - pd.left);
+                    const uint32_t pos = node[1];
+                    len = node[2];
+                    st = pd.base + 3ull * pd.nodenum + pos;
+                    t.headers++;
+                    uint32_t u[kPullSerial];
+#pragma unroll
+                    for (uint32_t j = 0; j < kPullSerial; j++) u[j] = j < len ? __ldg(&g.pool[st + j]) : 0xFFFFFFFFu;
+                    uint32_t hit = 0;
+#pragma unroll
+                    for (uint32_t j = 0; j < kPullSerial; j++)
+                        if (u[j] < s.V && test_bit(s.front, u[j])) hit |= 1u << j;
+                    if (hit) {
+                        const uint32_t j = __ffs(hit) - 1;
+                        t.inspected += j + 1;
+                        const uint32_t par = u[j];
+                        s.depth[v] = s.level + 1;
+                        if (s.parent) s.parent[v] = par;
+                        atomicOr(&fnd[(v >> 5) - (wlo + tile * kPullTileWords)], 1u << (v & 31));
+                        const uint32_t dv = __ldg(&s.degree[v]);
+                        t.next++;
+                        t.next_edges += dv;
+                        if (s.page_nodes) hist_add(sm, s, hist_same ? p : page_of(s.hg, v), dv + 3);
+                    } else {
+                        t.inspected += min(len, kPullSerial);
+                        need = len > kPullSerial;
+                    }
+                } else {
+                    atomicOr(&s.ctr->error, 4u);
+                }
+            }
+            uint32_t nb;
+            const uint32_t bo = block_exclusive_scan<BLOCK>(need, wsum, nb);
+            if (need) {
+                bq_v[bo] = v;
+                bq_st[bo] = st;
+                bq_len[bo] = len;
+                bq_p[bo] = p;
+            }
+            __syncthreads();
+            // ---- phase B: groups of kGroup lanes, one vertex per group
+            for (uint32_t e0 = 0; e0 < nb; e0 += kGroups) {
+                const uint32_t e = e0 + grp;
+                const bool mine = e < nb;
+                unsigned long long a = 0, b = 0;
+                if (mine) {
+                    a = bq_st[e] + kPullSerial;
+                    b = bq_st[e] + bq_len[e];
+                }
+                const unsigned long long qa = a >> 2, qb = (b + 3) >> 2;
+                unsigned long long qd = qa + glane;
+                bool active = mine;
+                uint32_t hit_par = kNoParent;
+                unsigned long long hit_word = b;
+                while (__any_sync(0xFFFFFFFFu, active)) {
+                    uint32_t myhit = 0, vals[4] = {0, 0, 0, 0};
+                    if (active && qd < qb) {
+                        const uint4 val = ld_nc_v4(g.pool + qd * 4);
+                        vals[0] = val.x;
+                        vals[1] = val.y;
+                        vals[2] = val.z;
+                        vals[3] = val.w;
+#pragma unroll
+                        for (int j = 0; j < 4; j++) {
+                            const unsigned long long word = qd * 4 + j;
+                            if (word >= a && word < b && vals[j] < s.V && test_bit(s.front, vals[j])) myhit |= 1u << j;
+                        }
+                    }
+                    // every lane runs the same ballot/shuffles (warp stays converged)
+                    const uint32_t bal = __ballot_sync(0xFFFFFFFFu, myhit != 0);
+                    const uint32_t gb = (bal >> gshift) & ((1u << kGroup) - 1u);
+                    const int first = gb ? __ffs(gb) - 1 : 0;  // group lane holding the first hit
+                    const uint32_t fh = __shfl_sync(0xFFFFFFFFu, myhit, gshift + first);
+                    const int j = __ffs(fh | 0x10u) - 1;       // 4 when the group has no hit
+                    const uint32_t pick = j == 0 ? vals[0] : j == 1 ? vals[1] : j == 2 ? vals[2] : vals[3];
+                    const uint32_t hp = __shfl_sync(0xFFFFFFFFu, pick, gshift + first);
+                    if (active) {
+                        if (gb) {
+                            hit_par = hp;
+                            hit_word = (qd - glane + first) * 4 + j;
+                            active = false;
+                        } else {
+                            qd += kGroup;
+                            if (qd - glane >= qb) active = false;
+                        }
                     }
                 }
-                my_insp += k;
-            } else {
-                atomicOr(&s.ctr->error, 4u);
-            }
-        }
-        // warp-cooperative scan of the lanes that still have edges left
-        uint32_t need = __ballot_sync(0xFFFFFFFFu, mine && !found && len > kPullSerial);
-        while (need) {
-            const int leader = __ffs(need) - 1;
-            need &= need - 1;
-            const unsigned long long lst = __shfl_sync(0xFFFFFFFFu, st, leader);
-            const uint32_t llen = __shfl_sync(0xFFFFFFFFu, len, leader);
-            uint32_t hit_par = kNoParent, scanned = llen - kPullSerial;
-            for (uint32_t j0 = kPullSerial; j0 < llen; j0 += 32) {
-                const uint32_t j = j0 + lane;
-                uint32_t u = 0;
-                bool hit = false;
-                if (j < llen) {
-                    u = __ldg(&g.pool[lst + (unsigned long long)j * ew]);
-                    hit = u < s.V && test_bit(s.front, u);
-                }
-                const uint32_t b = __ballot_sync(0xFFFFFFFFu, hit);
-                if (b) {
-                    const int first = __ffs(b) - 1;
-                    hit_par = __shfl_sync(0xFFFFFFFFu, u, first);
-                    scanned = j0 + first + 1 - kPullSerial;
-                    break;
+                if (mine && glane == 0) {
+                    t.inspected += (uint32_t)(hit_word - a) + (hit_par != kNoParent ? 1u : 0u);
+                    if (hit_par != kNoParent) {
+                        const uint32_t vv = bq_v[e];
+                        s.depth[vv] = s.level + 1;
+                        if (s.parent) s.parent[vv] = hit_par;
+                        atomicOr(&fnd[(vv >> 5) - (wlo + tile * kPullTileWords)], 1u << (vv & 31));
+                        const uint32_t dv = __ldg(&s.degree[vv]);
+                        t.next++;
+                        t.next_edges += dv;
+                        if (s.page_nodes) hist_add(sm, s, hist_same ? bq_p[e] : page_of(s.hg, vv), dv + 3);
+                    }
                 }
             }
-            if (lane == leader) {
-                my_insp += scanned;
-                if (hit_par != kNoParent) { found = 1; par = hit_par; }
+            __syncthreads();
+        }
+        // ---- the tile's visited / next words, written once
+        if (threadIdx.x < kPullTileWords && w < whi) {
+            const uint32_t f = fnd[threadIdx.x];
+            if (f) {
+                s.visited[w] |= f;
+                s.next[w] = f;
             }
         }
-        const uint32_t fmask = __ballot_sync(0xFFFFFFFFu, found);
-        if (found) {
-            s.depth[v] = s.level + 1;
-            if (s.parent) s.parent[v] = par;
-            const uint32_t dv = __ldg(&s.degree[v]);
-            my_next++;
-            my_edges += dv;
-            hist_add(hn, hd, s, v, dv + 3);
-        }
-        if (lane == 0 && fmask) {
-            s.visited[w] = vis | fmask;
-            s.next[w] = fmask;
-        }
+        __syncthreads();
     }
-    __syncthreads();
-    flush_acc<BLOCK>(&acc, my_next, my_edges, my_insp, my_hdr, s.ctr);
-    hist_flush<BLOCK>(hn, hd, s);
+    level_epilogue<BLOCK>(sm, s, t);
+}
+
+// graph mode: the level's state from the device control block
+__device__ __forceinline__ BfsDev level_state(const BfsGraphArgs &a)
+{
+    BfsDev s = a.base;
+    const BfsCtl *c = a.ctl;
+    const uint32_t L = c->level;
+    s.level = L;
+    s.depth = c->depth;
+    s.parent = c->parent;
+    s.front = a.bm3 + (size_t)(L % 3) * s.nwords;
+    s.next = a.bm3 + (size_t)((L + 1) % 3) * s.nwords;
+    s.ctr = a.ctr0 + L;
+    if (a.hist0 && L < a.hist_levels) {
+        s.page_nodes = a.hist0 + (size_t)L * 2 * a.npages_h;
+        s.page_datas = s.page_nodes + a.npages_h;
+    } else {
+        s.page_nodes = s.page_datas = nullptr;
+    }
+    return s;
+}
+
+// clears the bitmap the NEXT level will write (it held level L-1's frontier)
+__device__ __forceinline__ void clear_third(const BfsGraphArgs &a, uint32_t L)
+{
+    uint32_t *b = a.bm3 + (size_t)((L + 2) % 3) * a.base.nwords;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < a.base.nwords; i += gridDim.x * blockDim.x) b[i] = 0;
+}
+
+__device__ __forceinline__ unsigned long long globaltimer()
+{
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// kernels: host-argument versions
+// ---------------------------------------------------------------------------
+template <int BLOCK>
+__global__ void __launch_bounds__(BLOCK) k_push(GraphDev g, BfsDev s, uint32_t vlo, uint32_t vhi)
+{
+    push_body<BLOCK>(g, s, vlo, vhi);
+}
+
+template <int BLOCK>
+__global__ void __launch_bounds__(BLOCK) k_push_giant(GraphDev g, BfsDev s)
+{
+    giant_body<BLOCK>(g, s);
+}
+
+template <int BLOCK>
+__global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) k_pull(GraphDev g, BfsDev s, uint32_t vlo, uint32_t vhi)
+{
+    pull_body<BLOCK>(g, s, vlo, vhi);
 }
 
 // ---------------------------------------------------------------------------
-// state init: depth = unreached, parent = none, bitmaps cleared, then the
-// source (bfs_init + setsrc of app/bfs.cu:20-37)
+// kernels: graph mode
+// ---------------------------------------------------------------------------
+template <int BLOCK>
+__global__ void __launch_bounds__(BLOCK) k_push_g(GraphDev g, BfsGraphArgs a)
+{
+    const BfsDev s = level_state(a);
+    clear_third(a, s.level);
+    push_body<BLOCK>(g, s, 0, s.V);
+}
+
+template <int BLOCK>
+__global__ void __launch_bounds__(BLOCK) k_push_giant_g(GraphDev g, BfsGraphArgs a)
+{
+    giant_body<BLOCK>(g, level_state(a));
+}
+
+template <int BLOCK>
+__global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) k_pull_g(GraphDev g, BfsGraphArgs a)
+{
+    const BfsDev s = level_state(a);
+    clear_third(a, s.level);
+    pull_body<BLOCK>(g, s, 0, s.V);
+}
+
+// First node of a BFS graph: run inputs into the control block, state reset
+// (bfs_init, app/bfs.cu:20-30: depth = unreached, nothing active).
+__global__ void k_graph_init(BfsGraphArgs a, uint32_t *depth, uint32_t *parent, uint32_t src, uint32_t unreached,
+                             const uint32_t *dead, uint32_t nlevels_clear)
+{
+    const BfsDev &b = a.base;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        BfsCtl *c = a.ctl;
+        c->depth = depth;
+        c->parent = parent;
+        c->src = src;
+        c->level = 0;
+        c->dir = 0;
+        c->done = 0;
+        c->t_start = globaltimer();
+    }
+    const size_t stride = (size_t)gridDim.x * blockDim.x;
+    const size_t i0 = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    for (size_t i = i0; i < b.V; i += stride) {
+        depth[i] = unreached;
+        if (parent) parent[i] = kNoParent;
+    }
+    for (size_t i = i0; i < b.nwords; i += stride) b.visited[i] = dead ? dead[i] : 0u;
+    for (size_t i = i0; i < 3ull * b.nwords; i += stride) a.bm3[i] = 0u;
+    uint32_t *cw = reinterpret_cast<uint32_t *>(a.ctr0);
+    const size_t nc = (size_t)nlevels_clear * sizeof(LevelCounters) / 4;
+    for (size_t i = i0; i < nc; i += stride) cw[i] = 0u;
+    if (a.hist0) {
+        const size_t nh = (size_t)a.hist_levels * 2 * a.npages_h;
+        for (size_t i = i0; i < nh; i += stride) a.hist0[i] = 0u;
+    }
+}
+
+// Second node: the source (setsrc, app/bfs.cu:32-37) and the loop state.
+__global__ void k_graph_start(BfsGraphArgs a)
+{
+    BfsCtl *c = a.ctl;
+    const uint32_t s = c->src;
+    c->depth[s] = 0;
+    if (c->parent) c->parent[s] = s;
+    a.base.visited[s >> 5] |= 1u << (s & 31);
+    a.bm3[s >> 5] |= 1u << (s & 31);
+    const unsigned long long d = a.base.degree[s];
+    c->nf = 1;
+    c->prev_nf = 0;
+    c->mf = d;
+    c->vis_n = 1;
+    c->vis_e = d;
+}
+
+// Last node of each level: counters -> next direction (Beamer alpha/beta, or
+// the forced direction) and the conditionals of the next iteration.
+__global__ void k_decide(BfsGraphArgs a, DecideArgs d, cudaGraphConditionalHandle h_loop,
+                         cudaGraphConditionalHandle h_push, cudaGraphConditionalHandle h_pull)
+{
+    BfsCtl *c = a.ctl;
+    const uint32_t L = c->level;
+    LevelCounters *lc = a.ctr0 + L;
+    lc->dir = c->dir;
+    lc->t_end = globaltimer();
+    c->prev_nf = c->nf;
+    c->nf = lc->next;
+    c->mf = lc->next_edges;
+    c->vis_n += c->nf;
+    c->vis_e += c->mf;
+    const bool stop = c->nf == 0 || lc->error != 0 || (int)L + 1 >= d.max_levels ||
+                      (unsigned long long)L + 2 >= d.unreached;
+    if (stop) {
+        c->done = 1;
+        cudaGraphSetConditional(h_loop, 0);
+        cudaGraphSetConditional(h_push, 0);
+        cudaGraphSetConditional(h_pull, 0);
+        return;
+    }
+    const unsigned long long used = c->vis_e + d.dead_edges;
+    const unsigned long long mu = d.E > used ? d.E - used : 0;
+    int nd;
+    if (d.mode == 1) nd = 0;
+    else if (d.mode == 2) nd = 1;
+    else nd = alpha_beta_next(c->dir, c->nf, c->prev_nf, c->mf, mu, d.V, d.alpha, d.beta);
+    c->dir = nd;
+    c->level = L + 1;
+    cudaGraphSetConditional(h_push, nd == 0 ? 1 : 0);
+    cudaGraphSetConditional(h_pull, nd == 1 ? 1 : 0);
+    cudaGraphSetConditional(h_loop, 1);
+}
+
+// ---------------------------------------------------------------------------
+// state init helpers (host loop)
 // ---------------------------------------------------------------------------
 __global__ void k_fill_u32_scalar(uint32_t *p, uint32_t value, unsigned long long n)
 {
@@ -438,16 +715,13 @@ __global__ void k_set_source(BfsDev s, uint32_t src, uint32_t *front)
 // ---------------------------------------------------------------------------
 // host launchers
 // ---------------------------------------------------------------------------
-// The push kernel's static shared memory (tile queue + page histogram) caps
-// it at 256 threads; 512-thread configurations run push at 256.
 template <int BLOCK>
 static cudaError_t launch_level(int dir, int grid, const GraphDev &g, const BfsDev &s, uint32_t vlo, uint32_t vhi,
                                 cudaStream_t st)
 {
-    constexpr int PB = BLOCK > 256 ? 256 : BLOCK;
     if (dir == 0) {
-        k_push<PB><<<grid, PB, 0, st>>>(g, s, vlo, vhi);
-        k_push_giant<PB><<<grid, PB, 0, st>>>(g, s);
+        k_push<BLOCK><<<grid, BLOCK, 0, st>>>(g, s, vlo, vhi);
+        k_push_giant<BLOCK><<<grid, BLOCK, 0, st>>>(g, s);
     } else {
         k_pull<BLOCK><<<grid, BLOCK, 0, st>>>(g, s, vlo, vhi);
     }
@@ -464,17 +738,41 @@ cudaError_t run_level(int dir, int block, int grid, const GraphDev &g, const Bfs
     }
 }
 
+template <int BLOCK>
+static cudaError_t launch_level_g(int dir, int grid, const GraphDev &g, const BfsGraphArgs &a, cudaStream_t st)
+{
+    if (dir == 0) {
+        k_push_g<BLOCK><<<grid, BLOCK, 0, st>>>(g, a);
+        k_push_giant_g<BLOCK><<<grid, BLOCK, 0, st>>>(g, a);
+    } else {
+        k_pull_g<BLOCK><<<grid, BLOCK, 0, st>>>(g, a);
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t run_level_graph(int dir, int block, int grid, const GraphDev &g, const BfsGraphArgs &a, cudaStream_t st)
+{
+    switch (block) {
+    case 128: return launch_level_g<128>(dir, grid, g, a, st);
+    case 512: return launch_level_g<512>(dir, grid, g, a, st);
+    default: return launch_level_g<256>(dir, grid, g, a, st);
+    }
+}
+
+const void *graph_init_kernel() { return (const void *)k_graph_init; }
+const void *graph_start_kernel() { return (const void *)k_graph_start; }
+const void *decide_kernel() { return (const void *)k_decide; }
+
 int level_occupancy(int dir, int block)
 {
     int n = 0;
+    const void *f = nullptr;
     switch (block) {
-    case 128: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, dir ? (const void *)k_pull<128> : (const void *)k_push<128>, 128, 0); break;
-    case 512:
-        if (dir) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, (const void *)k_pull<512>, 512, 0);
-        else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, (const void *)k_push<256>, 256, 0);
-        break;
-    default: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, dir ? (const void *)k_pull<256> : (const void *)k_push<256>, 256, 0); break;
+    case 128: f = dir ? (const void *)k_pull<128> : (const void *)k_push<128>; break;
+    case 512: f = dir ? (const void *)k_pull<512> : (const void *)k_push<512>; break;
+    default: f = dir ? (const void *)k_pull<256> : (const void *)k_push<256>; break;
     }
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, f, block, 0);
     return n;
 }
 

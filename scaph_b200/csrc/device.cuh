@@ -8,8 +8,10 @@ namespace scaph {
 
 constexpr unsigned long long kNotResident = ~0ull;
 constexpr uint32_t kNoParent = 0xFFFFFFFFu;
-constexpr int kHistCap = 1024;          // pages histogrammed in shared memory
-constexpr uint32_t kGiantEdges = 4096;  // push: adjacency longer than this is split
+constexpr int kHistCap = 512;           // pages histogrammed in shared memory
+constexpr int kLutPages = 512;          // page-table entries staged in shared memory
+constexpr int kLutCoarse = 1024;        // coarse-index entries staged in shared memory
+constexpr uint32_t kGiantEdges = 1024;  // push: adjacency longer than this is split
 constexpr int kMaxLevels = 4096;        // hard cap on BFS levels per run
 
 // One page of the device page table.  `base` is the word offset of the page's
@@ -23,10 +25,10 @@ struct __align__(16) PageDev {
 
 // Device view of one paged graph (out-edges, or in-edges for pull).
 struct GraphDev {
-    const uint32_t *pool;      // page pool, 16-byte aligned, slots of pagesize words
-    const PageDev *pages;      // npages + 1 entries; pages[npages].left == V
-    const uint32_t *coarse;    // coarse[i] = page holding vertex i << cshift
-    const uint32_t *zc_pool;   // host pages mapped for zero-copy reads (or null)
+    const uint32_t *pool;           // page pool, 16-byte aligned, slots of pagesize words
+    const PageDev *pages;           // npages + 1 entries; pages[npages].left == V
+    const uint32_t *coarse;         // coarse[i] = page holding vertex i << cshift
+    const uint32_t *zc_pool;        // host pages mapped for zero-copy reads (or null)
     unsigned long long pool_words;  // words addressable through `pool`
     uint32_t cshift;
     uint32_t npages;
@@ -43,6 +45,9 @@ struct LevelCounters {
     unsigned int giant;             // giant chunks queued (push)
     unsigned int error;             // nonzero: a kernel saw a bad index / overflow
     unsigned long long zc_words;    // words read zero-copy from host pages
+    int dir;                        // direction the level ran (graph mode)
+    unsigned int _pad;
+    unsigned long long t_end;       // %globaltimer when the level was decided (graph mode)
 };
 
 struct GiantChunk {
@@ -65,8 +70,67 @@ struct BfsDev {
     uint32_t giant_cap;
     uint32_t level;            // discovered vertices get depth level+1
     uint32_t V;
-    uint32_t weighted_edges;   // 1: pages hold {ngr,wgh} pairs (stride 2)
+    uint32_t nwords;           // (V + 31) / 32
     GraphDev hg;               // out-edge graph whose pages the histogram counts
+};
+
+// Graph mode: state of one traversal kept on the device, so a whole BFS runs
+// as one CUDA-graph launch with the level loop in a conditional WHILE node.
+struct BfsCtl {
+    uint32_t *depth;
+    uint32_t *parent;
+    uint32_t src;
+    uint32_t level;            // level being run
+    int32_t dir;               // 0 push, 1 pull
+    int32_t done;
+    unsigned long long nf, prev_nf, mf, vis_n, vis_e;
+    unsigned long long t_start;
+};
+
+// Static inputs of the graph-mode level kernels.
+struct BfsGraphArgs {
+    BfsDev base;               // depth/parent/front/next/ctr/level filled per level
+    uint32_t *bm3;             // three rotating frontier bitmaps, nwords each
+    LevelCounters *ctr0;       // counters of level 0 (level L at ctr0 + L)
+    uint32_t *hist0;           // histograms: level L at hist0 + L*2*npages_h (or null)
+    uint32_t hist_levels;
+    uint32_t npages_h;
+    BfsCtl *ctl;
+};
+
+struct DecideArgs {
+    unsigned long long E;           // out-edges (for m_u)
+    unsigned long long dead_edges;  // out-edges of vertices no edge reaches
+    unsigned long long dead;        // vertices no edge reaches
+    uint32_t V;
+    uint32_t unreached;
+    int32_t mode;                   // SCAPH_DIR_*
+    float alpha, beta;
+    int32_t max_levels;
+};
+
+// Beamer's direction-optimizing rule (SC'12): leave top-down when the
+// frontier's out-edges exceed the unexplored edges / alpha; leave bottom-up
+// when the frontier is below V / beta and shrinking.  0 = push, 1 = pull.
+__host__ __device__ inline int alpha_beta_next(int cur_dir, unsigned long long nf, unsigned long long prev_nf,
+                                               unsigned long long mf, unsigned long long mu, unsigned long long V,
+                                               float alpha, float beta)
+{
+    if (cur_dir == 0) return (double)mf > (double)mu / alpha ? 1 : 0;
+    return ((double)nf < (double)V / beta && nf < prev_nf) ? 0 : 1;
+}
+
+// Page lookup (page table + coarse index), in global or shared memory.
+struct PageLut {
+    const PageDev *pages;
+    const uint32_t *coarse;
+    uint32_t cshift;
+    __device__ __forceinline__ int of(uint32_t v) const
+    {
+        int p = (int)coarse[v >> cshift];
+        while (pages[p + 1].left <= v) ++p;
+        return p;
+    }
 };
 
 __device__ __forceinline__ int page_of(const GraphDev &g, uint32_t v)

@@ -2,9 +2,17 @@
 // level loop with the direction switch.  Replaces App (src/app.cuh:72-345)
 // for the BFS application: App::load_graph's allocations and pool fill
 // (src/app.cuh:267-345), App::run's round loop (:220-265) and iter_init's
-// per-round D2H of the whole stat array (:188-207).  Here the round loop is
-// a level-synchronous BFS; the only per-level host traffic is one 48-byte
-// counter record.
+// per-round D2H of the whole stat array (:188-207).
+//
+// Two ways to run the level loop:
+//  * graph mode (default when the whole graph is resident): one CUDA-graph
+//    launch per BFS.  Its level loop is a conditional WHILE node whose body
+//    is IF(push){push, giant} -> IF(pull){pull} -> decide; the decide kernel
+//    applies the direction rule on the device and sets the conditionals, so
+//    a BFS never returns to the host between levels;
+//  * host loop: one launch per level and a 64-byte counter read-back,
+//    with CUDA events around every level (per-level kernel timing) - used
+//    for out-of-core page batches and for the roofline pass.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -84,13 +92,6 @@ void DeviceGraph::release()
     coarse = nullptr;
 }
 
-int alpha_beta_next(int cur_dir, uint64_t nf, uint64_t prev_nf, uint64_t mf, uint64_t mu, uint64_t V,
-                    float alpha, float beta)
-{
-    if (cur_dir == 0) return (double)mf > (double)mu / alpha ? 1 : 0;
-    return ((double)nf < (double)V / beta && nf < prev_nf) ? 0 : 1;
-}
-
 }  // namespace scaph
 
 struct scaph_engine {
@@ -108,25 +109,61 @@ struct scaph_engine {
     uint32_t unreached = 0xFFFFFFFFu;
     int block = 256, grid_push = 0, grid_pull = 0;
 
-    uint32_t *d_depth = nullptr, *d_parent = nullptr, *d_visited = nullptr, *d_bm[2] = {nullptr, nullptr};
-    uint32_t *d_degree = nullptr;
+    uint32_t *d_depth = nullptr, *d_parent = nullptr, *d_visited = nullptr, *d_bm3 = nullptr;
+    uint32_t *d_degree = nullptr, *d_dead = nullptr;
+    uint64_t n_dead = 0, dead_edges = 0;
     LevelCounters *d_ctr = nullptr, *h_ctr = nullptr;
     uint32_t *d_hist = nullptr;  // [kHistLevels][2][npages]
     GiantChunk *d_giant = nullptr;
     uint32_t giant_cap = 0;
+    BfsCtl *d_ctl = nullptr, *h_ctl = nullptr;
     cudaEvent_t ev_start = nullptr, ev_stop = nullptr;
     std::vector<cudaEvent_t> ev_level;
 
+    // graph mode
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t gexec = nullptr;
+    cudaGraphNode_t n_init = nullptr;
+    cudaStream_t cap_st = nullptr;
+    BfsGraphArgs gargs{};
+    DecideArgs dargs{};
+
+    // last run
     std::vector<scaph_level_trace> trace;
     int last_levels = 0;
+    bool pending = false;  // a graph-mode run whose trace has not been read back
+    uint32_t pending_src = 0;
+    bool pending_parent = false;
+    scaph_bfs_stats last_stats{};
 
     static constexpr int kHistLevels = 256;
 
     const GraphDev &gin() const { return symmetric ? dout.view : din.view; }
+    bool graph_mode() const { return cfg.use_graph != 2; }
     int create(const Graph *g_, const Graph *gt_, const scaph_config *c);
     void destroy();
     int bfs(uint32_t src, uint32_t *depths, uint32_t *parents, int out_on_device, scaph_bfs_stats *stats);
+    int run_host_loop(uint32_t src, uint32_t *dd, uint32_t *dp);
+    int build_graph();
+    int launch_graph(uint32_t src, uint32_t *dd, uint32_t *dp);
+    int collect(bool from_graph);
+    BfsDev base_state(uint32_t *dd, uint32_t *dp) const;
 };
+
+BfsDev scaph_engine::base_state(uint32_t *dd, uint32_t *dp) const
+{
+    BfsDev s{};
+    s.depth = dd;
+    s.parent = dp;
+    s.visited = d_visited;
+    s.degree = d_degree;
+    s.giant = d_giant;
+    s.giant_cap = giant_cap;
+    s.V = V;
+    s.nwords = nwords;
+    s.hg = dout.view;
+    return s;
+}
 
 int scaph_engine::create(const Graph *g_, const Graph *gt_, const scaph_config *c)
 {
@@ -138,6 +175,7 @@ int scaph_engine::create(const Graph *g_, const Graph *gt_, const scaph_config *
     E = g->E;
     nwords = (V + 31) / 32;
     unreached = cfg.unreached ? cfg.unreached : 0xFFFFFFFFu;
+    if (unreached < 2) return set_error(SCAPH_EINVAL, "unreached sentinel must be >= 2");
     if (cfg.alpha <= 0) cfg.alpha = 14.0f;
     if (cfg.beta <= 0) cfg.beta = 24.0f;
     block = cfg.block_size == 128 || cfg.block_size == 512 ? cfg.block_size : 256;
@@ -159,21 +197,37 @@ int scaph_engine::create(const Graph *g_, const Graph *gt_, const scaph_config *
         const int64_t per = (int64_t)g->pagesize * 4;
         nslots = (int)std::max<int64_t>(1, cfg.pool_bytes / per);
         if (nslots < (int)g->pages.size() || (gt && nslots < (int)gt->pages.size()))
-            return set_error(SCAPH_EUNSUPPORTED, "pool of %d pages smaller than the graph: use scaph_ooc_create", nslots);
+            return set_error(SCAPH_EUNSUPPORTED, "pool of %d pages smaller than the graph: use the out-of-core engine",
+                             nslots);
     }
     int rc = dout.build(*g, nslots, st);
     if (rc) return rc;
     if (gt && (rc = din.build(*gt, nslots, st))) return rc;
 
+    // vertices no edge reaches (in-degree 0) are never discovered: they start
+    // out "visited" so pull levels skip them
+    const std::vector<uint32_t> &indeg = gt ? gt->degree : g->degree;
+    std::vector<uint32_t> dead(nwords, 0);
+    for (uint32_t v = 0; v < V; v++) {
+        if (indeg[v] == 0) {
+            dead[v >> 5] |= 1u << (v & 31);
+            n_dead++;
+            dead_edges += g->degree[v];
+        }
+    }
+    SCAPH_CUDA(cudaMalloc(&d_dead, (size_t)nwords * 4));
+    SCAPH_CUDA(cudaMemcpyAsync(d_dead, dead.data(), (size_t)nwords * 4, cudaMemcpyHostToDevice, st));
+
     SCAPH_CUDA(cudaMalloc(&d_depth, (size_t)V * 4));
     SCAPH_CUDA(cudaMalloc(&d_parent, (size_t)V * 4));
     SCAPH_CUDA(cudaMalloc(&d_visited, (size_t)nwords * 4));
-    SCAPH_CUDA(cudaMalloc(&d_bm[0], (size_t)nwords * 4));
-    SCAPH_CUDA(cudaMalloc(&d_bm[1], (size_t)nwords * 4));
+    SCAPH_CUDA(cudaMalloc(&d_bm3, (size_t)nwords * 4 * 3));
     SCAPH_CUDA(cudaMalloc(&d_degree, (size_t)V * 4));
     SCAPH_CUDA(cudaMemcpyAsync(d_degree, g->degree.data(), (size_t)V * 4, cudaMemcpyHostToDevice, st));
     SCAPH_CUDA(cudaMalloc(&d_ctr, sizeof(LevelCounters) * kMaxLevels));
     SCAPH_CUDA(cudaMallocHost(&h_ctr, sizeof(LevelCounters) * kMaxLevels));
+    SCAPH_CUDA(cudaMalloc(&d_ctl, sizeof(BfsCtl)));
+    SCAPH_CUDA(cudaMallocHost(&h_ctl, sizeof(BfsCtl)));
     const size_t np = g->pages.size();
     SCAPH_CUDA(cudaMalloc(&d_hist, sizeof(uint32_t) * 2 * np * kHistLevels));
     giant_cap = (uint32_t)std::min<uint64_t>(0xFFFFFFF0u, 2 * (E / kGiantEdges) + 1024);
@@ -193,16 +247,21 @@ int scaph_engine::create(const Graph *g_, const Graph *gt_, const scaph_config *
 void scaph_engine::destroy()
 {
     if (st) cudaStreamSynchronize(st);
+    if (gexec) cudaGraphExecDestroy(gexec);
+    if (graph) cudaGraphDestroy(graph);
+    if (cap_st) cudaStreamDestroy(cap_st);
     dout.release();
     din.release();
     cudaFree(d_depth);
     cudaFree(d_parent);
     cudaFree(d_visited);
-    cudaFree(d_bm[0]);
-    cudaFree(d_bm[1]);
+    cudaFree(d_bm3);
     cudaFree(d_degree);
+    cudaFree(d_dead);
     cudaFree(d_ctr);
     cudaFreeHost(h_ctr);
+    cudaFree(d_ctl);
+    cudaFreeHost(h_ctl);
     cudaFree(d_hist);
     cudaFree(d_giant);
     if (ev_start) cudaEventDestroy(ev_start);
@@ -211,54 +270,36 @@ void scaph_engine::destroy()
     if (own_stream && st) cudaStreamDestroy(st);
 }
 
-int scaph_engine::bfs(uint32_t src, uint32_t *depths, uint32_t *parents, int out_on_device, scaph_bfs_stats *stats)
+// Host-driven level loop (one launch + one counter read-back per level).
+int scaph_engine::run_host_loop(uint32_t src, uint32_t *dd, uint32_t *dp)
 {
-    if (src >= V) return set_error(SCAPH_EINVAL, "source %u out of range (V=%u)", src, V);
-    SCAPH_CUDA(cudaSetDevice(device));
-    uint32_t *dd = (out_on_device && depths) ? depths : d_depth;
-    uint32_t *dp = (out_on_device && parents) ? parents : (parents ? d_parent : nullptr);
     const int fill_grid = num_sms * 4;
     const size_t np = g->pages.size();
-    trace.clear();
-
-    SCAPH_CUDA(cudaEventRecord(ev_start, st));
-    // bfs_init + setsrc (app/bfs.cu:20-37)
     SCAPH_CUDA(fill_u32(dd, unreached, V, fill_grid, st));
     if (dp) SCAPH_CUDA(fill_u32(dp, kNoParent, V, fill_grid, st));
-    SCAPH_CUDA(cudaMemsetAsync(d_visited, 0, (size_t)nwords * 4, st));
-    SCAPH_CUDA(cudaMemsetAsync(d_bm[0], 0, (size_t)nwords * 4, st));
+    SCAPH_CUDA(cudaMemcpyAsync(d_visited, d_dead, (size_t)nwords * 4, cudaMemcpyDeviceToDevice, st));
+    SCAPH_CUDA(cudaMemsetAsync(d_bm3, 0, (size_t)nwords * 4, st));
     SCAPH_CUDA(cudaMemsetAsync(d_ctr, 0, sizeof(LevelCounters) * kMaxLevels, st));
     SCAPH_CUDA(cudaMemsetAsync(d_hist, 0, sizeof(uint32_t) * 2 * np * kHistLevels, st));
-
-    BfsDev s{};
-    s.depth = dd;
-    s.parent = dp;
-    s.visited = d_visited;
-    s.degree = d_degree;
-    s.giant = d_giant;
-    s.giant_cap = giant_cap;
-    s.V = V;
-    s.weighted_edges = 0;
-    s.hg = dout.view;
-    SCAPH_CUDA(set_source(s, src, d_bm[0], st));
+    BfsDev s = base_state(dd, dp);
+    uint32_t *bm[2] = {d_bm3, d_bm3 + nwords};
+    SCAPH_CUDA(set_source(s, src, bm[0], st));
 
     uint64_t nf = 1, prev_nf = 0, mf = g->degree[src];
-    uint64_t vis_n = 1, vis_e = mf;
-    uint64_t insp_total = 0, alg_total = 0;
-    uint64_t launches = dp ? 3 : 2;  // fills + set_source
-    int dir = 0, cur = 0, level = 0, npush = 0, npull = 0;
-    uint32_t err = 0;
+    uint64_t vis_e = mf;
+    int dir = 0, cur = 0, level = 0;
     while (nf > 0 && level < kMaxLevels && (uint64_t)level + 1 < unreached) {
-        const uint64_t mu = E - vis_e;
+        const uint64_t used = vis_e + dead_edges;
+        const uint64_t mu = E > used ? E - used : 0;
         switch (cfg.direction) {
         case SCAPH_DIR_PUSH: dir = 0; break;
         case SCAPH_DIR_PULL: dir = level == 0 ? 0 : 1; break;
         default: dir = level == 0 ? 0 : alpha_beta_next(dir, nf, prev_nf, mf, mu, V, cfg.alpha, cfg.beta); break;
         }
-        uint32_t *next = d_bm[cur ^ 1];
+        uint32_t *next = bm[cur ^ 1];
         SCAPH_CUDA(cudaEventRecord(ev_level[2 * level], st));
         SCAPH_CUDA(cudaMemsetAsync(next, 0, (size_t)nwords * 4, st));
-        s.front = d_bm[cur];
+        s.front = bm[cur];
         s.next = next;
         s.ctr = d_ctr + level;
         s.level = (uint32_t)level;
@@ -273,71 +314,238 @@ int scaph_engine::bfs(uint32_t src, uint32_t *depths, uint32_t *parents, int out
         SCAPH_CUDA(cudaEventRecord(ev_level[2 * level + 1], st));
         SCAPH_CUDA(cudaMemcpyAsync(h_ctr + level, d_ctr + level, sizeof(LevelCounters), cudaMemcpyDeviceToHost, st));
         SCAPH_CUDA(cudaStreamSynchronize(st));
-        const LevelCounters &lc = h_ctr[level];
+        h_ctr[level].dir = dir;
+        if (h_ctr[level].error) {
+            level++;
+            break;
+        }
+        prev_nf = nf;
+        nf = h_ctr[level].next;
+        mf = h_ctr[level].next_edges;
+        vis_e += mf;
+        cur ^= 1;
+        level++;
+    }
+    last_levels = level;
+    return SCAPH_OK;
+}
+
+int scaph_engine::build_graph()
+{
+    SCAPH_CUDA(cudaStreamCreateWithFlags(&cap_st, cudaStreamNonBlocking));
+    SCAPH_CUDA(cudaGraphCreate(&graph, 0));
+    cudaGraphConditionalHandle h_loop, h_push, h_pull;
+    SCAPH_CUDA(cudaGraphConditionalHandleCreate(&h_loop, graph, 1, cudaGraphCondAssignDefault));
+    SCAPH_CUDA(cudaGraphConditionalHandleCreate(&h_push, graph, 1, cudaGraphCondAssignDefault));
+    SCAPH_CUDA(cudaGraphConditionalHandleCreate(&h_pull, graph, 0, cudaGraphCondAssignDefault));
+
+    const size_t np = g->pages.size();
+    gargs.base = base_state(d_depth, nullptr);
+    gargs.bm3 = d_bm3;
+    gargs.ctr0 = d_ctr;
+    gargs.hist0 = d_hist;
+    gargs.hist_levels = kHistLevels;
+    gargs.npages_h = (uint32_t)np;
+    gargs.ctl = d_ctl;
+    dargs.E = E;
+    dargs.dead_edges = dead_edges;
+    dargs.dead = n_dead;
+    dargs.V = V;
+    dargs.unreached = unreached;
+    dargs.mode = cfg.direction == SCAPH_DIR_PUSH ? 1 : cfg.direction == SCAPH_DIR_PULL ? 2 : 0;
+    dargs.alpha = cfg.alpha;
+    dargs.beta = cfg.beta;
+    dargs.max_levels = kMaxLevels;
+
+    // init (run inputs are this node's arguments, replaced per launch)
+    uint32_t *depth0 = d_depth, *parent0 = nullptr, src0 = 0, unr = unreached, nclear = kMaxLevels;
+    const uint32_t *dead = d_dead;
+    void *init_args[] = {&gargs, &depth0, &parent0, &src0, &unr, &dead, &nclear};
+    cudaKernelNodeParams kp{};
+    kp.func = const_cast<void *>(graph_init_kernel());
+    kp.gridDim = dim3(num_sms * 4);
+    kp.blockDim = dim3(256);
+    kp.kernelParams = init_args;
+    SCAPH_CUDA(cudaGraphAddKernelNode(&n_init, graph, nullptr, 0, &kp));
+    void *start_args[] = {&gargs};
+    cudaKernelNodeParams sp{};
+    sp.func = const_cast<void *>(graph_start_kernel());
+    sp.gridDim = dim3(1);
+    sp.blockDim = dim3(1);
+    sp.kernelParams = start_args;
+    cudaGraphNode_t n_start;
+    SCAPH_CUDA(cudaGraphAddKernelNode(&n_start, graph, &n_init, 1, &sp));
+
+    // WHILE(loop) { IF(push){push, giant}; IF(pull){pull}; decide }
+    cudaGraphNodeParams wp{};
+    wp.type = cudaGraphNodeTypeConditional;
+    wp.conditional.handle = h_loop;
+    wp.conditional.type = cudaGraphCondTypeWhile;
+    wp.conditional.size = 1;
+    cudaGraphNode_t n_while;
+    SCAPH_CUDA(cudaGraphAddNode(&n_while, graph, &n_start, 1, &wp));
+    cudaGraph_t body = wp.conditional.phGraph_out[0];
+
+    cudaGraphNodeParams ip{};
+    ip.type = cudaGraphNodeTypeConditional;
+    ip.conditional.handle = h_push;
+    ip.conditional.type = cudaGraphCondTypeIf;
+    ip.conditional.size = 1;
+    cudaGraphNode_t n_ifpush;
+    SCAPH_CUDA(cudaGraphAddNode(&n_ifpush, body, nullptr, 0, &ip));
+    cudaGraph_t bpush = ip.conditional.phGraph_out[0];
+
+    cudaGraphNodeParams iq{};
+    iq.type = cudaGraphNodeTypeConditional;
+    iq.conditional.handle = h_pull;
+    iq.conditional.type = cudaGraphCondTypeIf;
+    iq.conditional.size = 1;
+    cudaGraphNode_t n_ifpull;
+    SCAPH_CUDA(cudaGraphAddNode(&n_ifpull, body, &n_ifpush, 1, &iq));
+    cudaGraph_t bpull = iq.conditional.phGraph_out[0];
+
+    void *dec_args[] = {&gargs, &dargs, &h_loop, &h_push, &h_pull};
+    cudaKernelNodeParams dp{};
+    dp.func = const_cast<void *>(decide_kernel());
+    dp.gridDim = dim3(1);
+    dp.blockDim = dim3(1);
+    dp.kernelParams = dec_args;
+    cudaGraphNode_t n_decide;
+    SCAPH_CUDA(cudaGraphAddKernelNode(&n_decide, body, &n_ifpull, 1, &dp));
+
+    SCAPH_CUDA(cudaStreamBeginCaptureToGraph(cap_st, bpush, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
+    cudaError_t e1 = run_level_graph(0, block, grid_push, dout.view, gargs, cap_st);
+    SCAPH_CUDA(cudaStreamEndCapture(cap_st, &bpush));
+    SCAPH_CUDA(e1);
+    SCAPH_CUDA(cudaStreamBeginCaptureToGraph(cap_st, bpull, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
+    cudaError_t e2 = run_level_graph(1, block, grid_pull, gin(), gargs, cap_st);
+    SCAPH_CUDA(cudaStreamEndCapture(cap_st, &bpull));
+    SCAPH_CUDA(e2);
+    SCAPH_CUDA(cudaGraphInstantiate(&gexec, graph, 0));
+    return SCAPH_OK;
+}
+
+int scaph_engine::launch_graph(uint32_t src, uint32_t *dd, uint32_t *dp)
+{
+    if (!gexec) {
+        int rc = build_graph();
+        if (rc) return rc;
+    }
+    uint32_t unr = unreached, nclear = kMaxLevels;
+    const uint32_t *dead = d_dead;
+    void *init_args[] = {&gargs, &dd, &dp, &src, &unr, &dead, &nclear};
+    cudaKernelNodeParams kp{};
+    kp.func = const_cast<void *>(graph_init_kernel());
+    kp.gridDim = dim3(num_sms * 4);
+    kp.blockDim = dim3(256);
+    kp.kernelParams = init_args;
+    SCAPH_CUDA(cudaGraphExecKernelNodeSetParams(gexec, n_init, &kp));
+    SCAPH_CUDA(cudaGraphLaunch(gexec, st));
+    return SCAPH_OK;
+}
+
+// Reads back the counters of the last run and rebuilds trace + stats.
+int scaph_engine::collect(bool from_graph)
+{
+    const size_t np = g->pages.size();
+    (void)np;
+    if (from_graph) {
+        SCAPH_CUDA(cudaMemcpyAsync(h_ctl, d_ctl, sizeof(BfsCtl), cudaMemcpyDeviceToHost, st));
+        SCAPH_CUDA(cudaStreamSynchronize(st));
+        last_levels = (int)h_ctl->level + 1;
+        SCAPH_CUDA(cudaMemcpyAsync(h_ctr, d_ctr, sizeof(LevelCounters) * last_levels, cudaMemcpyDeviceToHost, st));
+        SCAPH_CUDA(cudaStreamSynchronize(st));
+    }
+    const uint32_t src = pending_src;
+    const bool dp = pending_parent;
+    trace.clear();
+    uint64_t nf = 1, mf = g->degree[src], vis_n = 1, vis_e = mf, insp = 0, alg = 0, launches = 0;
+    int npush = 0, npull = 0;
+    uint32_t err = 0;
+    const bool src_dead = gt ? gt->degree[src] == 0 : g->degree[src] == 0;
+    unsigned long long tprev = from_graph ? h_ctl->t_start : 0;
+    launches = from_graph ? 2 : (dp ? 3 : 2);
+    for (int l = 0; l < last_levels; l++) {
+        const LevelCounters &lc = h_ctr[l];
         err |= lc.error;
         scaph_level_trace t{};
-        t.level = level;
-        t.direction = dir;
+        t.level = l;
+        t.direction = lc.dir;
         t.frontier = nf;
         t.frontier_edges = mf;
-        t.unvisited = V - vis_n;
-        t.unvisited_edges = mu;
+        const uint64_t used = vis_e + dead_edges;
+        t.unvisited = (uint64_t)V - n_dead - vis_n + (src_dead ? 1 : 0);
+        t.unvisited_edges = E > used ? E - used : 0;
         t.next = lc.next;
         t.edges_inspected = lc.inspected;
-        trace.push_back(t);
         // algorithmic bytes (push: headers + adjacency of the frontier;
         // pull: headers of unvisited vertices + in-edges up to the first
-        // frontier hit; both: a V/8 bitmap pass and depth+parent writes)
+        // frontier hit; both: a V/8 bitmap pass and depth (+parent) writes)
         const uint64_t state_w = lc.next * (dp ? 8 : 4) + (uint64_t)nwords * 4;
-        const uint64_t alg = dir == 0 ? nf * 12 + mf * 4 + state_w : (V - vis_n) * 12 + lc.inspected * 4 + state_w;
-        trace.back().alg_bytes = alg;
-        alg_total += alg;
-        if (dir == 0) {
-            npush++;
-            launches += 2;
+        t.alg_bytes = lc.dir == 0 ? nf * 12 + mf * 4 + state_w : t.unvisited * 12 + lc.inspected * 4 + state_w;
+        if (from_graph) {
+            t.ms = (double)(lc.t_end - tprev) * 1e-6;
+            tprev = lc.t_end;
+            launches += (lc.dir == 0 ? 2 : 1) + 1;
         } else {
-            npull++;
-            launches += 1;
+            float ms = 0;
+            cudaEventElapsedTime(&ms, ev_level[2 * l], ev_level[2 * l + 1]);
+            t.ms = ms;
+            launches += lc.dir == 0 ? 2 : 1;
         }
-        insp_total += lc.inspected;
-        prev_nf = nf;
+        trace.push_back(t);
+        alg += t.alg_bytes;
+        insp += lc.inspected;
+        if (lc.dir == 0) npush++; else npull++;
         nf = lc.next;
         mf = lc.next_edges;
         vis_n += nf;
         vis_e += mf;
-        cur ^= 1;
-        level++;
-        if (err) break;
     }
-    SCAPH_CUDA(cudaEventRecord(ev_stop, st));
-    SCAPH_CUDA(cudaEventSynchronize(ev_stop));
-    last_levels = level;
-    for (int l = 0; l < level; l++) {
-        float ms = 0;
-        cudaEventElapsedTime(&ms, ev_level[2 * l], ev_level[2 * l + 1]);
-        trace[l].ms = ms;
-    }
+    memset(&last_stats, 0, sizeof(last_stats));
+    last_stats.levels = last_levels;
+    last_stats.push_levels = npush;
+    last_stats.pull_levels = npull;
+    last_stats.reached = vis_n;
+    last_stats.reached_edges = vis_e;
+    last_stats.edges_inspected = insp;
+    last_stats.alg_bytes = alg;
+    last_stats.launches = launches;
+    pending = false;
     if (err) return set_error(SCAPH_EDEVICE, "level kernel reported error flags 0x%x", err);
+    return SCAPH_OK;
+}
+
+int scaph_engine::bfs(uint32_t src, uint32_t *depths, uint32_t *parents, int out_on_device, scaph_bfs_stats *stats)
+{
+    if (src >= V) return set_error(SCAPH_EINVAL, "source %u out of range (V=%u)", src, V);
+    SCAPH_CUDA(cudaSetDevice(device));
+    uint32_t *dd = (out_on_device && depths) ? depths : d_depth;
+    uint32_t *dp = (out_on_device && parents) ? parents : (parents ? d_parent : nullptr);
+    pending_src = src;
+    pending_parent = dp != nullptr;
+    const bool use_graph = graph_mode();
+    SCAPH_CUDA(cudaEventRecord(ev_start, st));
+    int rc = use_graph ? launch_graph(src, dd, dp) : run_host_loop(src, dd, dp);
+    if (rc) return rc;
+    SCAPH_CUDA(cudaEventRecord(ev_stop, st));
     if (!out_on_device) {
         if (depths) SCAPH_CUDA(cudaMemcpyAsync(depths, dd, (size_t)V * 4, cudaMemcpyDeviceToHost, st));
         if (parents) SCAPH_CUDA(cudaMemcpyAsync(parents, dp, (size_t)V * 4, cudaMemcpyDeviceToHost, st));
-        SCAPH_CUDA(cudaStreamSynchronize(st));
     }
+    if (use_graph && out_on_device && !stats) {
+        pending = true;  // asynchronous: trace/stats read back on demand
+        return SCAPH_OK;
+    }
+    rc = collect(use_graph);
+    SCAPH_CUDA(cudaStreamSynchronize(st));
     if (stats) {
-        memset(stats, 0, sizeof(*stats));
+        *stats = last_stats;
         float ms = 0;
         cudaEventElapsedTime(&ms, ev_start, ev_stop);
         stats->ms = ms;
-        stats->levels = level;
-        stats->push_levels = npush;
-        stats->pull_levels = npull;
-        stats->reached = vis_n;
-        stats->reached_edges = vis_e;
-        stats->edges_inspected = insp_total;
-        stats->alg_bytes = alg_total;
-        stats->launches = launches;
     }
-    return SCAPH_OK;
+    return rc;
 }
 
 extern "C" {
@@ -373,27 +581,42 @@ int scaph_bfs(scaph_engine *e, uint32_t src, uint32_t *depths, uint32_t *parents
     return e->bfs(src, depths, parents, out_on_device, stats);
 }
 
-int scaph_bfs_trace(const scaph_engine *e, scaph_level_trace *out, int cap)
+int scaph_engine_sync(scaph_engine *e)
+{
+    if (!e) return set_error(SCAPH_EINVAL, "null engine");
+    SCAPH_CUDA(cudaStreamSynchronize(e->st));
+    return SCAPH_OK;
+}
+
+int scaph_bfs_trace(scaph_engine *e, scaph_level_trace *out, int cap)
 {
     if (!e || (!out && cap > 0)) return set_error(SCAPH_EINVAL, "null argument");
+    if (e->pending) {
+        int rc = e->collect(true);
+        if (rc) return rc;
+    }
     int n = std::min<int>(cap, (int)e->trace.size());
     for (int i = 0; i < n; i++) out[i] = e->trace[i];
     return n;
 }
 
-int scaph_bfs_page_hist(const scaph_engine *e, int level, uint32_t *nodes, uint32_t *datas, int npages)
+int scaph_bfs_page_hist(scaph_engine *e, int level, uint32_t *nodes, uint32_t *datas, int npages)
 {
     if (!e || !nodes || !datas) return set_error(SCAPH_EINVAL, "null argument");
+    if (e->pending) {
+        int rc = e->collect(true);
+        if (rc) return rc;
+    }
     const int np = (int)e->g->pages.size();
     if (npages < np) return set_error(SCAPH_EINVAL, "need %d pages", np);
-    // histogram slot `level` holds the frontier discovered BY level; the
-    // frontier AT level L is slot L-1 (level 0 is the source alone)
+    // histogram slot L holds the frontier discovered BY level L, i.e. the
+    // frontier AT level L+1 (level 0's frontier is the source alone)
     if (level < 0 || level > e->last_levels || level > scaph_engine::kHistLevels)
         return set_error(SCAPH_EINVAL, "level %d not recorded", level);
     if (level == 0) {
         memset(nodes, 0, sizeof(uint32_t) * np);
         memset(datas, 0, sizeof(uint32_t) * np);
-        return SCAPH_OK;  // caller knows the source; kept simple
+        return SCAPH_OK;
     }
     const uint32_t *h = e->d_hist + (size_t)(level - 1) * 2 * np;
     SCAPH_CUDA(cudaMemcpy(nodes, h, sizeof(uint32_t) * np, cudaMemcpyDeviceToHost));

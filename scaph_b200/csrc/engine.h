@@ -33,10 +33,4 @@ struct DeviceGraph {
     void release();
 };
 
-// Beamer's direction-optimizing rule (SC'12): leave top-down when the
-// frontier's out-edges exceed the unexplored edges / alpha; leave bottom-up
-// when the frontier is below V / beta and shrinking.
-int alpha_beta_next(int cur_dir, uint64_t nf, uint64_t prev_nf, uint64_t mf, uint64_t mu,
-                    uint64_t V, float alpha, float beta);
-
 }  // namespace scaph

@@ -10,6 +10,14 @@ namespace scaph {
 // chunks over out-edge graph g), dir 1 = pull (k_pull over in-edge graph g).
 cudaError_t run_level(int dir, int block, int grid, const GraphDev &g, const BfsDev &s, uint32_t vlo,
                       uint32_t vhi, cudaStream_t st);
+// Graph mode: the same level kernels reading the level from a BfsCtl.
+cudaError_t run_level_graph(int dir, int block, int grid, const GraphDev &g, const BfsGraphArgs &a, cudaStream_t st);
+// k_graph_init(BfsGraphArgs, u32* depth, u32* parent, u32 src, u32 unreached, const u32* dead, u32 nlevels_clear)
+const void *graph_init_kernel();
+// k_graph_start(BfsGraphArgs)
+const void *graph_start_kernel();
+// k_decide(BfsGraphArgs, DecideArgs, handle loop, handle push, handle pull)
+const void *decide_kernel();
 // Resident CTAs per SM of the level kernel for `dir` at `block` threads.
 int level_occupancy(int dir, int block);
 cudaError_t fill_u32(uint32_t *p, uint32_t value, unsigned long long n, int grid, cudaStream_t st);

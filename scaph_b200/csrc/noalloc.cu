@@ -14,7 +14,7 @@
 // Limits and rules:
 //  * at most SCAPH_NOALLOC_MAX_V vertices and SCAPH_NOALLOC_MAX_E edges;
 //    larger graphs are rejected with SCAPH_EINVAL before any GPU work;
-//  * the scratch array is about 1.2 MB and is held by every GPU that loads
+//  * the scratch array is about 1.3 MB and is held by every GPU that loads
 //    the library, until the process exits;
 //  * every call shares that one array and leaves its contents behind; each
 //    call clears what must start at zero, but calls whose GPU work overlaps
@@ -160,7 +160,7 @@ extern "C" int scaph_bfs_page_noalloc(const uint32_t *d_page, uint32_t nodenum, 
     s.giant = reinterpret_cast<GiantChunk *>(scr + kOffGiant);
     s.giant_cap = kGiantCap;
     s.V = V;
-    s.weighted_edges = 0;
+    s.nwords = nwords;
     s.hg = g;
 
     const int grid_fill = sms * 4;

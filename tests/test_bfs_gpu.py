@@ -35,11 +35,47 @@ def rmat16():
     return csr, S.PagedGraph.from_csr(csr)  # 10 Mi-word pages, like the reference default
 
 
+@pytest.mark.parametrize("use_graph", [0, 2], ids=["graph", "hostloop"])
 @pytest.mark.parametrize("direction", DIRS)
-def test_rmat16_max_degree_source(rmat16, direction):
+def test_rmat16_max_degree_source(rmat16, direction, use_graph):
     csr, g = rmat16
     src = int(np.argmax(csr.degree()))
-    check_run(csr, g, src, direction=direction)
+    _, st, tr = check_run(csr, g, src, direction=direction, use_graph=use_graph)
+    assert [t["direction"] for t in tr][0] == 0
+    if direction == S.DIR_PUSH:
+        assert st.pull_levels == 0
+    if direction == S.DIR_PULL:
+        assert st.push_levels == 1
+
+
+def test_graph_and_host_loop_take_the_same_decisions():
+    csr = S.Csr.rmat(15, 16, seed=G.SEED + 8)
+    g = S.PagedGraph.from_csr(csr, pagesize_words=1 << 15)
+    for src in G.sources(csr, 3, 8):
+        _, _, t1 = check_run(csr, g, src, use_graph=0)
+        _, _, t2 = check_run(csr, g, src, use_graph=2)
+        assert [(t["direction"], t["next"], t["edges_inspected"]) for t in t1] == \
+               [(t["direction"], t["next"], t["edges_inspected"]) for t in t2]
+
+
+def test_async_runs_back_to_back():
+    """Enqueued graph-mode runs (no host sync in between) give the oracle's depths."""
+    import torch
+
+    csr = S.Csr.rmat(14, 16, seed=G.SEED + 9)
+    g = S.PagedGraph.from_csr(csr, pagesize_words=1 << 14)
+    stream = torch.cuda.current_stream()
+    eng = S.Engine(g, stream=stream.cuda_stream)
+    srcs = G.sources(csr, 4, 9)
+    outs = [torch.empty(csr.V, dtype=torch.int32, device="cuda") for _ in srcs]
+    for s, o in zip(srcs, outs):
+        eng.bfs_async(s, o.data_ptr())
+    eng.sync()
+    for s, o in zip(srcs, outs):
+        assert np.array_equal(o.cpu().numpy().view(np.uint32), O.bfs(csr.idx, csr.ngh, s))
+    tr = eng.trace()  # trace of the last run, read back on demand
+    assert 1 + sum(t["next"] for t in tr) == int((O.bfs(csr.idx, csr.ngh, srcs[-1]) != S.UNREACHED).sum())
+    eng.close()
 
 
 def test_rmat16_reference_sentinel(rmat16):
@@ -65,14 +101,16 @@ def test_block_sizes(block):
         check_run(csr, g, src, block_size=block)
 
 
-def test_deep_path_and_cap():
+@pytest.mark.parametrize("use_graph", [0, 2], ids=["graph", "hostloop"])
+def test_deep_path_and_cap(use_graph):
     """A 300-vertex path: native depths go to 299; with the reference sentinel
     63 the reference semantics cap reachability at depth 62."""
     csr = G.path(300)
     g = S.PagedGraph.from_csr(csr, pagesize_words=256)
-    check_run(csr, g, 0, direction=S.DIR_PUSH)
-    check_run(csr, g, 150, direction=S.DIR_PULL)
-    d, _, _ = check_run(csr, g, 0, unreached=S.REF_UNREACHED)
+    _, st, _ = check_run(csr, g, 0, direction=S.DIR_PUSH, use_graph=use_graph)
+    assert st.levels == 300
+    check_run(csr, g, 150, direction=S.DIR_PULL, use_graph=use_graph)
+    d, _, _ = check_run(csr, g, 0, unreached=S.REF_UNREACHED, use_graph=use_graph)
     assert d.max() == 63 and (d == 62).sum() == 1
 
 
@@ -112,13 +150,14 @@ def test_web_graph():
         check_run(csr, g, src, gt=gt)
 
 
-def test_trace_and_page_histogram():
+@pytest.mark.parametrize("use_graph", [0, 2], ids=["graph", "hostloop"])
+def test_trace_and_page_histogram(use_graph):
     """Per-level trace adds up, and the fused per-page frontier histogram equals
     get_page_info's (src/gpu_engine.cuh:397-441) restated in the oracle."""
     csr = S.Csr.rmat(14, 16, seed=G.SEED + 6)
     g = S.PagedGraph.from_csr(csr, pagesize_words=1 << 14)
     src = G.sources(csr, 1, 6)[0]
-    eng = S.Engine(g)
+    eng = S.Engine(g, use_graph=use_graph)
     depth, _, st = eng.bfs(src)
     tr = eng.trace()
     assert len(tr) == st.levels
