@@ -232,6 +232,21 @@ int scaph_bfs_trace(scaph_engine *e, scaph_level_trace *out, int cap);
 int scaph_bfs_page_hist(scaph_engine *e, int level, uint32_t *nodes,
                         uint32_t *datas, int npages);
 
+/* ---- multi-source BFS ---------------------------------------------------- */
+
+/* No counterpart in the reference (it runs one source per App::run,
+ * src/app.cuh:220-265).  Up to SCAPH_MSBFS_MAX sources share one traversal:
+ * per-vertex 64-bit (or 2x64-bit) source masks, the same direction rule,
+ * depths bit-exact with nsrc separate scaph_bfs runs.
+ * depths: u32[nsrc][V] (row i = source srcs[i]; unreached = cfg.unreached),
+ * host or device memory per out_on_device. */
+#define SCAPH_MSBFS_MAX 128
+int scaph_msbfs(scaph_engine *e, const uint32_t *srcs, int nsrc, uint32_t *depths,
+                int out_on_device, scaph_bfs_stats *stats);
+/* Per-level trace of the last scaph_msbfs (frontier = vertices with a
+ * nonzero mask; next = vertices newly reached by any source). */
+int scaph_msbfs_trace(scaph_engine *e, scaph_level_trace *out, int cap);
+
 /* ---- BFS without device allocation -------------------------------------- */
 
 /* No counterpart in the reference.  For callers that must not have the

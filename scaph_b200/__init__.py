@@ -100,6 +100,8 @@ def lib() -> C.CDLL:
         "scaph_bfs": ([vp, u32, vp, vp, i32, P(_Stats)], i32),
         "scaph_bfs_trace": ([vp, P(_Trace), i32], i32),
         "scaph_engine_sync": ([vp], i32),
+        "scaph_msbfs": ([vp, vp, i32, vp, i32, P(_Stats)], i32),
+        "scaph_msbfs_trace": ([vp, P(_Trace), i32], i32),
         "scaph_bfs_page_hist": ([vp, i32, vp, vp, i32], i32),
         "scaph_host_alloc": ([C.c_size_t], vp),
         "scaph_host_free": ([vp], None),
@@ -337,6 +339,26 @@ class Engine:
         """Enqueues one BFS writing into device buffers; returns at once."""
         _check(lib().scaph_bfs(self._h, src, C.c_void_p(depth_ptr), C.c_void_p(parent_ptr) if parent_ptr else None,
                                1, None))
+
+    def msbfs(self, srcs, depth_out: np.ndarray | None = None):
+        """Multi-source BFS (up to 128 sources in one traversal); returns
+        (depth[nsrc][V] as host array, BfsStats)."""
+        srcs = np.ascontiguousarray(srcs, np.uint32)
+        d = depth_out if depth_out is not None else np.empty((len(srcs), self.V), np.uint32)
+        st = _Stats()
+        _check(lib().scaph_msbfs(self._h, _ptr(srcs), len(srcs), _ptr(d), 0, C.byref(st)))
+        return d, _stats(st)
+
+    def msbfs_device(self, srcs, depth_ptr: int) -> BfsStats:
+        srcs = np.ascontiguousarray(srcs, np.uint32)
+        st = _Stats()
+        _check(lib().scaph_msbfs(self._h, _ptr(srcs), len(srcs), C.c_void_p(depth_ptr), 1, C.byref(st)))
+        return _stats(st)
+
+    def msbfs_trace(self) -> list[dict]:
+        buf = (_Trace * 4096)()
+        n = _check(lib().scaph_msbfs_trace(self._h, buf, 4096))
+        return [{f: getattr(buf[i], f) for f, _ in _Trace._fields_} for i in range(n)]
 
     def sync(self) -> None:
         _check(lib().scaph_engine_sync(self._h))

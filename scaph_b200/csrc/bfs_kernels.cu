@@ -186,18 +186,30 @@ __device__ __forceinline__ bool claim(const BfsDev &s, uint32_t u, uint32_t src)
     return true;
 }
 
-__device__ __forceinline__ void visit(LevelSmem &sm, const BfsDev &s, ThreadAcc &t, uint32_t u, uint32_t src,
-                                      bool hist_same, const PageLut &lut)
+// Visits up to four neighbours of `src` (in[j] marks the valid ones): the
+// four visited words are read first, all at once, and only neighbours whose
+// bit is still clear go on to the atomic claim.
+__device__ __forceinline__ void visit4(LevelSmem &sm, const BfsDev &s, ThreadAcc &t, const uint32_t (&u)[4],
+                                       const bool (&in)[4], uint32_t src, bool hist_same, const PageLut &lut)
 {
-    if (u >= s.V) {
-        atomicOr(&s.ctr->error, 1u);
-        return;
+    uint32_t vw[4];
+#pragma unroll
+    for (int j = 0; j < 4; j++)
+        vw[j] = (in[j] && u[j] < s.V) ? *((volatile const uint32_t *)&s.visited[u[j] >> 5]) : 0xFFFFFFFFu;
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+        if (!in[j]) continue;
+        if (u[j] >= s.V) {
+            atomicOr(&s.ctr->error, 1u);
+            continue;
+        }
+        if ((vw[j] >> (u[j] & 31)) & 1u) continue;
+        if (!claim(s, u[j], src)) continue;
+        t.next++;
+        const uint32_t du = __ldg(&s.degree[u[j]]);
+        t.next_edges += du;
+        if (s.page_nodes) hist_add(sm, s, hist_same ? lut.of(u[j]) : page_of(s.hg, u[j]), du + 3);
     }
-    if (!claim(s, u, src)) return;
-    t.next++;
-    const uint32_t du = __ldg(&s.degree[u]);
-    t.next_edges += du;
-    if (s.page_nodes) hist_add(sm, s, hist_same ? lut.of(u) : page_of(s.hg, u), du + 3);
 }
 
 // ---------------------------------------------------------------------------
@@ -290,11 +302,10 @@ __device__ __forceinline__ void push_body(const GraphDev &g, const BfsDev &s, ui
                 const uint4 val = ld_nc_v4(g.pool + quad * 4);
                 const uint32_t src = q[c0 + lo];
                 const uint32_t vals[4] = {val.x, val.y, val.z, val.w};
+                bool in[4];
 #pragma unroll
-                for (int j = 0; j < 4; j++) {
-                    const unsigned long long word = quad * 4 + j;
-                    if (word >= st && word < en) visit(sm, s, t, vals[j], src, hist_same, lut);
-                }
+                for (int j = 0; j < 4; j++) in[j] = quad * 4 + j >= st && quad * 4 + j < en;
+                visit4(sm, s, t, vals, in, src, hist_same, lut);
             }
             __syncthreads();
         }
@@ -323,11 +334,10 @@ __device__ __forceinline__ void giant_body(const GraphDev &g, const BfsDev &s)
         for (unsigned long long qd = q0 + threadIdx.x; qd < q1; qd += BLOCK) {
             const uint4 val = ld_nc_v4(g.pool + qd * 4);
             const uint32_t vals[4] = {val.x, val.y, val.z, val.w};
+            bool in[4];
 #pragma unroll
-            for (int j = 0; j < 4; j++) {
-                const unsigned long long word = qd * 4 + j;
-                if (word >= st && word < en) visit(sm, s, t, vals[j], gc.src, true, lut);
-            }
+            for (int j = 0; j < 4; j++) in[j] = qd * 4 + j >= st && qd * 4 + j < en;
+            visit4(sm, s, t, vals, in, gc.src, true, lut);
         }
     }
     level_epilogue<BLOCK>(sm, s, t);

@@ -94,62 +94,6 @@ void DeviceGraph::release()
 
 }  // namespace scaph
 
-struct scaph_engine {
-    scaph_config cfg{};
-    int device = 0;
-    int num_sms = 148;
-    cudaStream_t st = nullptr;
-    bool own_stream = false;
-    const Graph *g = nullptr;
-    const Graph *gt = nullptr;
-    DeviceGraph dout, din;
-    bool symmetric = true;
-    uint32_t V = 0, nwords = 0;
-    uint64_t E = 0;
-    uint32_t unreached = 0xFFFFFFFFu;
-    int block = 256, grid_push = 0, grid_pull = 0;
-
-    uint32_t *d_depth = nullptr, *d_parent = nullptr, *d_visited = nullptr, *d_bm3 = nullptr;
-    uint32_t *d_degree = nullptr, *d_dead = nullptr;
-    uint64_t n_dead = 0, dead_edges = 0;
-    LevelCounters *d_ctr = nullptr, *h_ctr = nullptr;
-    uint32_t *d_hist = nullptr;  // [kHistLevels][2][npages]
-    GiantChunk *d_giant = nullptr;
-    uint32_t giant_cap = 0;
-    BfsCtl *d_ctl = nullptr, *h_ctl = nullptr;
-    cudaEvent_t ev_start = nullptr, ev_stop = nullptr;
-    std::vector<cudaEvent_t> ev_level;
-
-    // graph mode
-    cudaGraph_t graph = nullptr;
-    cudaGraphExec_t gexec = nullptr;
-    cudaGraphNode_t n_init = nullptr;
-    cudaStream_t cap_st = nullptr;
-    BfsGraphArgs gargs{};
-    DecideArgs dargs{};
-
-    // last run
-    std::vector<scaph_level_trace> trace;
-    int last_levels = 0;
-    bool pending = false;  // a graph-mode run whose trace has not been read back
-    uint32_t pending_src = 0;
-    bool pending_parent = false;
-    scaph_bfs_stats last_stats{};
-
-    static constexpr int kHistLevels = 256;
-
-    const GraphDev &gin() const { return symmetric ? dout.view : din.view; }
-    bool graph_mode() const { return cfg.use_graph != 2; }
-    int create(const Graph *g_, const Graph *gt_, const scaph_config *c);
-    void destroy();
-    int bfs(uint32_t src, uint32_t *depths, uint32_t *parents, int out_on_device, scaph_bfs_stats *stats);
-    int run_host_loop(uint32_t src, uint32_t *dd, uint32_t *dp);
-    int build_graph();
-    int launch_graph(uint32_t src, uint32_t *dd, uint32_t *dp);
-    int collect(bool from_graph);
-    BfsDev base_state(uint32_t *dd, uint32_t *dp) const;
-};
-
 BfsDev scaph_engine::base_state(uint32_t *dd, uint32_t *dp) const
 {
     BfsDev s{};
@@ -247,6 +191,8 @@ int scaph_engine::create(const Graph *g_, const Graph *gt_, const scaph_config *
 void scaph_engine::destroy()
 {
     if (st) cudaStreamSynchronize(st);
+    ms_release(ms);
+    ms = nullptr;
     if (gexec) cudaGraphExecDestroy(gexec);
     if (graph) cudaGraphDestroy(graph);
     if (cap_st) cudaStreamDestroy(cap_st);

@@ -7,6 +7,7 @@
 
 #include "common.h"
 #include "device.cuh"
+#include "scaph/scaph.h"
 
 namespace scaph {
 
@@ -33,4 +34,77 @@ struct DeviceGraph {
     void release();
 };
 
+struct MsState;  // multi-source BFS state (msbfs.cu)
+void ms_release(MsState *m);
+
 }  // namespace scaph
+
+// The engine behind the opaque C-ABI handle.
+struct scaph_engine {
+    using DeviceGraph = scaph::DeviceGraph;
+    using Graph = scaph::Graph;
+    using LevelCounters = scaph::LevelCounters;
+    using GiantChunk = scaph::GiantChunk;
+    using BfsCtl = scaph::BfsCtl;
+    using BfsGraphArgs = scaph::BfsGraphArgs;
+    using DecideArgs = scaph::DecideArgs;
+    using BfsDev = scaph::BfsDev;
+    using GraphDev = scaph::GraphDev;
+
+    scaph_config cfg{};
+    int device = 0;
+    int num_sms = 148;
+    cudaStream_t st = nullptr;
+    bool own_stream = false;
+    const Graph *g = nullptr;
+    const Graph *gt = nullptr;
+    DeviceGraph dout, din;
+    bool symmetric = true;
+    uint32_t V = 0, nwords = 0;
+    uint64_t E = 0;
+    uint32_t unreached = 0xFFFFFFFFu;
+    int block = 256, grid_push = 0, grid_pull = 0;
+
+    uint32_t *d_depth = nullptr, *d_parent = nullptr, *d_visited = nullptr, *d_bm3 = nullptr;
+    uint32_t *d_degree = nullptr, *d_dead = nullptr;
+    uint64_t n_dead = 0, dead_edges = 0;
+    LevelCounters *d_ctr = nullptr, *h_ctr = nullptr;
+    uint32_t *d_hist = nullptr;  // [kHistLevels][2][npages]
+    GiantChunk *d_giant = nullptr;
+    uint32_t giant_cap = 0;
+    BfsCtl *d_ctl = nullptr, *h_ctl = nullptr;
+    cudaEvent_t ev_start = nullptr, ev_stop = nullptr;
+    std::vector<cudaEvent_t> ev_level;
+
+    // graph mode
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t gexec = nullptr;
+    cudaGraphNode_t n_init = nullptr;
+    cudaStream_t cap_st = nullptr;
+    BfsGraphArgs gargs{};
+    DecideArgs dargs{};
+
+    // last run
+    std::vector<scaph_level_trace> trace;
+    int last_levels = 0;
+    bool pending = false;  // a graph-mode run whose trace has not been read back
+    uint32_t pending_src = 0;
+    bool pending_parent = false;
+    scaph_bfs_stats last_stats{};
+
+    scaph::MsState *ms = nullptr;  // allocated by the first scaph_msbfs call
+
+    static constexpr int kHistLevels = 256;
+
+    const GraphDev &gin() const { return symmetric ? dout.view : din.view; }
+    bool graph_mode() const { return cfg.use_graph != 2; }
+    int create(const Graph *g_, const Graph *gt_, const scaph_config *c);
+    void destroy();
+    int bfs(uint32_t src, uint32_t *depths, uint32_t *parents, int out_on_device, scaph_bfs_stats *stats);
+    int run_host_loop(uint32_t src, uint32_t *dd, uint32_t *dp);
+    int build_graph();
+    int launch_graph(uint32_t src, uint32_t *dd, uint32_t *dp);
+    int collect(bool from_graph);
+    BfsDev base_state(uint32_t *dd, uint32_t *dp) const;
+};
+

@@ -1,0 +1,86 @@
+"""Multi-source BFS: every row of the batched result is bit-exact with the
+oracle's single-source BFS from that source."""
+import numpy as np
+import pytest
+
+import scaph_b200 as S
+from oracle import oracle as O
+from tests import graphs as G
+
+pytestmark = pytest.mark.gpu
+
+
+def check_batch(csr, eng, srcs, unreached=S.UNREACHED):
+    depth, st = eng.msbfs(srcs)
+    for i, s in enumerate(srcs):
+        ref = O.bfs(csr.idx, csr.ngh, int(s), unreached)
+        bad = np.flatnonzero(depth[i] != ref)
+        assert bad.size == 0, f"row {i} (src {s}): {bad.size} mismatches, v={bad[0]} gpu={depth[i][bad[0]]} " \
+                              f"cpu={ref[bad[0]]}"
+    return depth, st
+
+
+@pytest.mark.parametrize("direction", [S.DIR_ALPHABETA, S.DIR_PUSH, S.DIR_PULL])
+def test_msbfs_64_sources_rmat(direction):
+    csr = S.Csr.rmat(14, 16, seed=G.SEED + 20)
+    g = S.PagedGraph.from_csr(csr, pagesize_words=1 << 14)
+    eng = S.Engine(g, direction=direction)
+    check_batch(csr, eng, G.sources(csr, 64, 20))
+    eng.close()
+
+
+def test_msbfs_128_sources_two_words_and_repeat():
+    csr = S.Csr.rmat(13, 16, seed=G.SEED + 21)
+    g = S.PagedGraph.from_csr(csr, pagesize_words=1 << 13)
+    eng = S.Engine(g)
+    srcs = G.sources(csr, 120, 21) + [0, 0, 5, 5, 7, 9, 11, 13]  # duplicates and isolated ids too
+    check_batch(csr, eng, srcs)
+    # a second, smaller batch on the same engine reuses the state
+    check_batch(csr, eng, srcs[:3])
+    check_batch(csr, eng, srcs[:70])
+    eng.close()
+
+
+def test_msbfs_single_source_and_cap():
+    csr = G.path(200)
+    g = S.PagedGraph.from_csr(csr, pagesize_words=256)
+    eng = S.Engine(g)
+    check_batch(csr, eng, [0])
+    check_batch(csr, eng, [0, 199, 100])
+    eng.close()
+    eng = S.Engine(g, unreached=S.REF_UNREACHED)
+    d, _ = check_batch(csr, eng, [0, 199, 100], S.REF_UNREACHED)
+    assert d[0].max() == 63
+    eng.close()
+
+
+@pytest.mark.parametrize("direction", [S.DIR_ALPHABETA, S.DIR_PULL])
+def test_msbfs_directed_with_transpose(direction):
+    csr = S.Csr.powerlaw(20000, 250000, 1.9, 2000, seed=G.SEED + 22)
+    g = S.PagedGraph.from_csr(csr, pagesize_words=1 << 14)
+    gt = S.PagedGraph.from_csr(csr.transpose(), pagesize_words=1 << 14)
+    eng = S.Engine(g, gt, direction=direction)
+    check_batch(csr, eng, G.sources(csr, 64, 22))
+    eng.close()
+
+
+def test_msbfs_hub_giant_chunks():
+    csr = G.star(9000, center=5)
+    g = S.PagedGraph.from_csr(csr, pagesize_words=1 << 15)
+    eng = S.Engine(g, direction=S.DIR_PUSH)
+    check_batch(csr, eng, [5, 6, 7, 8000])
+    eng.close()
+
+
+def test_msbfs_matches_single_source_engine_and_trace():
+    csr = S.Csr.rmat(15, 16, seed=G.SEED + 23)
+    g = S.PagedGraph.from_csr(csr)
+    eng = S.Engine(g)
+    srcs = G.sources(csr, 32, 23)
+    d, st = eng.msbfs(srcs)
+    for i in (0, 13, 31):
+        single, _, _ = eng.bfs(srcs[i])
+        assert np.array_equal(single, d[i])
+    tr = eng.msbfs_trace()
+    assert len(tr) == st.levels and st.reached == int((d != S.UNREACHED).sum())
+    eng.close()
