@@ -206,6 +206,9 @@ typedef struct scaph_bfs_stats {
  * stats may be NULL. */
 int scaph_bfs(scaph_engine *e, uint32_t src, uint32_t *depths, uint32_t *parents,
               int out_on_device, scaph_bfs_stats *stats);
+/* Out-of-core engines (pool_bytes smaller than the graph's pages): drops
+ * every page from the HBM pool, so the next traversal starts cold. */
+int scaph_engine_evict_all(scaph_engine *e);
 /* With out_on_device != 0 and stats == NULL, scaph_bfs only enqueues the
  * traversal on the engine's stream and returns; scaph_engine_sync waits,
  * and scaph_bfs_trace / scaph_bfs_page_hist wait for the last run. */

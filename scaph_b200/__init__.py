@@ -100,6 +100,7 @@ def lib() -> C.CDLL:
         "scaph_bfs": ([vp, u32, vp, vp, i32, P(_Stats)], i32),
         "scaph_bfs_trace": ([vp, P(_Trace), i32], i32),
         "scaph_engine_sync": ([vp], i32),
+        "scaph_engine_evict_all": ([vp], i32),
         "scaph_msbfs": ([vp, vp, i32, vp, i32, P(_Stats)], i32),
         "scaph_msbfs_trace": ([vp, P(_Trace), i32], i32),
         "scaph_bfs_page_hist": ([vp, i32, vp, vp, i32], i32),
@@ -359,6 +360,10 @@ class Engine:
         buf = (_Trace * 4096)()
         n = _check(lib().scaph_msbfs_trace(self._h, buf, 4096))
         return [{f: getattr(buf[i], f) for f, _ in _Trace._fields_} for i in range(n)]
+
+    def evict_all(self) -> None:
+        """Out-of-core engines: start the next traversal with a cold page pool."""
+        _check(lib().scaph_engine_evict_all(self._h))
 
     def sync(self) -> None:
         _check(lib().scaph_engine_sync(self._h))

@@ -216,7 +216,8 @@ __device__ __forceinline__ void visit4(LevelSmem &sm, const BfsDev &s, ThreadAcc
 // bodies
 // ---------------------------------------------------------------------------
 template <int BLOCK>
-__device__ __forceinline__ void push_body(const GraphDev &g, const BfsDev &s, uint32_t vlo, uint32_t vhi)
+__device__ __forceinline__ void push_body(const GraphDev &g, const BfsDev &s, uint32_t vlo, uint32_t vhi,
+                                          const RangeList &rl)
 {
     __shared__ LevelSmem sm;
     __shared__ uint32_t q[kPushTileWords * 32];
@@ -231,13 +232,17 @@ __device__ __forceinline__ void push_body(const GraphDev &g, const BfsDev &s, ui
     __syncthreads();
 
     ThreadAcc t;
-    const uint32_t wlo = vlo >> 5, whi = (uint32_t)(((unsigned long long)vhi + 31) >> 5);
-    const uint32_t ntiles = (whi - wlo + kPushTileWords - 1) / kPushTileWords;
+    const uint32_t ntiles = rl.n ? rl.tile0[rl.n]
+                                 : (((uint32_t)(((unsigned long long)vhi + 31) >> 5)) - (vlo >> 5) + kPushTileWords - 1) /
+                                       kPushTileWords;
 
     for (uint32_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-        const uint32_t w = wlo + tile * kPushTileWords + threadIdx.x;
+        uint32_t rlo = vlo, rhi = vhi, local;
+        range_of_tile(rl, tile, rlo, rhi, local);
+        const uint32_t rwhi = (uint32_t)(((unsigned long long)rhi + 31) >> 5);
+        const uint32_t w = (rlo >> 5) + local * kPushTileWords + threadIdx.x;
         uint32_t f = 0;
-        if (threadIdx.x < kPushTileWords && w < whi) f = s.front[w] & range_mask(w, vlo, vhi);
+        if (threadIdx.x < kPushTileWords && w < rwhi) f = s.front[w] & range_mask(w, rlo, rhi);
         if (!__syncthreads_or(f != 0)) continue;
         uint32_t total;
         uint32_t off = block_exclusive_scan<BLOCK>(__popc(f), wsum, total);
@@ -344,7 +349,8 @@ __device__ __forceinline__ void giant_body(const GraphDev &g, const BfsDev &s)
 }
 
 template <int BLOCK>
-__device__ __forceinline__ void pull_body(const GraphDev &g, const BfsDev &s, uint32_t vlo, uint32_t vhi)
+__device__ __forceinline__ void pull_body(const GraphDev &g, const BfsDev &s, uint32_t vlo, uint32_t vhi,
+                                          const RangeList &rl)
 {
     // A CTA takes a tile of kPullTileWords visited-bitmap words, compacts the
     // tile's unvisited vertices into q, and runs them one per thread (phase
@@ -373,15 +379,20 @@ __device__ __forceinline__ void pull_body(const GraphDev &g, const BfsDev &s, ui
     __syncthreads();
 
     ThreadAcc t;
-    const uint32_t wlo = vlo >> 5, whi = (uint32_t)(((unsigned long long)vhi + 31) >> 5);
-    const uint32_t ntiles = (whi - wlo + kPullTileWords - 1) / kPullTileWords;
+    const uint32_t ntiles = rl.n ? rl.tile0[rl.n]
+                                 : (((uint32_t)(((unsigned long long)vhi + 31) >> 5)) - (vlo >> 5) + kPullTileWords - 1) /
+                                       kPullTileWords;
 
     for (uint32_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-        const uint32_t w = wlo + tile * kPullTileWords + threadIdx.x;
+        uint32_t rlo = vlo, rhi = vhi, local;
+        range_of_tile(rl, tile, rlo, rhi, local);
+        const uint32_t rwhi = (uint32_t)(((unsigned long long)rhi + 31) >> 5);
+        const uint32_t tbase = (rlo >> 5) + local * kPullTileWords;  // first word of the tile
+        const uint32_t w = tbase + threadIdx.x;
         uint32_t unv = 0;
         if (threadIdx.x < kPullTileWords) {
             fnd[threadIdx.x] = 0;
-            if (w < whi) unv = ~s.visited[w] & range_mask(w, vlo, vhi);
+            if (w < rwhi) unv = ~s.visited[w] & range_mask(w, rlo, rhi);
         }
         if (!__syncthreads_or(unv != 0)) continue;
         uint32_t total;
@@ -424,7 +435,7 @@ __device__ __forceinline__ void pull_body(const GraphDev &g, const BfsDev &s, ui
                         const uint32_t par = u[j];
                         s.depth[v] = s.level + 1;
                         if (s.parent) s.parent[v] = par;
-                        atomicOr(&fnd[(v >> 5) - (wlo + tile * kPullTileWords)], 1u << (v & 31));
+                        atomicOr(&fnd[(v >> 5) - tbase], 1u << (v & 31));
                         const uint32_t dv = __ldg(&s.degree[v]);
                         t.next++;
                         t.next_edges += dv;
@@ -499,7 +510,7 @@ __device__ __forceinline__ void pull_body(const GraphDev &g, const BfsDev &s, ui
                         const uint32_t vv = bq_v[e];
                         s.depth[vv] = s.level + 1;
                         if (s.parent) s.parent[vv] = hit_par;
-                        atomicOr(&fnd[(vv >> 5) - (wlo + tile * kPullTileWords)], 1u << (vv & 31));
+                        atomicOr(&fnd[(vv >> 5) - tbase], 1u << (vv & 31));
                         const uint32_t dv = __ldg(&s.degree[vv]);
                         t.next++;
                         t.next_edges += dv;
@@ -509,12 +520,13 @@ __device__ __forceinline__ void pull_body(const GraphDev &g, const BfsDev &s, ui
             }
             __syncthreads();
         }
-        // ---- the tile's visited / next words, written once
-        if (threadIdx.x < kPullTileWords && w < whi) {
+        // ---- the tile's visited / next words, written once (atomically:
+        // a word at a range boundary may belong to two tiles)
+        if (threadIdx.x < kPullTileWords && w < rwhi) {
             const uint32_t f = fnd[threadIdx.x];
             if (f) {
-                s.visited[w] |= f;
-                s.next[w] = f;
+                atomicOr(&s.visited[w], f);
+                atomicOr(&s.next[w], f);
             }
         }
         __syncthreads();
@@ -563,9 +575,9 @@ __device__ __forceinline__ unsigned long long globaltimer()
 // kernels: host-argument versions
 // ---------------------------------------------------------------------------
 template <int BLOCK>
-__global__ void __launch_bounds__(BLOCK) k_push(GraphDev g, BfsDev s, uint32_t vlo, uint32_t vhi)
+__global__ void __launch_bounds__(BLOCK) k_push(GraphDev g, BfsDev s, uint32_t vlo, uint32_t vhi, RangeList rl)
 {
-    push_body<BLOCK>(g, s, vlo, vhi);
+    push_body<BLOCK>(g, s, vlo, vhi, rl);
 }
 
 template <int BLOCK>
@@ -575,9 +587,10 @@ __global__ void __launch_bounds__(BLOCK) k_push_giant(GraphDev g, BfsDev s)
 }
 
 template <int BLOCK>
-__global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) k_pull(GraphDev g, BfsDev s, uint32_t vlo, uint32_t vhi)
+__global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) k_pull(GraphDev g, BfsDev s, uint32_t vlo, uint32_t vhi,
+                                                            RangeList rl)
 {
-    pull_body<BLOCK>(g, s, vlo, vhi);
+    pull_body<BLOCK>(g, s, vlo, vhi, rl);
 }
 
 // ---------------------------------------------------------------------------
@@ -588,7 +601,7 @@ __global__ void __launch_bounds__(BLOCK) k_push_g(GraphDev g, BfsGraphArgs a)
 {
     const BfsDev s = level_state(a);
     clear_third(a, s.level);
-    push_body<BLOCK>(g, s, 0, s.V);
+    push_body<BLOCK>(g, s, 0, s.V, RangeList{nullptr, nullptr, nullptr, 0});
 }
 
 template <int BLOCK>
@@ -602,7 +615,7 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) k_pull_g(GraphDev g, BfsG
 {
     const BfsDev s = level_state(a);
     clear_third(a, s.level);
-    pull_body<BLOCK>(g, s, 0, s.V);
+    pull_body<BLOCK>(g, s, 0, s.V, RangeList{nullptr, nullptr, nullptr, 0});
 }
 
 // First node of a BFS graph: run inputs into the control block, state reset
@@ -729,11 +742,41 @@ template <int BLOCK>
 static cudaError_t launch_level(int dir, int grid, const GraphDev &g, const BfsDev &s, uint32_t vlo, uint32_t vhi,
                                 cudaStream_t st)
 {
+    const RangeList one{nullptr, nullptr, nullptr, 0};
     if (dir == 0) {
-        k_push<BLOCK><<<grid, BLOCK, 0, st>>>(g, s, vlo, vhi);
+        k_push<BLOCK><<<grid, BLOCK, 0, st>>>(g, s, vlo, vhi, one);
         k_push_giant<BLOCK><<<grid, BLOCK, 0, st>>>(g, s);
     } else {
-        k_pull<BLOCK><<<grid, BLOCK, 0, st>>>(g, s, vlo, vhi);
+        k_pull<BLOCK><<<grid, BLOCK, 0, st>>>(g, s, vlo, vhi, one);
+    }
+    return cudaGetLastError();
+}
+
+template <int BLOCK>
+static cudaError_t launch_ranges(int dir, int grid, const GraphDev &g, const BfsDev &s, const RangeList &rl,
+                                 cudaStream_t st)
+{
+    if (dir == 0) k_push<BLOCK><<<grid, BLOCK, 0, st>>>(g, s, 0, 0, rl);
+    else k_pull<BLOCK><<<grid, BLOCK, 0, st>>>(g, s, 0, 0, rl);
+    return cudaGetLastError();
+}
+
+cudaError_t run_ranges(int dir, int block, int grid, const GraphDev &g, const BfsDev &s, const RangeList &rl,
+                       cudaStream_t st)
+{
+    switch (block) {
+    case 128: return launch_ranges<128>(dir, grid, g, s, rl, st);
+    case 512: return launch_ranges<512>(dir, grid, g, s, rl, st);
+    default: return launch_ranges<256>(dir, grid, g, s, rl, st);
+    }
+}
+
+cudaError_t run_giant(int block, int grid, const GraphDev &g, const BfsDev &s, cudaStream_t st)
+{
+    switch (block) {
+    case 128: k_push_giant<128><<<grid, 128, 0, st>>>(g, s); break;
+    case 512: k_push_giant<512><<<grid, 512, 0, st>>>(g, s); break;
+    default: k_push_giant<256><<<grid, 256, 0, st>>>(g, s); break;
     }
     return cudaGetLastError();
 }

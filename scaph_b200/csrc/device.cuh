@@ -150,6 +150,35 @@ __device__ __forceinline__ uint32_t test_bit(const uint32_t *bm, uint32_t v)
     return (__ldg(&bm[v >> 5]) >> (v & 31)) & 1u;
 }
 
+// Several vertex ranges processed by one launch (out-of-core page batches).
+// Tiles of 128 bitmap words are numbered across the ranges: range i owns
+// tiles [tile0[i], tile0[i+1]).  n == 0 means the single range (vlo, vhi)
+// passed to the kernel directly.
+struct RangeList {
+    const uint32_t *lo;
+    const uint32_t *hi;
+    const uint32_t *tile0;  // n + 1 entries
+    uint32_t n;
+};
+
+// Maps a global tile number to its range and local tile number.
+__device__ __forceinline__ void range_of_tile(const RangeList &rl, uint32_t tile, uint32_t &rlo, uint32_t &rhi,
+                                              uint32_t &local)
+{
+    if (rl.n == 0) {
+        local = tile;
+        return;  // rlo/rhi already hold the single range
+    }
+    uint32_t lo = 0, hi = rl.n - 1;
+    while (lo < hi) {
+        const uint32_t mid = (lo + hi + 1) >> 1;
+        if (rl.tile0[mid] <= tile) lo = mid; else hi = mid - 1;
+    }
+    rlo = rl.lo[lo];
+    rhi = rl.hi[lo];
+    local = tile - rl.tile0[lo];
+}
+
 // Mask of the vertices of word w that lie in [vlo, vhi).
 __device__ __forceinline__ uint32_t range_mask(uint32_t w, uint32_t vlo, uint32_t vhi)
 {

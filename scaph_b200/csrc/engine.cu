@@ -94,6 +94,14 @@ void DeviceGraph::release()
 
 }  // namespace scaph
 
+const GraphDev &scaph_engine::out_view() const { return pager ? pager_view(pager, 0) : dout.view; }
+
+const GraphDev &scaph_engine::gin() const
+{
+    if (pager) return pager_view(pager, symmetric ? 0 : 1);
+    return symmetric ? dout.view : din.view;
+}
+
 BfsDev scaph_engine::base_state(uint32_t *dd, uint32_t *dp) const
 {
     BfsDev s{};
@@ -105,7 +113,7 @@ BfsDev scaph_engine::base_state(uint32_t *dd, uint32_t *dp) const
     s.giant_cap = giant_cap;
     s.V = V;
     s.nwords = nwords;
-    s.hg = dout.view;
+    s.hg = out_view();
     return s;
 }
 
@@ -136,17 +144,22 @@ int scaph_engine::create(const Graph *g_, const Graph *gt_, const scaph_config *
         SCAPH_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
         own_stream = true;
     }
-    int nslots = 0;
-    if (cfg.pool_bytes > 0) {
-        const int64_t per = (int64_t)g->pagesize * 4;
-        nslots = (int)std::max<int64_t>(1, cfg.pool_bytes / per);
-        if (nslots < (int)g->pages.size() || (gt && nslots < (int)gt->pages.size()))
-            return set_error(SCAPH_EUNSUPPORTED, "pool of %d pages smaller than the graph: use the out-of-core engine",
-                             nslots);
+    int rc;
+    const size_t total_pages = g->pages.size() + (gt ? gt->pages.size() : 0);
+    const int64_t per = (int64_t)g->pagesize * 4;
+    const int nslots = cfg.pool_bytes > 0 ? (int)std::max<int64_t>(1, cfg.pool_bytes / per) : 0;
+    if (nslots > 0 && (size_t)nslots < total_pages) {
+        // out-of-core: pages stream through a pool of nslots page slots
+        if ((rc = pager_create(this, nslots, &pager))) return rc;
+    } else {
+        if ((rc = dout.build(*g, 0, st))) return rc;
+        if (gt && (rc = din.build(*gt, 0, st))) return rc;
     }
-    int rc = dout.build(*g, nslots, st);
-    if (rc) return rc;
-    if (gt && (rc = din.build(*gt, nslots, st))) return rc;
+    {
+        const std::vector<uint32_t> &indeg = gt ? gt->degree : g->degree;
+        SCAPH_CUDA(cudaMalloc(&d_indeg, (size_t)V * 4));
+        SCAPH_CUDA(cudaMemcpyAsync(d_indeg, indeg.data(), (size_t)V * 4, cudaMemcpyHostToDevice, st));
+    }
 
     // vertices no edge reaches (in-degree 0) are never discovered: they start
     // out "visited" so pull levels skip them
@@ -193,6 +206,9 @@ void scaph_engine::destroy()
     if (st) cudaStreamSynchronize(st);
     ms_release(ms);
     ms = nullptr;
+    pager_release(pager);
+    pager = nullptr;
+    cudaFree(d_indeg);
     if (gexec) cudaGraphExecDestroy(gexec);
     if (graph) cudaGraphDestroy(graph);
     if (cap_st) cudaStreamDestroy(cap_st);
@@ -230,6 +246,8 @@ int scaph_engine::run_host_loop(uint32_t src, uint32_t *dd, uint32_t *dp)
     BfsDev s = base_state(dd, dp);
     uint32_t *bm[2] = {d_bm3, d_bm3 + nwords};
     SCAPH_CUDA(set_source(s, src, bm[0], st));
+    level_h2d.clear();
+    if (pager) pager_reset_counters(pager);
 
     uint64_t nf = 1, prev_nf = 0, mf = g->degree[src];
     uint64_t vis_e = mf;
@@ -255,8 +273,19 @@ int scaph_engine::run_host_loop(uint32_t src, uint32_t *dd, uint32_t *dp)
         } else {
             s.page_nodes = s.page_datas = nullptr;
         }
-        const GraphDev &gv = dir == 0 ? dout.view : gin();
-        SCAPH_CUDA(run_level(dir, block, dir == 0 ? grid_push : grid_pull, gv, s, 0, V, st));
+        if (pager) {
+            std::vector<int> needed;
+            std::vector<uint32_t> datas;
+            int rc = pager_needs(this, pager, dir, level, src, needed, datas);
+            if (!rc) rc = pager_run_level(this, pager, dir, s, needed, datas);
+            if (rc) return rc;
+            uint64_t h2d, zc, f, pf, hits, lh;
+            pager_counters(pager, &h2d, &zc, &f, &pf, &hits, &lh);
+            level_h2d.push_back(lh);
+        } else {
+            const GraphDev &gv = dir == 0 ? dout.view : gin();
+            SCAPH_CUDA(run_level(dir, block, dir == 0 ? grid_push : grid_pull, gv, s, 0, V, st));
+        }
         SCAPH_CUDA(cudaEventRecord(ev_level[2 * level + 1], st));
         SCAPH_CUDA(cudaMemcpyAsync(h_ctr + level, d_ctr + level, sizeof(LevelCounters), cudaMemcpyDeviceToHost, st));
         SCAPH_CUDA(cudaStreamSynchronize(st));
@@ -438,6 +467,7 @@ int scaph_engine::collect(bool from_graph)
             cudaEventElapsedTime(&ms, ev_level[2 * l], ev_level[2 * l + 1]);
             t.ms = ms;
             launches += lc.dir == 0 ? 2 : 1;
+            if ((size_t)l < level_h2d.size()) t.h2d_bytes = level_h2d[l];
         }
         trace.push_back(t);
         alg += t.alg_bytes;
@@ -457,6 +487,14 @@ int scaph_engine::collect(bool from_graph)
     last_stats.edges_inspected = insp;
     last_stats.alg_bytes = alg;
     last_stats.launches = launches;
+    if (pager && !from_graph) {
+        uint64_t h2d, zc, f, pf, hits, lh;
+        pager_counters(pager, &h2d, &zc, &f, &pf, &hits, &lh);
+        last_stats.h2d_bytes = h2d;
+        last_stats.zc_bytes = zc;
+        last_stats.page_faults = f;
+        last_stats.prefetched = pf;
+    }
     pending = false;
     if (err) return set_error(SCAPH_EDEVICE, "level kernel reported error flags 0x%x", err);
     return SCAPH_OK;
@@ -525,6 +563,16 @@ int scaph_bfs(scaph_engine *e, uint32_t src, uint32_t *depths, uint32_t *parents
     clear_error();
     if (!e) return set_error(SCAPH_EINVAL, "null engine");
     return e->bfs(src, depths, parents, out_on_device, stats);
+}
+
+int scaph_engine_evict_all(scaph_engine *e)
+{
+    if (!e) return set_error(SCAPH_EINVAL, "null engine");
+    if (e->pager) {
+        SCAPH_CUDA(cudaStreamSynchronize(e->st));
+        pager_evict_all(e->pager);
+    }
+    return SCAPH_OK;
 }
 
 int scaph_engine_sync(scaph_engine *e)

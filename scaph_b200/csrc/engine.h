@@ -37,6 +37,25 @@ struct DeviceGraph {
 struct MsState;  // multi-source BFS state (msbfs.cu)
 void ms_release(MsState *m);
 
+struct Pager;  // out-of-core page manager (pager.cu)
+int coarse_index(const Graph &g, std::vector<uint32_t> &hc, uint32_t &cshift);
+
+}  // namespace scaph
+
+namespace scaph {
+int pager_create(scaph_engine *e, int nslots, Pager **out);
+void pager_release(Pager *p);
+const GraphDev &pager_view(const Pager *p, int gid);
+int pager_needs(scaph_engine *e, Pager *pg, int dir, int level, uint32_t src, std::vector<int> &needed,
+                std::vector<uint32_t> &datas);
+int pager_run_level(scaph_engine *e, Pager *pg, int dir, const BfsDev &s, const std::vector<int> &needed,
+                    const std::vector<uint32_t> &datas);
+int pager_prefetch(scaph_engine *e, Pager *pg, int gid, const std::vector<int> &pages);
+void pager_counters(const Pager *pg, uint64_t *h2d, uint64_t *zc, uint64_t *faults, uint64_t *prefetched,
+                    uint64_t *hits, uint64_t *level_h2d);
+void pager_reset_counters(Pager *pg);
+void pager_evict_all(Pager *pg);
+int pager_nslots(const Pager *pg);
 }  // namespace scaph
 
 // The engine behind the opaque C-ABI handle.
@@ -93,11 +112,16 @@ struct scaph_engine {
     scaph_bfs_stats last_stats{};
 
     scaph::MsState *ms = nullptr;  // allocated by the first scaph_msbfs call
+    scaph::Pager *pager = nullptr;  // out-of-core mode: pool smaller than the graph
+    uint32_t *d_indeg = nullptr;    // in-degree per vertex (pull page statistics)
+    std::vector<uint64_t> level_h2d;  // page bytes copied per level of the last run
+    scaph_bfs_stats pager_stats{};
 
     static constexpr int kHistLevels = 256;
 
-    const GraphDev &gin() const { return symmetric ? dout.view : din.view; }
-    bool graph_mode() const { return cfg.use_graph != 2; }
+    const GraphDev &out_view() const;
+    const GraphDev &gin() const;
+    bool graph_mode() const { return cfg.use_graph != 2 && !pager; }
     int create(const Graph *g_, const Graph *gt_, const scaph_config *c);
     void destroy();
     int bfs(uint32_t src, uint32_t *depths, uint32_t *parents, int out_on_device, scaph_bfs_stats *stats);

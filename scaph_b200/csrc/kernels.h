@@ -10,6 +10,11 @@ namespace scaph {
 // chunks over out-edge graph g), dir 1 = pull (k_pull over in-edge graph g).
 cudaError_t run_level(int dir, int block, int grid, const GraphDev &g, const BfsDev &s, uint32_t vlo,
                       uint32_t vhi, cudaStream_t st);
+// A push or pull pass over a list of vertex ranges (out-of-core page batches;
+// push only: the giant chunks they queue run in run_giant).
+cudaError_t run_ranges(int dir, int block, int grid, const GraphDev &g, const BfsDev &s, const RangeList &rl,
+                       cudaStream_t st);
+cudaError_t run_giant(int block, int grid, const GraphDev &g, const BfsDev &s, cudaStream_t st);
 // Graph mode: the same level kernels reading the level from a BfsCtl.
 cudaError_t run_level_graph(int dir, int block, int grid, const GraphDev &g, const BfsGraphArgs &a, cudaStream_t st);
 // k_graph_init(BfsGraphArgs, u32* depth, u32* parent, u32 src, u32 unreached, const u32* dead, u32 nlevels_clear)

@@ -848,6 +848,7 @@ extern "C" int scaph_msbfs(scaph_engine *e, const uint32_t *srcs, int nsrc, uint
     if (nsrc < 1 || nsrc > SCAPH_MSBFS_MAX) return set_error(SCAPH_EINVAL, "nsrc %d outside 1..%d", nsrc, SCAPH_MSBFS_MAX);
     for (int i = 0; i < nsrc; i++)
         if (srcs[i] >= e->V) return set_error(SCAPH_EINVAL, "source %u out of range (V=%u)", srcs[i], e->V);
+    if (e->pager) return set_error(SCAPH_EUNSUPPORTED, "multi-source BFS needs the graph resident");
     SCAPH_CUDA(cudaSetDevice(e->device));
     const int nw = nsrc > 64 ? 2 : 1;
     int rc = ms_alloc(e, nw);
