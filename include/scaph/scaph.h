@@ -168,6 +168,11 @@ typedef struct scaph_config {
                                   (one launch per level, per-level events)  */
     int32_t  device;           /* CUDA device ordinal                       */
     void    *stream;           /* cudaStream_t to run on; NULL = own stream */
+    int32_t  record_features;  /* host loop: keep the scheduler's feature
+                                  vector of every level (scaph_bfs_features) */
+    int32_t  dual_timing;      /* host loop, graph resident: run every level
+                                  both ways from the same state and record
+                                  both times (training labels)             */
 } scaph_config;
 
 typedef struct scaph_engine scaph_engine;
@@ -228,12 +233,56 @@ typedef struct scaph_level_trace {
     uint64_t alg_bytes;         /* algorithmic HBM bytes of this level      */
     uint64_t h2d_bytes;
     double   ms;                /* device time of this level's kernels      */
+    double   push_ms;           /* dual_timing: both directions' times      */
+    double   pull_ms;
 } scaph_level_trace;
 int scaph_bfs_trace(scaph_engine *e, scaph_level_trace *out, int cap);
 /* Active-vertex histogram of the frontier at `level` of the last run:
  * nodes[p] / datas[p] as get_page_info computes them (src/gpu_engine.cuh:397-441). */
 int scaph_bfs_page_hist(scaph_engine *e, int level, uint32_t *nodes,
                         uint32_t *datas, int npages);
+
+/* ---- learned scheduler ---------------------------------------------------- */
+
+/* No counterpart in the reference.  A 3-layer perceptron (in -> 64 -> 64 ->
+ * out, ReLU; BF16 weights, FP32 accumulation) trained on the GPU with the
+ * library's own forward / backward / Adam kernels (tensor-core GEMMs).
+ * For a scheduler: in = SCAPH_SCHED_GLOBALS + npages, out = 1 + npages
+ * (npages = pages of the out-edge graph); output 0 is the push(<0)/pull(>0)
+ * logit of the coming level, outputs 1.. the logits "page p holds frontier
+ * vertices at the level after". */
+#define SCAPH_SCHED_GLOBALS 16
+typedef struct scaph_mlp scaph_mlp;
+int scaph_mlp_create(int in_dim, int out_dim, uint64_t seed, int device, scaph_mlp **m);
+void scaph_mlp_destroy(scaph_mlp *m);
+size_t scaph_mlp_num_params(const scaph_mlp *m);
+/* parameters, in order W1[in][64] b1[64] W2[64][64] b2[64] W3[64][out] b3[out] */
+int scaph_mlp_get_params(const scaph_mlp *m, float *out, size_t n);
+int scaph_mlp_set_params(scaph_mlp *m, const float *in, size_t n);
+/* X: n rows of `in` floats (host); Y: n rows of `out` logits (host) */
+int scaph_mlp_forward(scaph_mlp *m, const float *X, int n, float *Y);
+/* sum over rows and outputs of W * BCE-with-logits(Y, T), and its gradient
+ * w.r.t. the parameters (grad may be NULL) */
+int scaph_mlp_loss_grad(scaph_mlp *m, const float *X, const float *T, const float *W, int n,
+                        float *loss, float *grad);
+int scaph_mlp_adam_step(scaph_mlp *m, const float *X, const float *T, const float *W, int n,
+                        float lr, float *loss);
+int scaph_mlp_train(scaph_mlp *m, const float *X, const float *T, const float *W, int n,
+                    int epochs, int batch, float lr, uint64_t seed, float *final_loss);
+int scaph_mlp_save(const scaph_mlp *m, const char *path);
+int scaph_mlp_load(scaph_mlp *m, const char *path);
+
+/* Makes SCAPH_DIR_LEARNED engines use `m` (NULL: back to alpha/beta): the
+ * network picks each level's direction and, out of core, pages whose
+ * logit exceeds 0 are prefetched while the level runs.  The engine keeps
+ * the pointer; it never changes depths. */
+int scaph_engine_set_scheduler(scaph_engine *e, scaph_mlp *m);
+/* Feature rows of the last host-loop run (record_features or learned mode):
+ * returns the row count, writes min(rows, cap) rows of *dim floats. */
+int scaph_bfs_features(scaph_engine *e, float *out, int cap, int *dim);
+/* Unvisited vertices per in-edge page at `level` of the last run
+ * (record_features): the pages a pull at that level would read. */
+int scaph_bfs_pull_pages(scaph_engine *e, int level, uint32_t *cnt, int npages);
 
 /* ---- multi-source BFS ---------------------------------------------------- */
 

@@ -46,7 +46,7 @@ class _Config(C.Structure):
                 ("alpha", C.c_float), ("beta", C.c_float), ("block_size", C.c_int32),
                 ("ctas_per_sm", C.c_int32), ("copy_streams", C.c_int32), ("prefetch", C.c_int32),
                 ("compact_threshold", C.c_int32), ("use_graph", C.c_int32), ("device", C.c_int32),
-                ("stream", C.c_void_p)]
+                ("stream", C.c_void_p), ("record_features", C.c_int32), ("dual_timing", C.c_int32)]
 
 
 class _Stats(C.Structure):
@@ -61,7 +61,7 @@ class _Trace(C.Structure):
     _fields_ = [("level", C.c_int32), ("direction", C.c_int32), ("frontier", C.c_uint64),
                 ("frontier_edges", C.c_uint64), ("unvisited", C.c_uint64), ("unvisited_edges", C.c_uint64),
                 ("next", C.c_uint64), ("edges_inspected", C.c_uint64), ("alg_bytes", C.c_uint64),
-                ("h2d_bytes", C.c_uint64), ("ms", C.c_double)]
+                ("h2d_bytes", C.c_uint64), ("ms", C.c_double), ("push_ms", C.c_double), ("pull_ms", C.c_double)]
 
 
 _lib = None
@@ -101,6 +101,20 @@ def lib() -> C.CDLL:
         "scaph_bfs_trace": ([vp, P(_Trace), i32], i32),
         "scaph_engine_sync": ([vp], i32),
         "scaph_engine_evict_all": ([vp], i32),
+        "scaph_mlp_create": ([i32, i32, u64, i32, P(vp)], i32),
+        "scaph_mlp_destroy": ([vp], None),
+        "scaph_mlp_num_params": ([vp], C.c_size_t),
+        "scaph_mlp_get_params": ([vp, vp, C.c_size_t], i32),
+        "scaph_mlp_set_params": ([vp, vp, C.c_size_t], i32),
+        "scaph_mlp_forward": ([vp, vp, i32, vp], i32),
+        "scaph_mlp_loss_grad": ([vp, vp, vp, vp, i32, P(C.c_float), vp], i32),
+        "scaph_mlp_adam_step": ([vp, vp, vp, vp, i32, C.c_float, P(C.c_float)], i32),
+        "scaph_mlp_train": ([vp, vp, vp, vp, i32, i32, i32, C.c_float, u64, P(C.c_float)], i32),
+        "scaph_mlp_save": ([vp, C.c_char_p], i32),
+        "scaph_mlp_load": ([vp, C.c_char_p], i32),
+        "scaph_engine_set_scheduler": ([vp, vp], i32),
+        "scaph_bfs_features": ([vp, vp, i32, P(i32)], i32),
+        "scaph_bfs_pull_pages": ([vp, i32, vp, i32], i32),
         "scaph_msbfs": ([vp, vp, i32, vp, i32, P(_Stats)], i32),
         "scaph_msbfs_trace": ([vp, P(_Trace), i32], i32),
         "scaph_bfs_page_hist": ([vp, i32, vp, vp, i32], i32),
@@ -270,6 +284,64 @@ class PagedGraph:
         return np.ctypeslib.as_array(lib().scaph_graph_degree(self._h), shape=(self.V,))
 
 
+class Mlp:
+    """The scheduler network (scaph_mlp_*): in -> 64 -> 64 -> out, BF16
+    weights, FP32 accumulation, trained with the library's GPU kernels."""
+
+    def __init__(self, in_dim: int, out_dim: int, seed: int = 1, device: int = 0):
+        h = C.c_void_p()
+        _check(lib().scaph_mlp_create(in_dim, out_dim, seed, device, C.byref(h)))
+        self._h, self.in_dim, self.out_dim = h, in_dim, out_dim
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            try:
+                lib().scaph_mlp_destroy(h)
+            except Exception:
+                pass
+            self._h = None
+
+    @property
+    def num_params(self) -> int:
+        return int(lib().scaph_mlp_num_params(self._h))
+
+    def params(self) -> np.ndarray:
+        out = np.zeros(self.num_params, np.float32)
+        _check(lib().scaph_mlp_get_params(self._h, _ptr(out), out.size))
+        return out
+
+    def set_params(self, p: np.ndarray) -> None:
+        p = np.ascontiguousarray(p, np.float32)
+        _check(lib().scaph_mlp_set_params(self._h, _ptr(p), p.size))
+
+    def forward(self, X: np.ndarray) -> np.ndarray:
+        X = np.ascontiguousarray(X, np.float32)
+        Y = np.zeros((X.shape[0], self.out_dim), np.float32)
+        _check(lib().scaph_mlp_forward(self._h, _ptr(X), X.shape[0], _ptr(Y)))
+        return Y
+
+    def loss_grad(self, X, T, W):
+        X, T, W = (np.ascontiguousarray(a, np.float32) for a in (X, T, W))
+        g = np.zeros(self.num_params, np.float32)
+        loss = C.c_float()
+        _check(lib().scaph_mlp_loss_grad(self._h, _ptr(X), _ptr(T), _ptr(W), X.shape[0], C.byref(loss), _ptr(g)))
+        return float(loss.value), g
+
+    def train(self, X, T, W, epochs: int = 50, batch: int = 256, lr: float = 1e-3, seed: int = 1) -> float:
+        X, T, W = (np.ascontiguousarray(a, np.float32) for a in (X, T, W))
+        loss = C.c_float()
+        _check(lib().scaph_mlp_train(self._h, _ptr(X), _ptr(T), _ptr(W), X.shape[0], epochs, batch, lr, seed,
+                                     C.byref(loss)))
+        return float(loss.value)
+
+    def save(self, path: str) -> None:
+        _check(lib().scaph_mlp_save(self._h, path.encode()))
+
+    def load(self, path: str) -> None:
+        _check(lib().scaph_mlp_load(self._h, path.encode()))
+
+
 @dataclass
 class BfsStats:
     levels: int
@@ -299,10 +371,10 @@ class Engine:
                  unreached: int = UNREACHED, direction: int = DIR_ALPHABETA, alpha: float = 14.0,
                  beta: float = 24.0, block_size: int = 256, ctas_per_sm: int = 0, copy_streams: int = 2,
                  prefetch: int = 0, compact_threshold: int = 3, use_graph: int = 0, device: int = 0,
-                 stream: int | None = None):
+                 stream: int | None = None, record_features: int = 0, dual_timing: int = 0):
         self.graph, self.transposed = graph, transposed
         cfg = _Config(pool_bytes, unreached, direction, alpha, beta, block_size, ctas_per_sm, copy_streams,
-                      prefetch, compact_threshold, use_graph, device, stream)
+                      prefetch, compact_threshold, use_graph, device, stream, record_features, dual_timing)
         self._cfg = cfg
         h = C.c_void_p()
         _check(lib().scaph_engine_create(graph._h, transposed._h if transposed else None, C.byref(cfg), C.byref(h)))
@@ -360,6 +432,24 @@ class Engine:
         buf = (_Trace * 4096)()
         n = _check(lib().scaph_msbfs_trace(self._h, buf, 4096))
         return [{f: getattr(buf[i], f) for f, _ in _Trace._fields_} for i in range(n)]
+
+    def set_scheduler(self, mlp: "Mlp | None") -> None:
+        _check(lib().scaph_engine_set_scheduler(self._h, mlp._h if mlp is not None else None))
+        self._sched = mlp  # keep the network alive while the engine uses it
+
+    def features(self) -> np.ndarray:
+        """Scheduler feature rows of the last host-loop run (levels x dim)."""
+        dim = C.c_int()
+        rows = _check(lib().scaph_bfs_features(self._h, None, 0, C.byref(dim)))
+        out = np.zeros((rows, dim.value), np.float32)
+        if rows:
+            lib().scaph_bfs_features(self._h, _ptr(out), rows, C.byref(dim))
+        return out
+
+    def pull_pages(self, level: int, npages_in: int) -> np.ndarray:
+        out = np.zeros(npages_in, np.uint32)
+        _check(lib().scaph_bfs_pull_pages(self._h, level, _ptr(out), npages_in))
+        return out
 
     def evict_all(self) -> None:
         """Out-of-core engines: start the next traversal with a cold page pool."""

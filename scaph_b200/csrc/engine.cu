@@ -19,6 +19,7 @@
 #include <cmath>
 #include <cstring>
 #include <memory>
+#include <utility>
 
 #include "engine.h"
 #include "kernels.h"
@@ -159,6 +160,9 @@ int scaph_engine::create(const Graph *g_, const Graph *gt_, const scaph_config *
         const std::vector<uint32_t> &indeg = gt ? gt->degree : g->degree;
         SCAPH_CUDA(cudaMalloc(&d_indeg, (size_t)V * 4));
         SCAPH_CUDA(cudaMemcpyAsync(d_indeg, indeg.data(), (size_t)V * 4, cudaMemcpyHostToDevice, st));
+        const size_t npi = (gt ? gt->pages.size() : g->pages.size()) + 1;
+        SCAPH_CUDA(cudaMalloc(&d_pcnt, npi * 4));
+        SCAPH_CUDA(cudaMalloc(&d_pdatas, npi * 4));
     }
 
     // vertices no edge reaches (in-degree 0) are never discovered: they start
@@ -191,6 +195,8 @@ int scaph_engine::create(const Graph *g_, const Graph *gt_, const scaph_config *
     SCAPH_CUDA(cudaMalloc(&d_giant, sizeof(GiantChunk) * (size_t)giant_cap));
     SCAPH_CUDA(cudaEventCreate(&ev_start));
     SCAPH_CUDA(cudaEventCreate(&ev_stop));
+    SCAPH_CUDA(cudaEventCreate(&ev_dual[0]));
+    SCAPH_CUDA(cudaEventCreate(&ev_dual[1]));
     ev_level.resize(2 * kMaxLevels);
     for (auto &e : ev_level) SCAPH_CUDA(cudaEventCreate(&e));
     int occ_push = std::max(1, level_occupancy(0, block));
@@ -209,6 +215,9 @@ void scaph_engine::destroy()
     pager_release(pager);
     pager = nullptr;
     cudaFree(d_indeg);
+    cudaFree(d_snap);
+    cudaFree(d_pcnt);
+    cudaFree(d_pdatas);
     if (gexec) cudaGraphExecDestroy(gexec);
     if (graph) cudaGraphDestroy(graph);
     if (cap_st) cudaStreamDestroy(cap_st);
@@ -228,8 +237,66 @@ void scaph_engine::destroy()
     cudaFree(d_giant);
     if (ev_start) cudaEventDestroy(ev_start);
     if (ev_stop) cudaEventDestroy(ev_stop);
+    for (auto &ev : ev_dual)
+        if (ev) cudaEventDestroy(ev);
     for (auto &e : ev_level) if (e) cudaEventDestroy(e);
     if (own_stream && st) cudaStreamDestroy(st);
+}
+
+// Scheduler features of the coming level (layout in scaph.h /
+// DESIGN.md): 16 globals, then the frontier's share of every out-edge page.
+int scaph_engine::features(int level, uint32_t src, uint64_t nf, uint64_t mf, uint64_t unvis, uint64_t mu,
+                           int prev_dir, int ab_dir, float *f, std::vector<uint32_t> &pull_cnt)
+{
+    const size_t np = g->pages.size();
+    const GraphDev &gi = gin();
+    const int npi = (int)gi.npages;
+    // frontier histogram over out-pages (level 0: the source alone)
+    std::vector<uint32_t> hist(np, 0);
+    if (level == 0) {
+        size_t p = 0;
+        while (p + 1 < np && g->pages[p + 1].left <= src) p++;
+        hist[p] = 1;
+    } else if (level - 1 < kHistLevels) {
+        SCAPH_CUDA(cudaMemcpyAsync(hist.data(), d_hist + (size_t)(level - 1) * 2 * np, np * 4, cudaMemcpyDeviceToHost, st));
+    }
+    // unvisited vertices per in-edge page
+    pull_cnt.assign(npi, 0);
+    SCAPH_CUDA(page_unvisited(gi, d_visited, d_indeg, d_pcnt, d_pdatas, num_sms * 4, st));
+    SCAPH_CUDA(cudaMemcpyAsync(pull_cnt.data(), d_pcnt, npi * 4, cudaMemcpyDeviceToHost, st));
+    SCAPH_CUDA(cudaStreamSynchronize(st));
+    auto lg = [](double x, double d) { return (float)(std::log2(1.0 + x) / d); };
+    f[0] = lg((double)nf, 32);
+    f[1] = lg((double)mf, 40);
+    f[2] = lg((double)unvis, 32);
+    f[3] = lg((double)mu, 40);
+    f[4] = (float)((double)nf / V);
+    f[5] = (float)std::min(1.0, (double)mf / std::max<uint64_t>(1, E));
+    f[6] = (float)((double)unvis / V);
+    f[7] = (float)std::min(1.0, (double)mu / std::max<uint64_t>(1, E));
+    f[8] = (float)level / 32.f;
+    f[9] = (float)prev_dir;
+    float res_out = 1.f, res_in = 1.f, res_push = 1.f, res_pull = 1.f;
+    if (pager) {
+        std::vector<int> push_pages, pull_pages;
+        for (size_t p = 0; p < np; p++)
+            if (hist[p]) push_pages.push_back((int)p);
+        for (int p = 0; p < npi; p++)
+            if (pull_cnt[p]) pull_pages.push_back(p);
+        const int gid_in = symmetric ? 0 : 1;
+        res_out = pager_resident_fraction(pager, 0, nullptr);
+        res_in = pager_resident_fraction(pager, gid_in, nullptr);
+        res_push = pager_resident_fraction(pager, 0, &push_pages);
+        res_pull = pager_resident_fraction(pager, gid_in, &pull_pages);
+    }
+    f[10] = res_out;
+    f[11] = res_in;
+    f[12] = res_push;
+    f[13] = res_pull;
+    f[14] = (float)ab_dir;
+    f[15] = 1.f;
+    for (size_t p = 0; p < np; p++) f[SCAPH_SCHED_GLOBALS + p] = (float)hist[p] / (float)std::max(1u, g->pages[p].nodenum);
+    return SCAPH_OK;
 }
 
 // Host-driven level loop (one launch + one counter read-back per level).
@@ -237,6 +304,9 @@ int scaph_engine::run_host_loop(uint32_t src, uint32_t *dd, uint32_t *dp)
 {
     const int fill_grid = num_sms * 4;
     const size_t np = g->pages.size();
+    const bool learned = cfg.direction == SCAPH_DIR_LEARNED && sched;
+    const bool want_feat = learned || cfg.record_features;
+    const bool dual = cfg.dual_timing && !pager;
     SCAPH_CUDA(fill_u32(dd, unreached, V, fill_grid, st));
     if (dp) SCAPH_CUDA(fill_u32(dp, kNoParent, V, fill_grid, st));
     SCAPH_CUDA(cudaMemcpyAsync(d_visited, d_dead, (size_t)nwords * 4, cudaMemcpyDeviceToDevice, st));
@@ -247,22 +317,47 @@ int scaph_engine::run_host_loop(uint32_t src, uint32_t *dd, uint32_t *dp)
     uint32_t *bm[2] = {d_bm3, d_bm3 + nwords};
     SCAPH_CUDA(set_source(s, src, bm[0], st));
     level_h2d.clear();
+    dual_ms.clear();
+    feat_log.clear();
+    pull_log.clear();
+    feat_dim = SCAPH_SCHED_GLOBALS + (int)np;
     if (pager) pager_reset_counters(pager);
+    if (dual && !d_snap) SCAPH_CUDA(cudaMalloc(&d_snap, (size_t)nwords * 4));
+    const bool src_dead = (gt ? gt->degree[src] : g->degree[src]) == 0;
 
     uint64_t nf = 1, prev_nf = 0, mf = g->degree[src];
-    uint64_t vis_e = mf;
+    uint64_t vis_n = 1, vis_e = mf;
     int dir = 0, cur = 0, level = 0;
+    std::vector<float> f(feat_dim), y;
     while (nf > 0 && level < kMaxLevels && (uint64_t)level + 1 < unreached) {
         const uint64_t used = vis_e + dead_edges;
         const uint64_t mu = E > used ? E - used : 0;
+        const int ab = level == 0 ? 0 : alpha_beta_next(dir, nf, prev_nf, mf, mu, V, cfg.alpha, cfg.beta);
+        const int prev_dir = dir;
         switch (cfg.direction) {
         case SCAPH_DIR_PUSH: dir = 0; break;
         case SCAPH_DIR_PULL: dir = level == 0 ? 0 : 1; break;
-        default: dir = level == 0 ? 0 : alpha_beta_next(dir, nf, prev_nf, mf, mu, V, cfg.alpha, cfg.beta); break;
+        default: dir = ab; break;
+        }
+        std::vector<int> prefetch_pages;
+        if (want_feat) {
+            std::vector<uint32_t> pc;
+            const uint64_t unvis = (uint64_t)V - n_dead - vis_n + (src_dead ? 1 : 0);
+            int rc = features(level, src, nf, mf, unvis, mu, prev_dir, ab, f.data(), pc);
+            if (rc) return rc;
+            feat_log.insert(feat_log.end(), f.begin(), f.end());
+            pull_log.push_back(std::move(pc));
+            if (learned) {
+                int in = 0, out = 0;
+                mlp_dims(sched, &in, &out);
+                y.resize(out);
+                if ((rc = mlp_forward_device(sched, f.data(), 1, y.data()))) return rc;
+                if (level > 0) dir = y[0] > 0.f ? 1 : 0;
+                for (int p = 0; p + 1 < out && p < (int)np; p++)
+                    if (y[1 + p] > 0.f) prefetch_pages.push_back(p);
+            }
         }
         uint32_t *next = bm[cur ^ 1];
-        SCAPH_CUDA(cudaEventRecord(ev_level[2 * level], st));
-        SCAPH_CUDA(cudaMemsetAsync(next, 0, (size_t)nwords * 4, st));
         s.front = bm[cur];
         s.next = next;
         s.ctr = d_ctr + level;
@@ -273,22 +368,50 @@ int scaph_engine::run_host_loop(uint32_t src, uint32_t *dd, uint32_t *dp)
         } else {
             s.page_nodes = s.page_datas = nullptr;
         }
+        double dual_push = 0, dual_pull = 0;
+        if (dual && level > 0) {
+            // both directions from the same state: push first, then the
+            // state is restored and pull runs (both discover the same set)
+            SCAPH_CUDA(cudaMemcpyAsync(d_snap, d_visited, (size_t)nwords * 4, cudaMemcpyDeviceToDevice, st));
+            SCAPH_CUDA(cudaMemsetAsync(next, 0, (size_t)nwords * 4, st));
+            SCAPH_CUDA(cudaEventRecord(ev_dual[0], st));
+            SCAPH_CUDA(run_level(0, block, grid_push, dout.view, s, 0, V, st));
+            SCAPH_CUDA(cudaEventRecord(ev_dual[1], st));
+            SCAPH_CUDA(cudaEventSynchronize(ev_dual[1]));
+            float ms = 0;
+            cudaEventElapsedTime(&ms, ev_dual[0], ev_dual[1]);
+            dual_push = ms;
+            SCAPH_CUDA(cudaMemcpyAsync(d_visited, d_snap, (size_t)nwords * 4, cudaMemcpyDeviceToDevice, st));
+            SCAPH_CUDA(cudaMemsetAsync(d_ctr + level, 0, sizeof(LevelCounters), st));
+            if (s.page_nodes) SCAPH_CUDA(cudaMemsetAsync(s.page_nodes, 0, sizeof(uint32_t) * 2 * np, st));
+        }
+        SCAPH_CUDA(cudaEventRecord(ev_level[2 * level], st));
+        SCAPH_CUDA(cudaMemsetAsync(next, 0, (size_t)nwords * 4, st));
+        const int run_dir = (dual && level > 0) ? 1 : dir;
         if (pager) {
             std::vector<int> needed;
             std::vector<uint32_t> datas;
-            int rc = pager_needs(this, pager, dir, level, src, needed, datas);
-            if (!rc) rc = pager_run_level(this, pager, dir, s, needed, datas);
+            int rc = pager_needs(this, pager, run_dir, level, src, needed, datas);
+            if (!rc) rc = pager_run_level(this, pager, run_dir, s, needed, datas);
+            if (!rc && !prefetch_pages.empty() && run_dir == 0) rc = pager_prefetch(this, pager, 0, prefetch_pages);
             if (rc) return rc;
-            uint64_t h2d, zc, f, pf, hits, lh;
-            pager_counters(pager, &h2d, &zc, &f, &pf, &hits, &lh);
+            uint64_t h2d, zc, ff, pf, hits, lh;
+            pager_counters(pager, &h2d, &zc, &ff, &pf, &hits, &lh);
             level_h2d.push_back(lh);
         } else {
-            const GraphDev &gv = dir == 0 ? dout.view : gin();
-            SCAPH_CUDA(run_level(dir, block, dir == 0 ? grid_push : grid_pull, gv, s, 0, V, st));
+            const GraphDev &gv = run_dir == 0 ? dout.view : gin();
+            SCAPH_CUDA(run_level(run_dir, block, run_dir == 0 ? grid_push : grid_pull, gv, s, 0, V, st));
         }
         SCAPH_CUDA(cudaEventRecord(ev_level[2 * level + 1], st));
         SCAPH_CUDA(cudaMemcpyAsync(h_ctr + level, d_ctr + level, sizeof(LevelCounters), cudaMemcpyDeviceToHost, st));
         SCAPH_CUDA(cudaStreamSynchronize(st));
+        if (dual) {
+            float ms = 0;
+            cudaEventElapsedTime(&ms, ev_level[2 * level], ev_level[2 * level + 1]);
+            dual_pull = level > 0 ? ms : 0;
+            if (level == 0) dual_push = ms;
+            dual_ms.push_back({dual_push, dual_pull});
+        }
         h_ctr[level].dir = dir;
         if (h_ctr[level].error) {
             level++;
@@ -297,6 +420,7 @@ int scaph_engine::run_host_loop(uint32_t src, uint32_t *dd, uint32_t *dp)
         prev_nf = nf;
         nf = h_ctr[level].next;
         mf = h_ctr[level].next_edges;
+        vis_n += nf;
         vis_e += mf;
         cur ^= 1;
         level++;
@@ -468,6 +592,10 @@ int scaph_engine::collect(bool from_graph)
             t.ms = ms;
             launches += lc.dir == 0 ? 2 : 1;
             if ((size_t)l < level_h2d.size()) t.h2d_bytes = level_h2d[l];
+            if ((size_t)l < dual_ms.size()) {
+                t.push_ms = dual_ms[l].first;
+                t.pull_ms = dual_ms[l].second;
+            }
         }
         trace.push_back(t);
         alg += t.alg_bytes;
@@ -563,6 +691,40 @@ int scaph_bfs(scaph_engine *e, uint32_t src, uint32_t *depths, uint32_t *parents
     clear_error();
     if (!e) return set_error(SCAPH_EINVAL, "null engine");
     return e->bfs(src, depths, parents, out_on_device, stats);
+}
+
+int scaph_engine_set_scheduler(scaph_engine *e, scaph_mlp *m)
+{
+    if (!e) return set_error(SCAPH_EINVAL, "null engine");
+    if (m) {
+        int in = 0, out = 0;
+        mlp_dims(m, &in, &out);
+        const int np = (int)e->g->pages.size();
+        if (in != SCAPH_SCHED_GLOBALS + np || out != 1 + np)
+            return set_error(SCAPH_EINVAL, "scheduler network must be %d -> %d for this graph (is %d -> %d)",
+                             SCAPH_SCHED_GLOBALS + np, 1 + np, in, out);
+    }
+    e->sched = m;
+    return SCAPH_OK;
+}
+
+int scaph_bfs_features(scaph_engine *e, float *out, int cap, int *dim)
+{
+    if (!e) return set_error(SCAPH_EINVAL, "null engine");
+    const int rows = e->feat_dim ? (int)(e->feat_log.size() / e->feat_dim) : 0;
+    if (dim) *dim = e->feat_dim;
+    if (out && cap > 0) memcpy(out, e->feat_log.data(), sizeof(float) * (size_t)std::min(cap, rows) * e->feat_dim);
+    return rows;
+}
+
+int scaph_bfs_pull_pages(scaph_engine *e, int level, uint32_t *cnt, int npages)
+{
+    if (!e || !cnt) return set_error(SCAPH_EINVAL, "null argument");
+    if (level < 0 || level >= (int)e->pull_log.size()) return set_error(SCAPH_EINVAL, "level %d not recorded", level);
+    const auto &v = e->pull_log[level];
+    if (npages < (int)v.size()) return set_error(SCAPH_EINVAL, "need %zu pages", v.size());
+    memcpy(cnt, v.data(), v.size() * 4);
+    return (int)v.size();
 }
 
 int scaph_engine_evict_all(scaph_engine *e)

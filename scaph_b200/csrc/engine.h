@@ -56,6 +56,11 @@ void pager_counters(const Pager *pg, uint64_t *h2d, uint64_t *zc, uint64_t *faul
 void pager_reset_counters(Pager *pg);
 void pager_evict_all(Pager *pg);
 int pager_nslots(const Pager *pg);
+float pager_resident_fraction(const Pager *pg, int gid, const std::vector<int> *pages);
+cudaError_t page_unvisited(const GraphDev &g, const uint32_t *visited, const uint32_t *indeg, uint32_t *cnt,
+                           uint32_t *datas, int grid, cudaStream_t st);
+int mlp_forward_device(scaph_mlp *m, const float *hX, int n, float *hY);
+int mlp_dims(const scaph_mlp *m, int *in, int *out);
 }  // namespace scaph
 
 // The engine behind the opaque C-ABI handle.
@@ -92,7 +97,7 @@ struct scaph_engine {
     GiantChunk *d_giant = nullptr;
     uint32_t giant_cap = 0;
     BfsCtl *d_ctl = nullptr, *h_ctl = nullptr;
-    cudaEvent_t ev_start = nullptr, ev_stop = nullptr;
+    cudaEvent_t ev_start = nullptr, ev_stop = nullptr, ev_dual[2] = {nullptr, nullptr};
     std::vector<cudaEvent_t> ev_level;
 
     // graph mode
@@ -116,6 +121,13 @@ struct scaph_engine {
     uint32_t *d_indeg = nullptr;    // in-degree per vertex (pull page statistics)
     std::vector<uint64_t> level_h2d;  // page bytes copied per level of the last run
     scaph_bfs_stats pager_stats{};
+    // learned scheduler / training traces
+    scaph_mlp *sched = nullptr;
+    std::vector<float> feat_log;                    // levels x feat_dim
+    int feat_dim = 0;
+    std::vector<std::vector<uint32_t>> pull_log;    // unvisited per in-page, per level
+    std::vector<std::pair<double, double>> dual_ms; // (push, pull) per level
+    uint32_t *d_snap = nullptr, *d_pcnt = nullptr, *d_pdatas = nullptr;
 
     static constexpr int kHistLevels = 256;
 
@@ -126,6 +138,8 @@ struct scaph_engine {
     void destroy();
     int bfs(uint32_t src, uint32_t *depths, uint32_t *parents, int out_on_device, scaph_bfs_stats *stats);
     int run_host_loop(uint32_t src, uint32_t *dd, uint32_t *dp);
+    int features(int level, uint32_t src, uint64_t nf, uint64_t mf, uint64_t unvis, uint64_t mu, int prev_dir,
+                 int ab_dir, float *f, std::vector<uint32_t> &pull_cnt);
     int build_graph();
     int launch_graph(uint32_t src, uint32_t *dd, uint32_t *dp);
     int collect(bool from_graph);

@@ -538,4 +538,26 @@ void pager_evict_all(Pager *pg) { pg->evict_all(); }
 
 int pager_nslots(const Pager *pg) { return pg->nslots; }
 
+float pager_resident_fraction(const Pager *pg, int gid, const std::vector<int> *pages)
+{
+    const Pager::GState &G = pg->gs[gid];
+    if (pages) {
+        if (pages->empty()) return 1.f;
+        int r = 0;
+        for (int p : *pages) r += G.slot_of[p] >= 0 ? 1 : 0;
+        return (float)r / (float)pages->size();
+    }
+    int r = 0;
+    for (int s : G.slot_of) r += s >= 0 ? 1 : 0;
+    return G.slot_of.empty() ? 1.f : (float)r / (float)G.slot_of.size();
+}
+
+cudaError_t page_unvisited(const GraphDev &g, const uint32_t *visited, const uint32_t *indeg, uint32_t *cnt,
+                           uint32_t *datas, int grid, cudaStream_t st)
+{
+    k_page_unvisited<<<std::max(1, std::min((int)g.npages, grid)), 256, 0, st>>>(visited, g.pages, g.npages, g.V,
+                                                                                indeg, cnt, datas);
+    return cudaGetLastError();
+}
+
 }  // namespace scaph

@@ -1,0 +1,56 @@
+"""The learned scheduler against the method without it (alpha/beta + demand
+paging), out of core, on held-out sources.  The page link is modelled slow
+(page_ms per page fetched) so that, as at full scale, page traffic and not
+kernel time dominates; the gain is measured in fetched pages and in that
+modelled time.  Depths must stay bit-exact either way."""
+import numpy as np
+import pytest
+
+import scaph_b200 as S
+from oracle import oracle as O
+from scaph_b200 import scheduler
+from tests import graphs as G
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def setup():
+    csr = S.Csr.powerlaw(60000, 900000, 1.9, 3000, seed=G.SEED + 60)
+    g = S.PagedGraph.from_csr(csr, pagesize_words=1 << 13)
+    gt = S.PagedGraph.from_csr(csr.transpose(), pagesize_words=1 << 13)
+    srcs = G.sources(csr, 24, 60)
+    return csr, g, gt, srcs[:16], srcs[16:]
+
+
+def test_traces_and_labels(setup):
+    csr, g, gt, train, _ = setup
+    tr = scheduler.collect(g, gt, train[:2])
+    for t in tr:
+        assert t.feats.shape[1] == scheduler.G + g.npages
+        assert np.all(t.push_ms[1:] > 0) and np.all(t.pull_ms[1:] > 0)
+        dirs, rows, best, ab = scheduler.label(t, 40, 0.5, g.V, g.npages, gt.npages, False)
+        assert best <= ab + 1e-9 and dirs[0] == 0 and rows.shape == t.feats.shape
+
+
+def test_learned_scheduler_beats_alpha_beta_out_of_core(setup):
+    csr, g, gt, train, held = setup
+    total = g.npages + gt.npages
+    nslots = int(0.5 * total)
+    pool = nslots * g.pagesize * 4
+    page_ms = 0.5
+    traces = scheduler.collect(g, gt, train)
+    net, info = scheduler.train(traces, g, gt, nslots, page_ms, epochs=300)
+    assert info["loss"] < info["loss0"] and info["direction_accuracy"] > 0.8, info
+    plain = scheduler.evaluate(g, gt, held, None, pool)
+    learned = scheduler.evaluate(g, gt, held, net, pool)
+    for s, a, b in zip(held, plain["depths"], learned["depths"]):
+        ref = O.bfs(csr.idx, csr.ngh, s)
+        assert np.array_equal(a, ref) and np.array_equal(b, ref)
+    cost_plain = plain["ms"] + plain["page_faults"] * page_ms
+    cost_learned = learned["ms"] + learned["page_faults"] * page_ms
+    print(f"\nalpha/beta: {plain['page_faults']} pages, modelled {cost_plain:.1f} ms; "
+          f"learned: {learned['page_faults']} pages (+{learned['prefetched']} prefetched), "
+          f"modelled {cost_learned:.1f} ms; training {info}")
+    assert learned["page_faults"] + learned["prefetched"] < plain["page_faults"]
+    assert cost_learned < cost_plain
