@@ -47,6 +47,9 @@ def parse_args():
     ap.add_argument("--sources", type=int, default=64)
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="bounded CPU-baseline sample")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the other configurations (rank 0, N=1 only anyway)")
+    ap.add_argument("--config5", action="store_true", help="also run the 105M-vertex web graph (slow to generate)")
     return ap.parse_args()
 
 
@@ -223,6 +226,142 @@ def cpu_baseline(csr, srcs, budget_s):
 
 
 # ---------------------------------------------------------------------------
+# the other configurations (reported beside the headline, rank 0, N = 1)
+# ---------------------------------------------------------------------------
+def extra_config1():
+    """RMAT-16, max-degree source, checked bit-exact against the oracle."""
+    import numpy as np
+
+    import scaph_b200 as S
+    from oracle import oracle as O
+    from scaph_b200 import workloads
+
+    csr, (src,) = workloads.config1()
+    g = workloads.paged(csr)
+    eng = S.Engine(g)
+    eng.bfs(src)
+    d, _, st = eng.bfs(src)
+    ok = bool(np.array_equal(d, O.bfs(csr.idx, csr.ngh, src)))
+    eng.close()
+    return {"graph": "RMAT-16 ef16", "V": csr.V, "E": csr.E, "source": src, "levels": st.levels,
+            "ms": st.ms, "gteps": csr.E / (st.ms / 1e3) / 1e9, "bit_exact_vs_oracle": ok}
+
+
+def extra_config4a(stream):
+    """RMAT-25: 64 sources in one multi-source launch vs 64 plain runs."""
+    import torch
+
+    import scaph_b200 as S
+    from scaph_b200 import workloads
+
+    csr, srcs = workloads.config4a()
+    g = workloads.paged(csr)
+    eng = S.Engine(g, stream=stream.cuda_stream)
+    out = torch.empty((len(srcs), csr.V), dtype=torch.int32, device="cuda")
+    eng.msbfs_device(srcs, out.data_ptr())
+    runs = [eng.msbfs_device(srcs, out.data_ptr()) for _ in range(3)]
+    ms_batch = min(r.ms for r in runs)
+    tr = eng.msbfs_trace()
+    d = torch.empty(csr.V, dtype=torch.int32, device="cuda")
+    for s in srcs[:3]:
+        eng.bfs_device(s, d.data_ptr())
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for s in srcs:
+        eng.bfs_async(s, d.data_ptr())
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms_plain = e0.elapsed_time(e1)
+    eng.close()
+    n = len(srcs)
+    return {"graph": "RMAT-25 ef16", "V": csr.V, "E": csr.E, "sources_per_launch": n,
+            "batched_ms": ms_batch, "batched_gteps_per_source": n * csr.E / (ms_batch / 1e3) / 1e9,
+            "plain_ms_for_same_sources": ms_plain, "plain_gteps": n * csr.E / (ms_plain / 1e3) / 1e9,
+            "speedup_vs_plain": ms_plain / ms_batch, "levels": len(tr),
+            "directions": "".join("p" if t["direction"] else "P" for t in tr)}
+
+
+def _run_set(S, g, gt, srcs, pool, net=None, cold=False, warm_pass=True, **kw):
+    """Times `srcs`; returns total ms, PCIe bytes, levels."""
+    eng = S.Engine(g, gt, pool_bytes=pool, direction=S.DIR_LEARNED if net else 0, **kw)
+    if net:
+        eng.set_scheduler(net)
+    if warm_pass and not cold:
+        for s in srcs:
+            eng.bfs(s)
+    ms, h2d, zc, levels = 0.0, 0, 0, 0
+    for s in srcs:
+        if cold:
+            eng.evict_all()
+        _, _, st = eng.bfs(s)
+        ms += st.ms
+        h2d += st.h2d_bytes
+        zc += st.zc_bytes
+        levels += st.levels
+    eng.close()
+    return {"ms": ms, "h2d_bytes": h2d, "zc_bytes": zc, "levels": levels}
+
+
+def extra_config3(nsrc_train=16, nsrc_eval=16):
+    """Directed power law 41.6M / 1.47B: the learned scheduler (trained on
+    dual-timed plain runs) against alpha/beta + demand paging, in HBM and out
+    of core with the 12 GB page pool (warm: steady-state serving; cold: every
+    source starts from an empty pool)."""
+    import time as _t
+
+    import scaph_b200 as S
+    from scaph_b200 import scheduler, workloads
+
+    t0 = _t.time()
+    csr, tcsr = workloads.config3()
+    g, gt = workloads.paged(csr), workloads.paged(tcsr)
+    gen_s = _t.time() - t0
+    srcs = workloads.random_sources(csr, nsrc_train + nsrc_eval, workloads.SEED_BASE + 2)
+    train, held = srcs[:nsrc_train], srcs[nsrc_train:]
+    pool = 12 * 10**9
+    nslots = pool // (g.pagesize * 4)
+    page_ms = g.pagesize * 4 / 50e9 * 1e3  # page copy at ~50 GB/s (PCIe Gen5 x16, pinned)
+    traces = scheduler.collect(g, gt, train)
+    net, info = scheduler.train(traces, g, gt, nslots, page_ms, epochs=200)
+    E, n = csr.E, len(held)
+    res = {"graph": "directed power law, Zipf 1.9 out-degree, preferential-attachment destinations",
+           "V": csr.V, "E": E, "out_pages": g.npages, "in_pages": gt.npages, "pool_bytes": pool,
+           "graph_gen_s": round(gen_s, 1), "train_sources": nsrc_train, "eval_sources": n, "training": info}
+    for name, kw in (("hbm", dict(pool=0, use_graph=0)), ("ooc_warm", dict(pool=pool)),
+                     ("ooc_cold", dict(pool=pool, cold=True))):
+        plain = _run_set(S, g, gt, held, kw["pool"], None, cold=kw.get("cold", False),
+                         use_graph=kw.get("use_graph", 0))
+        learned = _run_set(S, g, gt, held, kw["pool"], net, cold=kw.get("cold", False),
+                           use_graph=kw.get("use_graph", 0) if kw["pool"] else 0)
+        res[name] = {
+            "plain_gteps": n * E / (plain["ms"] / 1e3) / 1e9, "learned_gteps": n * E / (learned["ms"] / 1e3) / 1e9,
+            "speedup": plain["ms"] / learned["ms"],
+            "plain_pcie_bytes_per_level": plain["h2d_bytes"] / max(1, plain["levels"]),
+            "learned_pcie_bytes_per_level": learned["h2d_bytes"] / max(1, learned["levels"]),
+            "plain_zero_copy_bytes": plain["zc_bytes"], "learned_zero_copy_bytes": learned["zc_bytes"]}
+    return res
+
+
+def extra_pcie(stream):
+    """Pinned host->device copy bandwidth (best of 5, 1 GiB)."""
+    import torch
+
+    h = torch.empty(1 << 30, dtype=torch.uint8).pin_memory()
+    d = torch.empty(1 << 30, dtype=torch.uint8, device="cuda")
+    best = 0.0
+    for _ in range(5):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        d.copy_(h, non_blocking=True)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        best = max(best, (1 << 30) / (e0.elapsed_time(e1) / 1e3) / 1e9)
+    del h, d
+    return {"h2d_gbs_measured": best, "nominal_gbs": 64.0}
+
+
+# ---------------------------------------------------------------------------
 # our arm
 # ---------------------------------------------------------------------------
 def run_ours(args, world):
@@ -338,6 +477,17 @@ def run_ours(args, world):
     L.scaph_host_free(ptr)
     eng_h.close()
     eng.close()
+    if rank == 0 and world == 1 and not args.no_extras:
+        extras = {}
+        for name, fn in (("pcie", lambda: extra_pcie(stream)), ("config1", extra_config1),
+                         ("config4a_batched", lambda: extra_config4a(stream)),
+                         ("config3_learned", extra_config3)):
+            try:
+                extras[name] = fn()
+            except Exception as exc:  # report, keep the headline line
+                extras[name] = {"error": f"{type(exc).__name__}: {exc}"}
+            print(f"[bench] {name}: {json.dumps(extras[name])[:300]}", file=sys.stderr, flush=True)
+        line["extras"] = extras
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()

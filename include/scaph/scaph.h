@@ -173,6 +173,9 @@ typedef struct scaph_config {
     int32_t  dual_timing;      /* host loop, graph resident: run every level
                                   both ways from the same state and record
                                   both times (training labels)             */
+    float    link_gbs;         /* out-of-core learned scheduler: host->HBM
+                                  page bandwidth (GB/s) its transfer-cost
+                                  estimate assumes; 0 = measured at create  */
 } scaph_config;
 
 typedef struct scaph_engine scaph_engine;
@@ -281,8 +284,9 @@ int scaph_engine_set_scheduler(scaph_engine *e, scaph_mlp *m);
  * returns the row count, writes min(rows, cap) rows of *dim floats. */
 int scaph_bfs_features(scaph_engine *e, float *out, int cap, int *dim);
 /* Unvisited vertices per in-edge page at `level` of the last run
- * (record_features): the pages a pull at that level would read. */
-int scaph_bfs_pull_pages(scaph_engine *e, int level, uint32_t *cnt, int npages);
+ * (record_features): the pages a pull at that level would read, and their
+ * active words sum(indeg+3) (datas may be NULL). */
+int scaph_bfs_pull_pages(scaph_engine *e, int level, uint32_t *cnt, uint32_t *datas, int npages);
 
 /* ---- multi-source BFS ---------------------------------------------------- */
 

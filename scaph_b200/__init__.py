@@ -46,7 +46,8 @@ class _Config(C.Structure):
                 ("alpha", C.c_float), ("beta", C.c_float), ("block_size", C.c_int32),
                 ("ctas_per_sm", C.c_int32), ("copy_streams", C.c_int32), ("prefetch", C.c_int32),
                 ("compact_threshold", C.c_int32), ("use_graph", C.c_int32), ("device", C.c_int32),
-                ("stream", C.c_void_p), ("record_features", C.c_int32), ("dual_timing", C.c_int32)]
+                ("stream", C.c_void_p), ("record_features", C.c_int32), ("dual_timing", C.c_int32),
+                ("link_gbs", C.c_float)]
 
 
 class _Stats(C.Structure):
@@ -114,7 +115,7 @@ def lib() -> C.CDLL:
         "scaph_mlp_load": ([vp, C.c_char_p], i32),
         "scaph_engine_set_scheduler": ([vp, vp], i32),
         "scaph_bfs_features": ([vp, vp, i32, P(i32)], i32),
-        "scaph_bfs_pull_pages": ([vp, i32, vp, i32], i32),
+        "scaph_bfs_pull_pages": ([vp, i32, vp, vp, i32], i32),
         "scaph_msbfs": ([vp, vp, i32, vp, i32, P(_Stats)], i32),
         "scaph_msbfs_trace": ([vp, P(_Trace), i32], i32),
         "scaph_bfs_page_hist": ([vp, i32, vp, vp, i32], i32),
@@ -371,10 +372,12 @@ class Engine:
                  unreached: int = UNREACHED, direction: int = DIR_ALPHABETA, alpha: float = 14.0,
                  beta: float = 24.0, block_size: int = 256, ctas_per_sm: int = 0, copy_streams: int = 2,
                  prefetch: int = 0, compact_threshold: int = 3, use_graph: int = 0, device: int = 0,
-                 stream: int | None = None, record_features: int = 0, dual_timing: int = 0):
+                 stream: int | None = None, record_features: int = 0, dual_timing: int = 0,
+                 link_gbs: float = 0.0):
         self.graph, self.transposed = graph, transposed
         cfg = _Config(pool_bytes, unreached, direction, alpha, beta, block_size, ctas_per_sm, copy_streams,
-                      prefetch, compact_threshold, use_graph, device, stream, record_features, dual_timing)
+                      prefetch, compact_threshold, use_graph, device, stream, record_features, dual_timing,
+                      link_gbs)
         self._cfg = cfg
         h = C.c_void_p()
         _check(lib().scaph_engine_create(graph._h, transposed._h if transposed else None, C.byref(cfg), C.byref(h)))
@@ -446,10 +449,12 @@ class Engine:
             lib().scaph_bfs_features(self._h, _ptr(out), rows, C.byref(dim))
         return out
 
-    def pull_pages(self, level: int, npages_in: int) -> np.ndarray:
-        out = np.zeros(npages_in, np.uint32)
-        _check(lib().scaph_bfs_pull_pages(self._h, level, _ptr(out), npages_in))
-        return out
+    def pull_pages(self, level: int, npages_in: int):
+        """(unvisited vertices, their active words) per in-edge page at `level`."""
+        cnt = np.zeros(npages_in, np.uint32)
+        datas = np.zeros(npages_in, np.uint32)
+        _check(lib().scaph_bfs_pull_pages(self._h, level, _ptr(cnt), _ptr(datas), npages_in))
+        return cnt, datas
 
     def evict_all(self) -> None:
         """Out-of-core engines: start the next traversal with a cold page pool."""

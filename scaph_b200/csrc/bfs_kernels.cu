@@ -26,6 +26,7 @@
 // arguments (host-driven loop, out-of-core page batches), the other reads it
 // from a device control block (graph mode: a whole BFS is one CUDA-graph
 // launch whose level loop is a conditional WHILE node, see engine.cu).
+#include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
 #include "device.cuh"
@@ -705,6 +706,94 @@ __global__ void k_decide(BfsGraphArgs a, DecideArgs d, cudaGraphConditionalHandl
     cudaGraphSetConditional(h_loop, 1);
 }
 
+// Learned variant of k_decide (64 threads): the scheduler's feature row of
+// the coming level - the same 16 globals the host loop computes (scaph.h),
+// page residency 1 (graph resident), then the new frontier's share of every
+// out-page - through the network's three layers; output 0 > 0 means pull.
+__global__ void __launch_bounds__(64) k_decide_learned(BfsGraphArgs a, DecideArgs d, MlpDev net,
+                                                       cudaGraphConditionalHandle h_loop,
+                                                       cudaGraphConditionalHandle h_push,
+                                                       cudaGraphConditionalHandle h_pull)
+{
+    constexpr int kG = 16;
+    __shared__ float f[kG + kHistCap];
+    __shared__ float h1[64], h2[64];
+    __shared__ int s_stop, s_ab;
+    BfsCtl *c = a.ctl;
+    const uint32_t L = c->level;
+    const int t = threadIdx.x;
+    if (t == 0) {
+        LevelCounters *lc = a.ctr0 + L;
+        lc->dir = c->dir;
+        lc->t_end = globaltimer();
+        c->prev_nf = c->nf;
+        c->nf = lc->next;
+        c->mf = lc->next_edges;
+        c->vis_n += c->nf;
+        c->vis_e += c->mf;
+        s_stop = c->nf == 0 || lc->error != 0 || (int)L + 1 >= d.max_levels ||
+                 (unsigned long long)L + 2 >= d.unreached;
+        const unsigned long long used = c->vis_e + d.dead_edges;
+        const unsigned long long mu = d.E > used ? d.E - used : 0;
+        const uint32_t src = c->src;
+        const unsigned long long src_dead = (d.dead_bm[src >> 5] >> (src & 31)) & 1u;
+        const unsigned long long unv = (unsigned long long)d.V - d.dead - c->vis_n + src_dead;
+        s_ab = alpha_beta_next(c->dir, c->nf, c->prev_nf, c->mf, mu, d.V, d.alpha, d.beta);
+        f[0] = log2f(1.f + (float)c->nf) / 32.f;
+        f[1] = log2f(1.f + (float)c->mf) / 40.f;
+        f[2] = log2f(1.f + (float)unv) / 32.f;
+        f[3] = log2f(1.f + (float)mu) / 40.f;
+        f[4] = (float)c->nf / (float)d.V;
+        f[5] = fminf(1.f, (float)c->mf / (float)(d.E ? d.E : 1));
+        f[6] = (float)unv / (float)d.V;
+        f[7] = fminf(1.f, (float)mu / (float)(d.E ? d.E : 1));
+        f[8] = (float)(L + 1) / 32.f;
+        f[9] = (float)c->dir;
+        f[10] = f[11] = f[12] = f[13] = 1.f;
+        f[14] = (float)s_ab;
+        f[15] = 1.f;
+    }
+    // frontier of level L+1 = vertices discovered by level L (histogram slot L)
+    const int np = net.in - kG;
+    const PageDev *pg = a.base.hg.pages;
+    for (int p = t; p < np; p += 64) {
+        const uint32_t hn = (a.hist0 && L < a.hist_levels) ? a.hist0[(size_t)L * 2 * a.npages_h + p] : 0u;
+        f[kG + p] = (float)hn / (float)max(1u, pg[p].nodenum);
+    }
+    __syncthreads();
+    if (s_stop) {
+        if (t == 0) {
+            c->done = 1;
+            cudaGraphSetConditional(h_loop, 0);
+            cudaGraphSetConditional(h_push, 0);
+            cudaGraphSetConditional(h_pull, 0);
+        }
+        return;
+    }
+    // weights (and GEMM operands) rounded to bf16, FP32 accumulation, as in
+    // the training kernels
+    auto bf = [](float x) { return __bfloat162float(__float2bfloat16_rn(x)); };
+    const float *W1 = net.w + net.off_w1, *W2 = net.w + net.off_w2, *W3 = net.w + net.off_w3;
+    float acc = net.w[net.off_b1 + t];
+    for (int i = 0; i < net.in; i++) acc += bf(f[i]) * bf(W1[(size_t)i * 64 + t]);
+    h1[t] = fmaxf(acc, 0.f);
+    __syncthreads();
+    acc = net.w[net.off_b2 + t];
+    for (int i = 0; i < 64; i++) acc += bf(h1[i]) * bf(W2[i * 64 + t]);
+    h2[t] = fmaxf(acc, 0.f);
+    __syncthreads();
+    if (t == 0) {
+        float y = net.w[net.off_b3];
+        for (int j = 0; j < 64; j++) y += bf(h2[j]) * bf(W3[(size_t)j * net.out]);
+        const int nd = d.mode == 1 ? 0 : d.mode == 2 ? 1 : (y > 0.f ? 1 : 0);
+        c->dir = nd;
+        c->level = L + 1;
+        cudaGraphSetConditional(h_push, nd == 0 ? 1 : 0);
+        cudaGraphSetConditional(h_pull, nd == 1 ? 1 : 0);
+        cudaGraphSetConditional(h_loop, 1);
+    }
+}
+
 // ---------------------------------------------------------------------------
 // state init helpers (host loop)
 // ---------------------------------------------------------------------------
@@ -815,6 +904,7 @@ cudaError_t run_level_graph(int dir, int block, int grid, const GraphDev &g, con
 const void *graph_init_kernel() { return (const void *)k_graph_init; }
 const void *graph_start_kernel() { return (const void *)k_graph_start; }
 const void *decide_kernel() { return (const void *)k_decide; }
+const void *decide_learned_kernel() { return (const void *)k_decide_learned; }
 
 int level_occupancy(int dir, int block)
 {

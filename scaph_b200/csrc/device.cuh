@@ -98,10 +98,19 @@ struct BfsGraphArgs {
     BfsCtl *ctl;
 };
 
+// The scheduler network as the decide kernel reads it (weights already
+// rounded to bf16): W1[in][64] b1[64] W2[64][64] b2[64] W3[64][out] b3[out].
+struct MlpDev {
+    const float *w;
+    int in, out;
+    unsigned long long off_w1, off_b1, off_w2, off_b2, off_w3, off_b3;
+};
+
 struct DecideArgs {
     unsigned long long E;           // out-edges (for m_u)
     unsigned long long dead_edges;  // out-edges of vertices no edge reaches
     unsigned long long dead;        // vertices no edge reaches
+    const uint32_t *dead_bm;        // their bitmap
     uint32_t V;
     uint32_t unreached;
     int32_t mode;                   // SCAPH_DIR_*

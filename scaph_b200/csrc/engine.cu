@@ -151,7 +151,7 @@ int scaph_engine::create(const Graph *g_, const Graph *gt_, const scaph_config *
     const int nslots = cfg.pool_bytes > 0 ? (int)std::max<int64_t>(1, cfg.pool_bytes / per) : 0;
     if (nslots > 0 && (size_t)nslots < total_pages) {
         // out-of-core: pages stream through a pool of nslots page slots
-        if ((rc = pager_create(this, nslots, &pager))) return rc;
+        if ((rc = pager_create(g, gt, nslots, cfg.copy_streams, cfg.link_gbs, &pager))) return rc;
     } else {
         if ((rc = dout.build(*g, 0, st))) return rc;
         if (gt && (rc = din.build(*gt, 0, st))) return rc;
@@ -246,24 +246,32 @@ void scaph_engine::destroy()
 // Scheduler features of the coming level (layout in scaph.h /
 // DESIGN.md): 16 globals, then the frontier's share of every out-edge page.
 int scaph_engine::features(int level, uint32_t src, uint64_t nf, uint64_t mf, uint64_t unvis, uint64_t mu,
-                           int prev_dir, int ab_dir, float *f, std::vector<uint32_t> &pull_cnt)
+                           int prev_dir, int ab_dir, float *f, std::vector<uint32_t> &pull_cnt,
+                           std::vector<uint32_t> &hist)
 {
     const size_t np = g->pages.size();
     const GraphDev &gi = gin();
     const int npi = (int)gi.npages;
-    // frontier histogram over out-pages (level 0: the source alone)
-    std::vector<uint32_t> hist(np, 0);
+    // frontier histogram over out-pages, counts then active words (level 0:
+    // the source alone)
+    hist.assign(2 * np, 0);
     if (level == 0) {
         size_t p = 0;
         while (p + 1 < np && g->pages[p + 1].left <= src) p++;
         hist[p] = 1;
+        hist[np + p] = g->degree[src] + 3;
     } else if (level - 1 < kHistLevels) {
-        SCAPH_CUDA(cudaMemcpyAsync(hist.data(), d_hist + (size_t)(level - 1) * 2 * np, np * 4, cudaMemcpyDeviceToHost, st));
+        SCAPH_CUDA(cudaMemcpyAsync(hist.data(), d_hist + (size_t)(level - 1) * 2 * np, 2 * np * 4,
+                                   cudaMemcpyDeviceToHost, st));
     }
-    // unvisited vertices per in-edge page
-    pull_cnt.assign(npi, 0);
-    SCAPH_CUDA(page_unvisited(gi, d_visited, d_indeg, d_pcnt, d_pdatas, num_sms * 4, st));
-    SCAPH_CUDA(cudaMemcpyAsync(pull_cnt.data(), d_pcnt, npi * 4, cudaMemcpyDeviceToHost, st));
+    // unvisited vertices per in-edge page (only needed out of core, for the
+    // residency features, and for training traces)
+    pull_cnt.assign(2 * (size_t)npi, 0);  // counts, then active words
+    if (pager || cfg.record_features) {
+        SCAPH_CUDA(page_unvisited(gi, d_visited, d_indeg, d_pcnt, d_pdatas, num_sms * 4, st));
+        SCAPH_CUDA(cudaMemcpyAsync(pull_cnt.data(), d_pcnt, npi * 4, cudaMemcpyDeviceToHost, st));
+        SCAPH_CUDA(cudaMemcpyAsync(pull_cnt.data() + npi, d_pdatas, npi * 4, cudaMemcpyDeviceToHost, st));
+    }
     SCAPH_CUDA(cudaStreamSynchronize(st));
     auto lg = [](double x, double d) { return (float)(std::log2(1.0 + x) / d); };
     f[0] = lg((double)nf, 32);
@@ -282,7 +290,7 @@ int scaph_engine::features(int level, uint32_t src, uint64_t nf, uint64_t mf, ui
         for (size_t p = 0; p < np; p++)
             if (hist[p]) push_pages.push_back((int)p);
         for (int p = 0; p < npi; p++)
-            if (pull_cnt[p]) pull_pages.push_back(p);
+            if (pull_cnt[p]) pull_pages.push_back(p);  // counts are the first npi entries
         const int gid_in = symmetric ? 0 : 1;
         res_out = pager_resident_fraction(pager, 0, nullptr);
         res_in = pager_resident_fraction(pager, gid_in, nullptr);
@@ -341,21 +349,38 @@ int scaph_engine::run_host_loop(uint32_t src, uint32_t *dd, uint32_t *dp)
         }
         std::vector<int> prefetch_pages;
         if (want_feat) {
-            std::vector<uint32_t> pc;
+            std::vector<uint32_t> pc, hist;
             const uint64_t unvis = (uint64_t)V - n_dead - vis_n + (src_dead ? 1 : 0);
-            int rc = features(level, src, nf, mf, unvis, mu, prev_dir, ab, f.data(), pc);
+            int rc = features(level, src, nf, mf, unvis, mu, prev_dir, ab, f.data(), pc, hist);
             if (rc) return rc;
             feat_log.insert(feat_log.end(), f.begin(), f.end());
-            pull_log.push_back(std::move(pc));
             if (learned) {
                 int in = 0, out = 0;
                 mlp_dims(sched, &in, &out);
                 y.resize(out);
-                if ((rc = mlp_forward_device(sched, f.data(), 1, y.data()))) return rc;
-                if (level > 0) dir = y[0] > 0.f ? 1 : 0;
+                if ((rc = mlp_forward1(sched, f.data(), y.data(), st))) return rc;
+                if (level > 0) {
+                    // the network models kernel time (trained resident);
+                    // out of core the page traffic each direction would
+                    // cause is known exactly and overrides it when it
+                    // clearly dominates
+                    dir = y[0] > 0.f ? 1 : 0;
+                    if (pager) {
+                        const int npi = (int)pc.size() / 2;
+                        const double t_push = pager_transfer_ms(pager, 0, hist.data(), hist.data() + np, (int)np,
+                                                                cfg.compact_threshold);
+                        const double t_pull = pager_transfer_ms(pager, symmetric ? 0 : 1, pc.data(), pc.data() + npi,
+                                                                npi, cfg.compact_threshold);
+                        if (t_push > 2 * t_pull + 1.0) dir = 1;
+                        else if (t_pull > 2 * t_push + 1.0) dir = 0;
+                    }
+                }
+                // prefetch only pages the network is confident about (into
+                // free slots; never at the expense of resident pages)
                 for (int p = 0; p + 1 < out && p < (int)np; p++)
-                    if (y[1 + p] > 0.f) prefetch_pages.push_back(p);
+                    if (y[1 + p] > 2.f) prefetch_pages.push_back(p);
             }
+            pull_log.push_back(std::move(pc));
         }
         uint32_t *next = bm[cur ^ 1];
         s.front = bm[cur];
@@ -449,6 +474,7 @@ int scaph_engine::build_graph()
     dargs.E = E;
     dargs.dead_edges = dead_edges;
     dargs.dead = n_dead;
+    dargs.dead_bm = d_dead;
     dargs.V = V;
     dargs.unreached = unreached;
     dargs.mode = cfg.direction == SCAPH_DIR_PUSH ? 1 : cfg.direction == SCAPH_DIR_PULL ? 2 : 0;
@@ -503,12 +529,16 @@ int scaph_engine::build_graph()
     SCAPH_CUDA(cudaGraphAddNode(&n_ifpull, body, &n_ifpush, 1, &iq));
     cudaGraph_t bpull = iq.conditional.phGraph_out[0];
 
+    const bool learned = cfg.direction == SCAPH_DIR_LEARNED && sched;
+    MlpDev net{};
+    if (learned) mlp_device_view(sched, &net);
     void *dec_args[] = {&gargs, &dargs, &h_loop, &h_push, &h_pull};
+    void *dec_learned_args[] = {&gargs, &dargs, &net, &h_loop, &h_push, &h_pull};
     cudaKernelNodeParams dp{};
-    dp.func = const_cast<void *>(decide_kernel());
+    dp.func = const_cast<void *>(learned ? decide_learned_kernel() : decide_kernel());
     dp.gridDim = dim3(1);
-    dp.blockDim = dim3(1);
-    dp.kernelParams = dec_args;
+    dp.blockDim = dim3(learned ? 64 : 1);
+    dp.kernelParams = learned ? dec_learned_args : dec_args;
     cudaGraphNode_t n_decide;
     SCAPH_CUDA(cudaGraphAddKernelNode(&n_decide, body, &n_ifpull, 1, &dp));
 
@@ -522,6 +552,17 @@ int scaph_engine::build_graph()
     SCAPH_CUDA(e2);
     SCAPH_CUDA(cudaGraphInstantiate(&gexec, graph, 0));
     return SCAPH_OK;
+}
+
+void scaph_engine::drop_graph()
+{
+    if (st) cudaStreamSynchronize(st);
+    if (gexec) cudaGraphExecDestroy(gexec);
+    if (graph) cudaGraphDestroy(graph);
+    if (cap_st) cudaStreamDestroy(cap_st);
+    gexec = nullptr;
+    graph = nullptr;
+    cap_st = nullptr;
 }
 
 int scaph_engine::launch_graph(uint32_t src, uint32_t *dd, uint32_t *dp)
@@ -704,6 +745,7 @@ int scaph_engine_set_scheduler(scaph_engine *e, scaph_mlp *m)
             return set_error(SCAPH_EINVAL, "scheduler network must be %d -> %d for this graph (is %d -> %d)",
                              SCAPH_SCHED_GLOBALS + np, 1 + np, in, out);
     }
+    if (e->sched != m) e->drop_graph();  // the decide node embeds the network
     e->sched = m;
     return SCAPH_OK;
 }
@@ -717,14 +759,16 @@ int scaph_bfs_features(scaph_engine *e, float *out, int cap, int *dim)
     return rows;
 }
 
-int scaph_bfs_pull_pages(scaph_engine *e, int level, uint32_t *cnt, int npages)
+int scaph_bfs_pull_pages(scaph_engine *e, int level, uint32_t *cnt, uint32_t *datas, int npages)
 {
     if (!e || !cnt) return set_error(SCAPH_EINVAL, "null argument");
     if (level < 0 || level >= (int)e->pull_log.size()) return set_error(SCAPH_EINVAL, "level %d not recorded", level);
     const auto &v = e->pull_log[level];
-    if (npages < (int)v.size()) return set_error(SCAPH_EINVAL, "need %zu pages", v.size());
-    memcpy(cnt, v.data(), v.size() * 4);
-    return (int)v.size();
+    const int n = (int)v.size() / 2;
+    if (npages < n) return set_error(SCAPH_EINVAL, "need %d pages", n);
+    memcpy(cnt, v.data(), (size_t)n * 4);
+    if (datas) memcpy(datas, v.data() + n, (size_t)n * 4);
+    return n;
 }
 
 int scaph_engine_evict_all(scaph_engine *e)

@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 
 #include <string>
+#include <functional>
 #include <vector>
 
 #include "common.h"
@@ -43,24 +44,46 @@ int coarse_index(const Graph &g, std::vector<uint32_t> &hc, uint32_t &cshift);
 }  // namespace scaph
 
 namespace scaph {
-int pager_create(scaph_engine *e, int nslots, Pager **out);
+// Runs the kernels of one batch of resident (or zero-copy) pages: `view` is
+// the graph's page table as the kernels must read it, `rl` the batch's
+// vertex ranges; range i owns the tiles tile0[i].. of 128 bitmap words
+// counted from its first word (`tiles` in all, see range_of_tile).
+struct PageLaunch {
+    std::function<int(const GraphDev &view, int gid, const RangeList &rl, uint32_t tiles, cudaStream_t st)> run;
+};
+int pager_create(const Graph *g, const Graph *gt, int nslots, int copy_streams, float link_gbs, Pager **out);
 void pager_release(Pager *p);
 const GraphDev &pager_view(const Pager *p, int gid);
 int pager_needs(scaph_engine *e, Pager *pg, int dir, int level, uint32_t src, std::vector<int> &needed,
                 std::vector<uint32_t> &datas);
 int pager_run_level(scaph_engine *e, Pager *pg, int dir, const BfsDev &s, const std::vector<int> &needed,
                     const std::vector<uint32_t> &datas);
+int pager_run_level(Pager *pg, int gid, const std::vector<int> &needed, const std::vector<uint32_t> &datas,
+                    int compact_threshold, const PageLaunch &fn, cudaStream_t st);
 int pager_prefetch(scaph_engine *e, Pager *pg, int gid, const std::vector<int> &pages);
+// Pages of graph gid holding set bits of `bits` (invert: clear bits), with
+// their words sum(deg*ew+3); synchronises st.
+int pager_page_counts(Pager *pg, int gid, const uint32_t *bits, bool invert, const uint32_t *deg, uint32_t ew,
+                      int grid, cudaStream_t st, std::vector<int> &needed, std::vector<uint32_t> &datas);
 void pager_counters(const Pager *pg, uint64_t *h2d, uint64_t *zc, uint64_t *faults, uint64_t *prefetched,
                     uint64_t *hits, uint64_t *level_h2d);
 void pager_reset_counters(Pager *pg);
 void pager_evict_all(Pager *pg);
 int pager_nslots(const Pager *pg);
 float pager_resident_fraction(const Pager *pg, int gid, const std::vector<int> *pages);
+// Page traffic (ms at the measured PCIe bandwidth) a level would cause on
+// graph gid: per page with cnt > 0, nothing if resident, its active words
+// if sparse enough for zero-copy reads, else a full page copy.
+double pager_transfer_ms(const Pager *pg, int gid, const uint32_t *cnt, const uint32_t *datas, int npages,
+                         int compact_threshold);
 cudaError_t page_unvisited(const GraphDev &g, const uint32_t *visited, const uint32_t *indeg, uint32_t *cnt,
                            uint32_t *datas, int grid, cudaStream_t st);
+cudaError_t page_counts(const GraphDev &g, const uint32_t *bits, bool invert, const uint32_t *deg, uint32_t ew,
+                        uint32_t *cnt, uint32_t *datas, int grid, cudaStream_t st);
 int mlp_forward_device(scaph_mlp *m, const float *hX, int n, float *hY);
 int mlp_dims(const scaph_mlp *m, int *in, int *out);
+int mlp_device_view(const scaph_mlp *m, MlpDev *v);
+int mlp_forward1(scaph_mlp *m, const float *hX, float *hY, cudaStream_t st);
 }  // namespace scaph
 
 // The engine behind the opaque C-ABI handle.
@@ -133,13 +156,18 @@ struct scaph_engine {
 
     const GraphDev &out_view() const;
     const GraphDev &gin() const;
-    bool graph_mode() const { return cfg.use_graph != 2 && !pager; }
+    bool graph_mode() const
+    {
+        return cfg.use_graph != 2 && !pager && !cfg.record_features && !cfg.dual_timing &&
+               (cfg.direction != SCAPH_DIR_LEARNED || sched);
+    }
+    void drop_graph();
     int create(const Graph *g_, const Graph *gt_, const scaph_config *c);
     void destroy();
     int bfs(uint32_t src, uint32_t *depths, uint32_t *parents, int out_on_device, scaph_bfs_stats *stats);
     int run_host_loop(uint32_t src, uint32_t *dd, uint32_t *dp);
     int features(int level, uint32_t src, uint64_t nf, uint64_t mf, uint64_t unvis, uint64_t mu, int prev_dir,
-                 int ab_dir, float *f, std::vector<uint32_t> &pull_cnt);
+                 int ab_dir, float *f, std::vector<uint32_t> &pull_cnt, std::vector<uint32_t> &hist);
     int build_graph();
     int launch_graph(uint32_t src, uint32_t *dd, uint32_t *dp);
     int collect(bool from_graph);

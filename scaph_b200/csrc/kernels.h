@@ -23,6 +23,8 @@ const void *graph_init_kernel();
 const void *graph_start_kernel();
 // k_decide(BfsGraphArgs, DecideArgs, handle loop, handle push, handle pull)
 const void *decide_kernel();
+// k_decide_learned(BfsGraphArgs, DecideArgs, MlpDev, handle loop, handle push, handle pull): 64 threads
+const void *decide_learned_kernel();
 // Resident CTAs per SM of the level kernel for `dir` at `block` threads.
 int level_occupancy(int dir, int block);
 cudaError_t fill_u32(uint32_t *p, uint32_t value, unsigned long long n, int grid, cudaStream_t st);

@@ -170,14 +170,37 @@ __global__ void k_adam(float *w, const float *g, float *m, float *v, size_t n, f
     w[i] -= lr * (mi / c1) / (sqrtf(vi / c2) + eps);
 }
 
-// Rounds the master weights to bf16 in place (the weights the network keeps).
-__global__ void k_round_bf16(float *w, size_t n)
-{
-    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) w[i] = __bfloat162float(__float2bfloat16_rn(w[i]));
-}
-
 inline unsigned grid_of(size_t n) { return (unsigned)((n + 255) / 256); }
+
+// One row through the network in a single CTA (scheduler inference, one
+// feature row per level): operands rounded to bf16, FP32 accumulation.
+__global__ void __launch_bounds__(256) k_forward1(const float *w, int in, int out, size_t ow1, size_t ob1,
+                                                  size_t ow2, size_t ob2, size_t ow3, size_t ob3, const float *x,
+                                                  float *y)
+{
+    extern __shared__ float sx[];  // in floats
+    __shared__ float h1[kH], h2[kH];
+    auto bf = [](float v) { return __bfloat162float(__float2bfloat16_rn(v)); };
+    for (int i = threadIdx.x; i < in; i += blockDim.x) sx[i] = bf(x[i]);
+    __syncthreads();
+    if (threadIdx.x < kH) {
+        float a = w[ob1 + threadIdx.x];
+        for (int i = 0; i < in; i++) a += sx[i] * bf(w[ow1 + (size_t)i * kH + threadIdx.x]);
+        h1[threadIdx.x] = bf(fmaxf(a, 0.f));
+    }
+    __syncthreads();
+    if (threadIdx.x < kH) {
+        float a = w[ob2 + threadIdx.x];
+        for (int i = 0; i < kH; i++) a += h1[i] * bf(w[ow2 + i * kH + threadIdx.x]);
+        h2[threadIdx.x] = bf(fmaxf(a, 0.f));
+    }
+    __syncthreads();
+    for (int o = threadIdx.x; o < out; o += blockDim.x) {
+        float a = w[ob3 + o];
+        for (int j = 0; j < kH; j++) a += h2[j] * bf(w[ow3 + (size_t)j * out + o]);
+        y[o] = a;
+    }
+}
 
 }  // namespace
 
@@ -274,6 +297,33 @@ int mlp_forward_device(scaph_mlp *m, const float *hX, int n, float *hY)
     if ((rc = m->forward(n))) return rc;
     SCAPH_CUDA(cudaMemcpyAsync(hY, m->Y, sizeof(float) * n * m->out, cudaMemcpyDeviceToHost, m->st));
     SCAPH_CUDA(cudaStreamSynchronize(m->st));
+    return SCAPH_OK;
+}
+
+int mlp_forward1(scaph_mlp *m, const float *hX, float *hY, cudaStream_t st)
+{
+    int rc = m->ensure(1);
+    if (rc) return rc;
+    SCAPH_CUDA(cudaMemcpyAsync(m->X, hX, sizeof(float) * m->in, cudaMemcpyHostToDevice, st));
+    k_forward1<<<1, 256, sizeof(float) * m->in, st>>>(m->w, m->in, m->out, m->off_w1, m->off_b1, m->off_w2,
+                                                       m->off_b2, m->off_w3, m->off_b3, m->X, m->Y);
+    SCAPH_CUDA(cudaGetLastError());
+    SCAPH_CUDA(cudaMemcpyAsync(hY, m->Y, sizeof(float) * m->out, cudaMemcpyDeviceToHost, st));
+    SCAPH_CUDA(cudaStreamSynchronize(st));
+    return SCAPH_OK;
+}
+
+int mlp_device_view(const scaph_mlp *m, MlpDev *v)
+{
+    v->w = m->w;
+    v->in = m->in;
+    v->out = m->out;
+    v->off_w1 = m->off_w1;
+    v->off_b1 = m->off_b1;
+    v->off_w2 = m->off_w2;
+    v->off_b2 = m->off_b2;
+    v->off_w3 = m->off_w3;
+    v->off_b3 = m->off_b3;
     return SCAPH_OK;
 }
 
@@ -382,8 +432,8 @@ int scaph_mlp_loss_grad(scaph_mlp *m, const float *X, const float *T, const floa
     return SCAPH_OK;
 }
 
-// One Adam step on the n rows given (beta1 0.9, beta2 0.999, eps 1e-8); the
-// updated weights are rounded to bf16.
+// One Adam step on the n rows given (beta1 0.9, beta2 0.999, eps 1e-8) on
+// the FP32 master weights; every use rounds them to bf16.
 int scaph_mlp_adam_step(scaph_mlp *m, const float *X, const float *T, const float *W, int n, float lr, float *loss)
 {
     clear_error();
@@ -395,7 +445,6 @@ int scaph_mlp_adam_step(scaph_mlp *m, const float *X, const float *T, const floa
     const float b1 = 0.9f, b2 = 0.999f;
     const float c1 = 1.f - std::pow(b1, (float)m->step), c2 = 1.f - std::pow(b2, (float)m->step);
     k_adam<<<grid_of(m->nparams), 256, 0, m->st>>>(m->w, m->g, m->m, m->v, m->nparams, lr, b1, b2, 1e-8f, c1, c2);
-    k_round_bf16<<<grid_of(m->nparams), 256, 0, m->st>>>(m->w, m->nparams);
     SCAPH_CUDA(cudaGetLastError());
     if (loss) SCAPH_CUDA(cudaMemcpyAsync(loss, m->loss, 4, cudaMemcpyDeviceToHost, m->st));
     SCAPH_CUDA(cudaStreamSynchronize(m->st));
@@ -433,7 +482,7 @@ int scaph_mlp_train(scaph_mlp *m, const float *X, const float *T, const float *W
     return SCAPH_OK;
 }
 
-// Checkpoint: dims, step, BF16 weights (as float) and the FP32 Adam moments.
+// Checkpoint: dims, step, the FP32 master weights and the FP32 Adam moments.
 int scaph_mlp_save(const scaph_mlp *m, const char *path)
 {
     if (!m || !path) return set_error(SCAPH_EINVAL, "bad argument");

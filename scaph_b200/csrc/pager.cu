@@ -51,39 +51,74 @@ __global__ void k_table_update(PageDev *tab, TableUpdate u)
     if (i < u.n) tab[u.page[i]].base = u.base[i];
 }
 
-// Per page of graph g: unvisited vertices (dead ones start visited) and their
-// words sum(indeg+3) - the pull-side counterpart of get_page_info.
-__global__ void k_page_unvisited(const uint32_t *visited, const PageDev *pages, uint32_t npages, uint32_t V,
-                                 const uint32_t *indeg, uint32_t *cnt, uint32_t *datas)
+// Per page of graph g: the vertices whose bit is set in bits ^ flip and their
+// words sum(deg*ew+3).  flip = 0: active vertices and their out-degrees, i.e.
+// get_page_info (src/gpu_engine.cuh:397-441, ew = 2 for weighted pages);
+// flip = ~0 over the visited bitmap: unvisited vertices (dead ones start
+// visited) with their in-degrees, the pull-side counterpart.  A warp
+// takes one visited word at a time (lane = vertex, coalesced in-degree
+// reads); a word spans at most two pages (pages hold >= 32 vertices or the
+// word is split lane by lane); per-CTA shared counters, one global atomic per
+// page per CTA.  cnt/datas must be zeroed by the caller.
+__global__ void k_page_counts(const uint32_t *bits, uint32_t flip, GraphDev g, const uint32_t *deg, uint32_t ew,
+                              uint32_t *cnt, uint32_t *datas)
 {
-    __shared__ unsigned long long sc, sd;
-    for (uint32_t p = blockIdx.x; p < npages; p += gridDim.x) {
-        if (threadIdx.x == 0) sc = sd = 0;
-        __syncthreads();
-        const uint32_t lo = pages[p].left, hi = pages[p + 1].left;  // [lo, hi)
-        unsigned long long c = 0, d = 0;
-        for (uint32_t w = (lo >> 5) + threadIdx.x; w <= ((hi - 1) >> 5); w += blockDim.x) {
-            uint32_t m = ~visited[w] & range_mask(w, lo, hi);
-            c += __popc(m);
-            while (m) {
-                const uint32_t v = (w << 5) + (__ffs(m) - 1);
-                d += indeg[v] + 3;
-                m &= m - 1;
+    __shared__ uint32_t sc[kHistCap], sd[kHistCap];
+    const bool local = g.npages <= (uint32_t)kHistCap;
+    if (local)
+        for (uint32_t i = threadIdx.x; i < g.npages; i += blockDim.x) sc[i] = sd[i] = 0;
+    __syncthreads();
+    const int lane = threadIdx.x & 31;
+    const uint32_t nwords = (g.V + 31) / 32;
+    const uint32_t wstride = (gridDim.x * blockDim.x) >> 5;
+    for (uint32_t w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < nwords; w += wstride) {
+        const uint32_t m = (bits[w] ^ flip) & range_mask(w, 0, g.V);
+        if (!m) continue;
+        const uint32_t v = (w << 5) + lane;
+        const bool on = (m >> lane) & 1u;
+        const int p = on ? page_of(g, v) : -1;
+        const uint32_t d = on ? deg[v] * ew + 3 : 0;
+        const int p0 = __shfl_sync(0xFFFFFFFFu, p, __ffs(m) - 1);
+        const bool first = on && p == p0;
+        const uint32_t c0 = __popc(__ballot_sync(0xFFFFFFFFu, first));
+        uint32_t d0 = first ? d : 0, d1 = (on && !first) ? d : 0;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            d0 += __shfl_xor_sync(0xFFFFFFFFu, d0, o);
+            d1 += __shfl_xor_sync(0xFFFFFFFFu, d1, o);
+        }
+        const uint32_t rest = __ballot_sync(0xFFFFFFFFu, on && !first);
+        if (lane == 0) {
+            if (local) {
+                atomicAdd(&sc[p0], c0);
+                atomicAdd(&sd[p0], d0);
+            } else {
+                atomicAdd(&cnt[p0], c0);
+                atomicAdd(&datas[p0], d0);
             }
         }
-        c = kc::warp_sum64(c);
-        d = kc::warp_sum64(d);
-        if ((threadIdx.x & 31) == 0) {
-            atomicAdd(&sc, c);
-            atomicAdd(&sd, d);
+        if (rest) {
+            // the lanes past the page boundary: rare, one atomic per lane
+            if (on && !first) {
+                if (local) {
+                    atomicAdd(&sc[p], 1u);
+                    atomicAdd(&sd[p], d);
+                } else {
+                    atomicAdd(&cnt[p], 1u);
+                    atomicAdd(&datas[p], d);
+                }
+            }
+            (void)d1;
         }
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            cnt[p] = (uint32_t)sc;
-            datas[p] = (uint32_t)min(sd, 0xFFFFFFFFull);
-        }
-        __syncthreads();
     }
+    __syncthreads();
+    if (local)
+        for (uint32_t i = threadIdx.x; i < g.npages; i += blockDim.x) {
+            if (sc[i]) {
+                atomicAdd(&cnt[i], sc[i]);
+                atomicAdd(&datas[i], sd[i]);
+            }
+        }
 }
 
 }  // namespace
@@ -142,18 +177,18 @@ struct Pager {
     // counters of the current run
     uint64_t h2d_bytes = 0, zc_bytes = 0, faults = 0, prefetched = 0, prefetch_hits = 0;
     uint64_t level_h2d = 0;
+    double h2d_gbs = 50.0;  // measured at init
 
     ~Pager();
-    int init(scaph_engine *e, int nslots_, int copy_streams);
-    int setup_graph(int gid, const Graph &g, cudaStream_t st);
+    int init(const Graph *g, const Graph *gt, int nslots_, int copy_streams, float link_gbs);
+    int setup_graph(int gid, const Graph &g);
     int acquire_slot(int gid, bool for_prefetch);
-    int load(int gid, int p, cudaStream_t compute, bool prefetch);
+    int load(int gid, int p, bool prefetch);
     int publish(int gid, const std::vector<int> &pages, cudaStream_t st);
-    int launch(int dir, int gid, bool zc, const std::vector<int> &pages, scaph_engine *e, const BfsDev &s,
-               cudaStream_t st);
-    int run_level(scaph_engine *e, int dir, const BfsDev &s, const std::vector<int> &needed,
-                  const std::vector<uint32_t> &datas, cudaStream_t st);
-    int prefetch(int gid, const std::vector<int> &pages, cudaStream_t st);
+    int launch(int gid, bool zc, const std::vector<int> &pages, const PageLaunch &fn, cudaStream_t st);
+    int run_level(int gid, const std::vector<int> &needed, const std::vector<uint32_t> &datas,
+                  int compact_threshold, const PageLaunch &fn, cudaStream_t st);
+    int prefetch(int gid, const std::vector<int> &pages);
     void evict_all();
 };
 
@@ -181,7 +216,7 @@ Pager::~Pager()
 
 void pager_release(Pager *p) { delete p; }
 
-int Pager::setup_graph(int gid, const Graph &g, cudaStream_t st)
+int Pager::setup_graph(int gid, const Graph &g)
 {
     GState &G = gs[gid];
     G.host = &g;
@@ -227,16 +262,15 @@ int Pager::setup_graph(int gid, const Graph &g, cudaStream_t st)
     G.zc.pool = G.host_dev;
     G.zc.pages = G.d_zc_tab;
     G.zc.pool_words = g.data_words;
-    (void)st;
     return SCAPH_OK;
 }
 
-int Pager::init(scaph_engine *e, int nslots_, int copy_streams)
+int Pager::init(const Graph *g, const Graph *gt, int nslots_, int copy_streams, float link_gbs)
 {
     nslots = nslots_;
-    pagesize = e->g->pagesize;
+    pagesize = g->pagesize;
     slot_words = pagesize;
-    if (e->gt && e->gt->pagesize != pagesize) return set_error(SCAPH_EINVAL, "out/in graphs need the same page size");
+    if (gt && gt->pagesize != pagesize) return set_error(SCAPH_EINVAL, "out/in graphs need the same page size");
     SCAPH_CUDA(cudaMalloc(&pool, (size_t)nslots * slot_words * 4));
     slots.resize(nslots);
     for (auto &s : slots) {
@@ -245,11 +279,30 @@ int Pager::init(scaph_engine *e, int nslots_, int copy_streams)
     }
     ncst = std::max(1, std::min(4, copy_streams));
     for (int i = 0; i < ncst; i++) SCAPH_CUDA(cudaStreamCreateWithFlags(&cst[i], cudaStreamNonBlocking));
-    ngraphs = e->gt ? 2 : 1;
-    int rc = setup_graph(0, *e->g, e->st);
+    ngraphs = gt ? 2 : 1;
+    int rc = setup_graph(0, *g);
     if (rc) return rc;
-    if (e->gt && (rc = setup_graph(1, *e->gt, e->st))) return rc;
-    size_t maxp = e->g->pages.size() + (e->gt ? e->gt->pages.size() : 0);
+    if (gt && (rc = setup_graph(1, *gt))) return rc;
+    if (link_gbs > 0) {
+        h2d_gbs = link_gbs;
+    } else {
+        // PCIe host->device bandwidth of one pinned page copy
+        cudaEvent_t a, b;
+        SCAPH_CUDA(cudaEventCreate(&a));
+        SCAPH_CUDA(cudaEventCreate(&b));
+        const size_t bytes = slot_words * 4;
+        SCAPH_CUDA(cudaMemcpyAsync(pool, g->page(0), bytes, cudaMemcpyHostToDevice, cst[0]));
+        SCAPH_CUDA(cudaEventRecord(a, cst[0]));
+        SCAPH_CUDA(cudaMemcpyAsync(pool, g->page(0), bytes, cudaMemcpyHostToDevice, cst[0]));
+        SCAPH_CUDA(cudaEventRecord(b, cst[0]));
+        SCAPH_CUDA(cudaEventSynchronize(b));
+        float ms = 0;
+        cudaEventElapsedTime(&ms, a, b);
+        if (ms > 0) h2d_gbs = bytes / (ms * 1e-3) / 1e9;
+        cudaEventDestroy(a);
+        cudaEventDestroy(b);
+    }
+    size_t maxp = g->pages.size() + (gt ? gt->pages.size() : 0);
     rl_words = 64 * (3 * maxp + 8);
     SCAPH_CUDA(cudaMallocHost(&h_rl, rl_words * 4));
     SCAPH_CUDA(cudaMalloc(&d_rl, rl_words * 4));
@@ -275,13 +328,13 @@ int Pager::acquire_slot(int gid, bool for_prefetch)
         const Slot &s = slots[i];
         if (s.g < 0) return i;
         if (gs[s.g].protect[s.p] == stamp) continue;
-        if (for_prefetch && s.used + 1 >= clock) continue;  // keep what the last level used
+        if (for_prefetch) continue;  // prefetches take free slots only
         if (best < 0 || s.used < slots[best].used) best = i;
     }
     return best;
 }
 
-int Pager::load(int gid, int p, cudaStream_t compute, bool prefetch_only)
+int Pager::load(int gid, int p, bool prefetch_only)
 {
     GState &G = gs[gid];
     const int si = acquire_slot(gid, prefetch_only);
@@ -290,7 +343,6 @@ int Pager::load(int gid, int p, cudaStream_t compute, bool prefetch_only)
     if (s.g >= 0) gs[s.g].slot_of[s.p] = -1;
     // the copy may not overwrite the slot before the kernels that read its
     // previous page are done (a never-recorded event is already complete)
-    (void)compute;
     cudaStream_t cs = cst[next_cst];
     next_cst = (next_cst + 1) % ncst;
     cudaStreamWaitEvent(cs, s.last_use, 0);
@@ -336,8 +388,7 @@ int Pager::publish(int gid, const std::vector<int> &pages, cudaStream_t st)
     return flush();
 }
 
-int Pager::launch(int dir, int gid, bool zc, const std::vector<int> &pages, scaph_engine *e, const BfsDev &s,
-                  cudaStream_t st)
+int Pager::launch(int gid, bool zc, const std::vector<int> &pages, const PageLaunch &fn, cudaStream_t st)
 {
     if (pages.empty()) return SCAPH_OK;
     GState &G = gs[gid];
@@ -368,15 +419,8 @@ int Pager::launch(int dir, int gid, bool zc, const std::vector<int> &pages, scap
     SCAPH_CUDA(cudaMemcpyAsync(d, h, (3 * n + 1) * 4, cudaMemcpyHostToDevice, st));
     rl_head += 3 * n + 1;
     RangeList rl{d, d + n, d + 2 * n, n};
-    const GraphDev &gv = zc ? G.zc : G.view;
-    const int grid = dir == 0 ? e->grid_push : e->grid_pull;
-    SCAPH_CUDA(run_ranges(dir, e->block, grid, gv, s, rl, st));
-    if (dir == 0) {
-        // the giant chunks reference this view's pool: run them now, then
-        // reset the chunk count for the next batch
-        SCAPH_CUDA(run_giant(e->block, grid, gv, s, st));
-        SCAPH_CUDA(cudaMemsetAsync(&s.ctr->giant, 0, sizeof(unsigned int), st));
-    }
+    int rc = fn.run(zc ? G.zc : G.view, gid, rl, t, st);
+    if (rc) return rc;
     if (!zc) {
         for (int p : pages) {
             const int si = G.slot_of[p];
@@ -388,15 +432,14 @@ int Pager::launch(int dir, int gid, bool zc, const std::vector<int> &pages, scap
     return SCAPH_OK;
 }
 
-int Pager::run_level(scaph_engine *e, int dir, const BfsDev &s, const std::vector<int> &needed,
-                     const std::vector<uint32_t> &datas, cudaStream_t st)
+int Pager::run_level(int gid, const std::vector<int> &needed, const std::vector<uint32_t> &datas,
+                     int compact_threshold, const PageLaunch &fn, cudaStream_t st)
 {
-    const int gid = (dir == 0 || ngraphs == 1) ? 0 : 1;
     GState &G = gs[gid];
     clock++;
     stamp++;
     level_h2d = 0;
-    const uint64_t thresh = (uint64_t)e->cfg.compact_threshold * (pagesize / 32);
+    const uint64_t thresh = (uint64_t)compact_threshold * (pagesize / 32);
     std::vector<int> resident, zcp, fetch;
     for (int p : needed) G.protect[p] = stamp;
     for (int p : needed) {
@@ -411,8 +454,8 @@ int Pager::run_level(scaph_engine *e, int dir, const BfsDev &s, const std::vecto
     }
     int rc = publish(gid, resident, st);
     if (rc) return rc;
-    if ((rc = launch(dir, gid, false, resident, e, s, st))) return rc;
-    if ((rc = launch(dir, gid, true, zcp, e, s, st))) return rc;
+    if ((rc = launch(gid, false, resident, fn, st))) return rc;
+    if ((rc = launch(gid, true, zcp, fn, st))) return rc;
     for (int p : zcp) zc_bytes += (uint64_t)datas[p] * 4;
     // demand fetches, in batches that start as soon as their copies land
     std::vector<int> done_pages = resident;
@@ -421,7 +464,7 @@ int Pager::run_level(scaph_engine *e, int dir, const BfsDev &s, const std::vecto
     while (i < fetch.size()) {
         std::vector<int> b;
         while (b.size() < batch && i < fetch.size()) {
-            if (load(gid, fetch[i], st, false) < 0) break;
+            if (load(gid, fetch[i], false) < 0) break;
             b.push_back(fetch[i]);
             faults++;
             i++;
@@ -435,18 +478,18 @@ int Pager::run_level(scaph_engine *e, int dir, const BfsDev &s, const std::vecto
             continue;
         }
         if ((rc = publish(gid, b, st))) return rc;
-        if ((rc = launch(dir, gid, false, b, e, s, st))) return rc;
+        if ((rc = launch(gid, false, b, fn, st))) return rc;
         done_pages.insert(done_pages.end(), b.begin(), b.end());
     }
     return SCAPH_OK;
 }
 
-int Pager::prefetch(int gid, const std::vector<int> &pages, cudaStream_t st)
+int Pager::prefetch(int gid, const std::vector<int> &pages)
 {
     GState &G = gs[gid];
     for (int p : pages) {
         if (p < 0 || p >= (int)G.slot_of.size() || G.slot_of[p] >= 0) continue;
-        if (load(gid, p, st, true) < 0) break;
+        if (load(gid, p, true) < 0) break;
         prefetched++;
     }
     return SCAPH_OK;
@@ -455,10 +498,10 @@ int Pager::prefetch(int gid, const std::vector<int> &pages, cudaStream_t st)
 // ---------------------------------------------------------------------------
 // engine glue
 // ---------------------------------------------------------------------------
-int pager_create(scaph_engine *e, int nslots, Pager **out)
+int pager_create(const Graph *g, const Graph *gt, int nslots, int copy_streams, float link_gbs, Pager **out)
 {
     Pager *p = new Pager();
-    int rc = p->init(e, nslots, e->cfg.copy_streams > 0 ? e->cfg.copy_streams : 2);
+    int rc = p->init(g, gt, nslots, copy_streams > 0 ? copy_streams : 2, link_gbs);
     if (rc) {
         delete p;
         return rc;
@@ -491,9 +534,7 @@ int pager_needs(scaph_engine *e, Pager *pg, int dir, int level, uint32_t src, st
         SCAPH_CUDA(cudaMemcpyAsync(G.h_cnt, h, np * 4, cudaMemcpyDeviceToHost, e->st));
         SCAPH_CUDA(cudaMemcpyAsync(G.h_datas, h + np, np * 4, cudaMemcpyDeviceToHost, e->st));
     } else {
-        k_page_unvisited<<<std::min(np, e->num_sms * 8), 256, 0, e->st>>>(e->d_visited, G.d_tab, np, e->V, e->d_indeg,
-                                                                         G.d_cnt, G.d_datas);
-        SCAPH_CUDA(cudaGetLastError());
+        SCAPH_CUDA(page_unvisited(G.view, e->d_visited, e->d_indeg, G.d_cnt, G.d_datas, e->num_sms * 4, e->st));
         SCAPH_CUDA(cudaMemcpyAsync(G.h_cnt, G.d_cnt, np * 4, cudaMemcpyDeviceToHost, e->st));
         SCAPH_CUDA(cudaMemcpyAsync(G.h_datas, G.d_datas, np * 4, cudaMemcpyDeviceToHost, e->st));
     }
@@ -510,12 +551,50 @@ int pager_needs(scaph_engine *e, Pager *pg, int dir, int level, uint32_t src, st
 int pager_run_level(scaph_engine *e, Pager *pg, int dir, const BfsDev &s, const std::vector<int> &needed,
                     const std::vector<uint32_t> &datas)
 {
-    return pg->run_level(e, dir, s, needed, datas, e->st);
+    const int gid = (dir == 0 || pg->ngraphs == 1) ? 0 : 1;
+    PageLaunch fn;
+    fn.run = [&](const GraphDev &gv, int, const RangeList &rl, uint32_t, cudaStream_t st) -> int {
+        const int grid = dir == 0 ? e->grid_push : e->grid_pull;
+        SCAPH_CUDA(run_ranges(dir, e->block, grid, gv, s, rl, st));
+        if (dir == 0) {
+            // the giant chunks reference this view's pool: run them now,
+            // then reset the chunk count for the next batch
+            SCAPH_CUDA(run_giant(e->block, grid, gv, s, st));
+            SCAPH_CUDA(cudaMemsetAsync(&s.ctr->giant, 0, sizeof(unsigned int), st));
+        }
+        return SCAPH_OK;
+    };
+    return pg->run_level(gid, needed, datas, e->cfg.compact_threshold, fn, e->st);
 }
 
-int pager_prefetch(scaph_engine *e, Pager *pg, int gid, const std::vector<int> &pages)
+int pager_run_level(Pager *pg, int gid, const std::vector<int> &needed, const std::vector<uint32_t> &datas,
+                    int compact_threshold, const PageLaunch &fn, cudaStream_t st)
 {
-    return pg->prefetch(gid, pages, e->st);
+    return pg->run_level(gid, needed, datas, compact_threshold, fn, st);
+}
+
+int pager_prefetch(scaph_engine *, Pager *pg, int gid, const std::vector<int> &pages)
+{
+    return pg->prefetch(gid, pages);
+}
+
+int pager_page_counts(Pager *pg, int gid, const uint32_t *bits, bool invert, const uint32_t *deg, uint32_t ew,
+                      int grid, cudaStream_t st, std::vector<int> &needed, std::vector<uint32_t> &datas)
+{
+    Pager::GState &G = pg->gs[gid];
+    const int np = (int)G.host->pages.size();
+    SCAPH_CUDA(page_counts(G.view, bits, invert, deg, ew, G.d_cnt, G.d_datas, grid, st));
+    SCAPH_CUDA(cudaMemcpyAsync(G.h_cnt, G.d_cnt, np * 4, cudaMemcpyDeviceToHost, st));
+    SCAPH_CUDA(cudaMemcpyAsync(G.h_datas, G.d_datas, np * 4, cudaMemcpyDeviceToHost, st));
+    SCAPH_CUDA(cudaStreamSynchronize(st));
+    needed.clear();
+    datas.assign(np, 0);
+    for (int p = 0; p < np; p++)
+        if (G.h_cnt[p]) {
+            needed.push_back(p);
+            datas[p] = G.h_datas[p];
+        }
+    return SCAPH_OK;
 }
 
 void pager_counters(const Pager *pg, uint64_t *h2d, uint64_t *zc, uint64_t *faults, uint64_t *prefetched,
@@ -552,12 +631,33 @@ float pager_resident_fraction(const Pager *pg, int gid, const std::vector<int> *
     return G.slot_of.empty() ? 1.f : (float)r / (float)G.slot_of.size();
 }
 
+double pager_transfer_ms(const Pager *pg, int gid, const uint32_t *cnt, const uint32_t *datas, int npages,
+                         int compact_threshold)
+{
+    const Pager::GState &G = pg->gs[gid];
+    const uint64_t thresh = (uint64_t)compact_threshold * (pg->pagesize / 32);
+    double bytes = 0;
+    for (int p = 0; p < npages && p < (int)G.slot_of.size(); p++) {
+        if (!cnt[p] || G.slot_of[p] >= 0) continue;
+        bytes += datas[p] <= thresh ? 4.0 * datas[p] : 4.0 * pg->slot_words;
+    }
+    return bytes / (pg->h2d_gbs * 1e9) * 1e3;
+}
+
+cudaError_t page_counts(const GraphDev &g, const uint32_t *bits, bool invert, const uint32_t *deg, uint32_t ew,
+                        uint32_t *cnt, uint32_t *datas, int grid, cudaStream_t st)
+{
+    cudaError_t e = cudaMemsetAsync(cnt, 0, sizeof(uint32_t) * g.npages, st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(datas, 0, sizeof(uint32_t) * g.npages, st);
+    if (e != cudaSuccess) return e;
+    k_page_counts<<<grid, 256, 0, st>>>(bits, invert ? ~0u : 0u, g, deg, ew, cnt, datas);
+    return cudaGetLastError();
+}
+
 cudaError_t page_unvisited(const GraphDev &g, const uint32_t *visited, const uint32_t *indeg, uint32_t *cnt,
                            uint32_t *datas, int grid, cudaStream_t st)
 {
-    k_page_unvisited<<<std::max(1, std::min((int)g.npages, grid)), 256, 0, st>>>(visited, g.pages, g.npages, g.V,
-                                                                                indeg, cnt, datas);
-    return cudaGetLastError();
+    return page_counts(g, visited, true, indeg, 1, cnt, datas, grid, st);
 }
 
 }  // namespace scaph

@@ -43,6 +43,8 @@ class Trace:
     mu: np.ndarray           # unexplored edges per level
     out_need: list           # out-pages a push would read, per level
     in_need: list            # in-pages a pull would read, per level
+    out_datas: list          # their active words sum(deg+3), per level
+    in_datas: list
     next_active: np.ndarray  # levels x P: out-page holds frontier at the next level
 
 
@@ -58,21 +60,32 @@ def collect(g: PagedGraph, gt: PagedGraph | None, sources, **engine_kw) -> list[
         F = eng.features()
         L = len(tr)
         nxt = np.zeros((L, P), np.float32)
-        out_need = []
+        out_need, out_datas = [], []
+        deg_src = int(g.degree()[int(s)])
         for lvl in range(L):
             hn, _ = eng.page_hist(lvl + 1)  # frontier of level lvl+1
             nxt[lvl] = hn > 0
             if lvl == 0:
-                out_need.append(np.flatnonzero(F[0, G:] > 0))
+                pages = np.flatnonzero(F[0, G:] > 0)
+                out_need.append(pages)
+                out_datas.append(np.full(len(pages), deg_src + 3, np.int64))
             else:
-                hp, _ = eng.page_hist(lvl)
-                out_need.append(np.flatnonzero(hp > 0))
-        in_need = [np.flatnonzero(eng.pull_pages(lvl, npi) > 0) for lvl in range(L)]
+                hp, hd = eng.page_hist(lvl)
+                pages = np.flatnonzero(hp > 0)
+                out_need.append(pages)
+                out_datas.append(hd[pages].astype(np.int64))
+        in_need, in_datas = [], []
+        for lvl in range(L):
+            c, d = eng.pull_pages(lvl, npi)
+            pages = np.flatnonzero(c > 0)
+            in_need.append(pages)
+            in_datas.append(d[pages].astype(np.int64))
         push = np.array([t["push_ms"] for t in tr])
         pull = np.array([t["pull_ms"] if lvl > 0 else np.inf for lvl, t in enumerate(tr)])
         out.append(Trace(int(s), F, push, pull, np.array([t["frontier"] for t in tr], np.float64),
                          np.array([t["frontier_edges"] for t in tr], np.float64),
-                         np.array([t["unvisited_edges"] for t in tr], np.float64), out_need, in_need, nxt))
+                         np.array([t["unvisited_edges"] for t in tr], np.float64), out_need, in_need, out_datas,
+                         in_datas, nxt))
     eng.close()
     return out
 
@@ -130,14 +143,35 @@ def sequences(L: int):
 
 
 def label(tr: Trace, nslots: int, page_ms: float, V: int, n_out: int, n_in: int, symmetric: bool,
-          alpha=14.0, beta=24.0):
+          alpha=14.0, beta=24.0, resident=False, zc_words=None, page_words=None):
     """Cheapest sequence under the cost model; returns (dirs, feature rows
-    recomputed along it, its cost, alpha/beta's cost)."""
+    recomputed along it, its cost, alpha/beta's cost).  resident=True: the
+    graph is all in HBM (no page traffic, residency features 1).  Pages whose
+    active words are at most zc_words (the engine's compact threshold) are
+    read zero-copy at their byte cost instead of being copied, as the engine
+    does."""
     L = len(tr.push_ms)
     gin = 0 if symmetric else 1
+    if resident:
+        page_ms = 0.0
+        nslots = n_out + n_in
+    words_ms = page_ms / page_words if page_words else 0.0
+
+    def need(gid, pages, datas, sim):
+        """Cost of one level's pages: zero-copy the sparse non-resident ones."""
+        big, zc = [], 0
+        for p, d in zip(pages, datas):
+            if zc_words is not None and d <= zc_words and (gid, int(p)) not in sim.slot:
+                zc += int(d)
+            else:
+                big.append(p)
+        return sim.touch(gid, big) * page_ms + zc * words_ms
 
     def cost(seq, want_rows=False):
         sim = PoolSim(nslots)
+        if resident:
+            for gid, npg in ((0, n_out), (gin, n_in)):
+                sim.touch(gid, range(npg))
         total = 0.0
         rows = tr.feats.copy() if want_rows else None
         for lvl in range(L):
@@ -152,8 +186,10 @@ def label(tr: Trace, nslots: int, page_ms: float, V: int, n_out: int, n_in: int,
                 rows[lvl, 14] = 0 if lvl == 0 else alpha_beta(prev, tr.nf[lvl], tr.nf[lvl - 1], tr.mf[lvl],
                                                              tr.mu[lvl], V, alpha, beta)
             k = tr.push_ms[lvl] if d == 0 else tr.pull_ms[lvl]
-            fetched = sim.touch(0, tr.out_need[lvl]) if d == 0 else sim.touch(gin, tr.in_need[lvl])
-            total += k + fetched * page_ms
+            if d == 0:
+                total += k + need(0, tr.out_need[lvl], tr.out_datas[lvl], sim)
+            else:
+                total += k + need(gin, tr.in_need[lvl], tr.in_datas[lvl], sim)
         return total, rows
 
     # alpha/beta's own sequence
@@ -170,27 +206,34 @@ def label(tr: Trace, nslots: int, page_ms: float, V: int, n_out: int, n_in: int,
     return np.array(best, np.float32), rows, best_cost, ab_cost
 
 
-def dataset(traces, nslots, page_ms, V, n_out, n_in, symmetric, w_dir=1.0, w_page=0.5):
+def dataset(traces, nslots, page_ms, V, n_out, n_in, symmetric, w_dir=1.0, w_page=0.5, zc_words=None,
+            page_words=None):
+    """Training rows: the direction labels are the kernel-time optimum of
+    the resident graph (the engine adds the exact page-traffic cost of each
+    direction itself when it runs out of core)."""
     Xs, Ts, Ws = [], [], []
     for tr in traces:
-        dirs, rows, _, _ = label(tr, nslots, page_ms, V, n_out, n_in, symmetric)
-        L = len(dirs)
-        T = np.concatenate([dirs[:, None], tr.next_active], axis=1)
-        W = np.zeros_like(T)
-        W[1:, 0] = w_dir  # level 0 is always push
-        W[:, 1:] = w_page / n_out
-        Xs.append(rows)
-        Ts.append(T)
-        Ws.append(W)
+        for resident in (True,):
+            dirs, rows, _, _ = label(tr, nslots, page_ms, V, n_out, n_in, symmetric, resident=resident,
+                                     zc_words=zc_words, page_words=page_words)
+            T = np.concatenate([dirs[:, None], tr.next_active], axis=1)
+            W = np.zeros_like(T)
+            W[1:, 0] = w_dir  # level 0 is always push
+            W[:, 1:] = w_page / n_out
+            Xs.append(rows)
+            Ts.append(T)
+            Ws.append(W)
     X, T, W = np.concatenate(Xs), np.concatenate(Ts), np.concatenate(Ws)
     W /= len(X)
     return X.astype(np.float32), T.astype(np.float32), W.astype(np.float32)
 
 
 def train(traces, g: PagedGraph, gt: PagedGraph | None, nslots: int, page_ms: float, epochs=300, lr=3e-3,
-          seed=7, device=0) -> tuple[Mlp, dict]:
+          seed=7, device=0, compact_threshold=3) -> tuple[Mlp, dict]:
     n_out, n_in = g.npages, (gt or g).npages
-    X, T, W = dataset(traces, nslots, page_ms, g.V, n_out, n_in, gt is None)
+    zc_words = compact_threshold * (g.pagesize // 32)
+    X, T, W = dataset(traces, nslots, page_ms, g.V, n_out, n_in, gt is None, zc_words=zc_words,
+                      page_words=g.pagesize)
     net = Mlp(G + n_out, 1 + n_out, seed=seed, device=device)
     loss0, _ = net.loss_grad(X, T, W)
     loss = net.train(X, T, W, epochs=epochs, batch=min(256, len(X)), lr=lr, seed=seed)

@@ -40,5 +40,27 @@ def config2(scale: int = 24, nsrc: int = 64):
     return csr, random_sources(csr, nsrc, SEED_BASE + 1)
 
 
+def config3(V: int = 41_600_000, E: int = 1_470_000_000, max_degree: int = 1 << 20):
+    """Directed power-law graph: out-degree Zipf s=1.9 (capped so that every
+    adjacency list fits a 10 Mi-word page), destinations by preferential
+    attachment; returns (out-edge CSR, in-edge CSR)."""
+    csr = Csr.powerlaw(V, E, 1.9, max_degree, seed=SEED_BASE + 2)
+    return csr, csr.transpose()
+
+
+def config4a(scale: int = 25):
+    """RMAT scale 25, ef 16, 64 sources per launch."""
+    csr = rmat(scale, 16, 3)
+    return csr, random_sources(csr, 64, SEED_BASE + 3)
+
+
+def config5(V: int = 105_000_000, E: int = 3_700_000_000, max_degree: int = 1 << 20):
+    """Directed web-crawl-like graph: out-degree power law s=2.1, 90 % of the
+    edges inside the source's block of 4096 consecutive ids, the rest uniform;
+    returns (out-edge CSR, in-edge CSR)."""
+    csr = Csr.web(V, E, 2.1, max_degree, 4096, 0.9, seed=SEED_BASE + 4)
+    return csr, csr.transpose()
+
+
 def paged(csr: Csr, pagesize_words: int = PAGESIZE_WORDS) -> PagedGraph:
     return PagedGraph.from_csr(csr, pagesize_words)

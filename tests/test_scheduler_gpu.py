@@ -42,8 +42,9 @@ def test_learned_scheduler_beats_alpha_beta_out_of_core(setup):
     traces = scheduler.collect(g, gt, train)
     net, info = scheduler.train(traces, g, gt, nslots, page_ms, epochs=300)
     assert info["loss"] < info["loss0"] and info["direction_accuracy"] > 0.8, info
+    link_gbs = g.pagesize * 4 / (page_ms * 1e-3) / 1e9  # the modelled link
     plain = scheduler.evaluate(g, gt, held, None, pool)
-    learned = scheduler.evaluate(g, gt, held, net, pool)
+    learned = scheduler.evaluate(g, gt, held, net, pool, link_gbs=link_gbs)
     for s, a, b in zip(held, plain["depths"], learned["depths"]):
         ref = O.bfs(csr.idx, csr.ngh, s)
         assert np.array_equal(a, ref) and np.array_equal(b, ref)
@@ -54,3 +55,23 @@ def test_learned_scheduler_beats_alpha_beta_out_of_core(setup):
           f"modelled {cost_learned:.1f} ms; training {info}")
     assert learned["page_faults"] + learned["prefetched"] < plain["page_faults"]
     assert cost_learned < cost_plain
+
+
+def test_learned_graph_mode_in_hbm_is_exact_and_matches_host_loop(setup):
+    """Resident graph: the learned decision runs on the device inside the
+    CUDA-graph traversal; same directions as the host-loop learned engine."""
+    csr, g, gt, train, held = setup
+    traces = scheduler.collect(g, gt, train[:6])
+    net, _ = scheduler.train(traces, g, gt, 64, 0.5, epochs=100)
+    eg = S.Engine(g, gt, direction=S.DIR_LEARNED)
+    eg.set_scheduler(net)
+    eh = S.Engine(g, gt, direction=S.DIR_LEARNED, use_graph=2)
+    eh.set_scheduler(net)
+    for s in held[:4]:
+        dg, _, _ = eg.bfs(s)
+        dh, _, _ = eh.bfs(s)
+        ref = O.bfs(csr.idx, csr.ngh, s)
+        assert np.array_equal(dg, ref) and np.array_equal(dh, ref)
+        assert [t["direction"] for t in eg.trace()] == [t["direction"] for t in eh.trace()]
+    eg.close()
+    eh.close()
