@@ -133,6 +133,13 @@ const scaph_page_info *scaph_graph_page_list(const scaph_graph *g);
 /* Per-vertex out-degree (u32[V]), the reference's csr_deg / d_degree. */
 const uint32_t *scaph_graph_degree(const scaph_graph *g);
 void scaph_graph_close(scaph_graph *g);
+/* The flat CSR of a paged graph, read back from its pages (the arrays that
+ * fetch_graph reads from <p>_csr.idx/.ngh/.wgh, src/graph.h:27-75; wgh only
+ * for weighted pages).  Free with scaph_csr_free. */
+int scaph_graph_to_csr(const scaph_graph *g, scaph_csr *out);
+/* 1 if every edge u->v has its reverse v->u (same multiset of neighbours),
+ * 0 if not, < 0 on error. */
+int scaph_csr_symmetric(const scaph_csr *csr);
 
 /* ---- engine ------------------------------------------------------------ */
 
@@ -302,6 +309,73 @@ int scaph_msbfs(scaph_engine *e, const uint32_t *srcs, int nsrc, uint32_t *depth
 /* Per-level trace of the last scaph_msbfs (frontier = vertices with a
  * nonzero mask; next = vertices newly reached by any source). */
 int scaph_msbfs_trace(scaph_engine *e, scaph_level_trace *out, int cap);
+
+/* ---- page store for App-hook engines ------------------------------------ */
+
+/* The reference's apps supply a vertex program as device hooks
+ * (cond/update, app/bfs_kernel.cuh:6-16, app/sssp_kernel.cuh:6-16,
+ * app/wcc_kernel.cuh:5-15) that App<> runs over the pages of the graph
+ * (gpu_push_csr, src/gpu_engine.cuh:41-169, scheduled by App::gpu_push_batch
+ * and App::PageCopy, src/app.cuh:371-468).  Here the application compiles
+ * its hooks into its own kernels (include/scaph/compat/app.cuh does this for
+ * the reference's apps) and the store hands it pages to run them on.
+ *
+ * A store keeps the graph's pages (weighted {ngr,wgh} pages too) on the
+ * device: all of them, or - when pool_bytes is smaller than the pages - a
+ * pool of pool_bytes of them managed like the BFS engine's out-of-core pool
+ * (zero-copy reads of pages whose active words are at most
+ * compact_threshold/32 of a page; demand copies on copy_streams streams). */
+typedef struct scaph_store scaph_store;
+
+/* Device page table entry: page p's words start at pool + base; it holds
+ * the vertices left .. left+nodenum-1 (Node{vtx,idx,len} triples, then the
+ * edges; idx counts edges, an edge being 1 word, or 2 when weighted). */
+typedef struct scaph_page_dev {
+    uint64_t base;
+    uint32_t left;
+    uint32_t nodenum;
+} scaph_page_dev;
+
+/* What a batch of pages looks like to the application's kernels. */
+typedef struct scaph_page_view {
+    const uint32_t       *pool;    /* device words                            */
+    const scaph_page_dev *pages;   /* device, npages + 1 (pages[npages].left = V) */
+    const uint32_t       *coarse;  /* device: coarse[v >> cshift] = a page at
+                                      or before the page holding v          */
+    uint32_t cshift, npages, V, pagesize, weighted;
+} scaph_page_view;
+
+/* The vertices of a batch: n ranges [lo[i], hi[i]) (device arrays).  Range
+ * i owns the tiles tile0[i] .. tile0[i+1]-1 (tile0[n] need not exist; tiles
+ * = the total): tile t of range i covers the 4096 vertices starting at
+ * 32 * (lo[i] / 32 + 128 * (t - tile0[i])). */
+typedef struct scaph_ranges {
+    const uint32_t *lo, *hi, *tile0;
+    uint32_t n, tiles;
+} scaph_ranges;
+
+/* Launches the application's kernels for one batch on `stream` (a
+ * cudaStream_t); returns 0, or a nonzero code that the level returns. */
+typedef int (*scaph_batch_fn)(void *user, const scaph_page_view *view,
+                              const scaph_ranges *ranges, void *stream);
+
+int scaph_store_create(const scaph_graph *g, int64_t pool_bytes, int compact_threshold,
+                       int copy_streams, int device, scaph_store **s);
+int scaph_store_destroy(scaph_store *s);
+/* 1 when every page is resident (then scaph_store_view gives the one view). */
+int scaph_store_resident(const scaph_store *s);
+int scaph_store_view(const scaph_store *s, scaph_page_view *out);
+/* Out-degrees on the device, u32[V] (the reference's d_degree). */
+const uint32_t *scaph_store_degree(const scaph_store *s);
+/* One round over the active vertices (device bitmap, V bits): calls fn for
+ * every batch of pages that hold active vertices, on `stream` or, out of
+ * core, on streams ordered after `stream`'s prior work and before its later
+ * work.  Out of core it synchronises `stream` once to read the page counts. */
+int scaph_store_level(scaph_store *s, const uint32_t *d_active, scaph_batch_fn fn,
+                      void *user, void *stream);
+/* Page bytes copied, read zero-copy, and demand copies, since create. */
+int scaph_store_counters(const scaph_store *s, uint64_t *h2d_bytes, uint64_t *zc_bytes,
+                         uint64_t *page_faults);
 
 /* ---- BFS without device allocation -------------------------------------- */
 

@@ -332,3 +332,139 @@ uint32_t oracle_set_run(uint32_t mark, int off, int n, int value) /* tools.h:67-
     }
     return mark;
 }
+
+/* ------------------------------------------------------------------------ */
+/* App-hook vertex programs (the reference's apps).                          */
+/*                                                                           */
+/* oracle_hook_fixpoint restates what App::run computes for an app's hooks   */
+/* (src/app.cuh:220-265 driving gpu_push_csr, src/gpu_engine.cuh:95-160):    */
+/* every active vertex v pushes value[v] along its edges; an edge to u fires */
+/* when cond(value[v], value[u][, w]) holds and then update() lowers         */
+/* value[u] and makes u active; the run ends when no vertex is active.  The  */
+/* hooks, in 32-bit unsigned arithmetic as on the GPU:                       */
+/*   app 0 BFS  cond d > s + 1,  update d = s + 1   (app/bfs_kernel.cuh:6-16)  */
+/*   app 1 SSSP cond d > s + w,  update d = s + w   (app/sssp_kernel.cuh:6-16) */
+/*   app 2 WCC  cond d > s,      update d = s       (app/wcc_kernel.cuh:5-15)  */
+/* Active vertices are processed first-in first-out; for these min-updates   */
+/* the fixed point does not depend on the order.  `active` (V bytes) is the  */
+/* initial stat[] of gpu_init.  Returns the vertices processed, -1 on error. */
+/* ------------------------------------------------------------------------ */
+int64_t oracle_hook_fixpoint(uint32_t V, const uint64_t *idx, const uint32_t *ngh,
+                             const uint32_t *wgh, int app, uint32_t *value,
+                             const uint8_t *active)
+{
+    if (app < 0 || app > 2 || (app == 1 && !wgh)) return -1;
+    uint32_t *q = (uint32_t *)malloc(sizeof(uint32_t) * ((size_t)V + 1));
+    uint8_t *inq = (uint8_t *)calloc((size_t)V + 1, 1);
+    if (!q || !inq) { free(q); free(inq); return -1; }
+    size_t head = 0, n = 0;                     /* ring of V+1 slots */
+    const size_t cap = (size_t)V + 1;
+    for (uint32_t v = 0; v < V; v++)
+        if (active[v]) { q[n++] = v; inq[v] = 1; }
+    int64_t processed = 0;
+    while (n) {
+        const uint32_t v = q[head];
+        head = (head + 1) % cap;
+        n--;
+        inq[v] = 0;
+        processed++;
+        const uint32_t s = value[v];
+        for (uint64_t e = idx[v]; e < idx[v + 1]; e++) {
+            const uint32_t u = ngh[e];
+            const uint32_t cand = app == 0 ? s + 1u : app == 1 ? s + wgh[e] : s;
+            if (value[u] > cand) {
+                value[u] = cand;
+                if (!inq[u]) {
+                    q[(head + n) % cap] = u;
+                    n++;
+                    inq[u] = 1;
+                }
+            }
+        }
+    }
+    free(q);
+    free(inq);
+    return processed;
+}
+
+/* Independent checks of oracle_hook_fixpoint (not restatements of the      */
+/* reference; textbook algorithms that must agree with it):                  */
+/* Dijkstra from src with a binary heap over 64-bit distances, then values   */
+/* at or above `far` reported as `far` (what the SSSP hooks leave there when */
+/* every vertex starts at far, weights < 2^31).                              */
+int oracle_sssp_dijkstra(uint32_t V, const uint64_t *idx, const uint32_t *ngh,
+                         const uint32_t *wgh, uint32_t src, uint32_t far, uint32_t *value)
+{
+    if (src >= V) return -1;
+    uint64_t *dist = (uint64_t *)malloc(sizeof(uint64_t) * (size_t)V);
+    uint64_t *hk = (uint64_t *)malloc(sizeof(uint64_t) * ((size_t)idx[V] + 1));
+    uint32_t *hv = (uint32_t *)malloc(sizeof(uint32_t) * ((size_t)idx[V] + 1));
+    if (!dist || !hk || !hv) { free(dist); free(hk); free(hv); return -1; }
+    for (uint32_t v = 0; v < V; v++) dist[v] = UINT64_MAX;
+    size_t hn = 0;
+    dist[src] = 0;
+    hk[0] = 0; hv[0] = src; hn = 1;
+    while (hn) {
+        const uint64_t d = hk[0];
+        const uint32_t v = hv[0];
+        /* pop */
+        hn--;
+        if (hn) {
+            uint64_t k = hk[hn]; uint32_t x = hv[hn];
+            size_t i = 0;
+            for (;;) {
+                size_t c = 2 * i + 1;
+                if (c >= hn) break;
+                if (c + 1 < hn && hk[c + 1] < hk[c]) c++;
+                if (hk[c] >= k) break;
+                hk[i] = hk[c]; hv[i] = hv[c]; i = c;
+            }
+            hk[i] = k; hv[i] = x;
+        }
+        if (d != dist[v]) continue;
+        for (uint64_t e = idx[v]; e < idx[v + 1]; e++) {
+            const uint32_t u = ngh[e];
+            const uint64_t nd = d + wgh[e];
+            if (nd < dist[u]) {
+                dist[u] = nd;
+                size_t i = hn++;
+                while (i) {
+                    size_t p = (i - 1) / 2;
+                    if (hk[p] <= nd) break;
+                    hk[i] = hk[p]; hv[i] = hv[p]; i = p;
+                }
+                hk[i] = nd; hv[i] = u;
+            }
+        }
+    }
+    for (uint32_t v = 0; v < V; v++) value[v] = dist[v] >= far ? far : (uint32_t)dist[v];
+    value[src] = 0;
+    free(dist); free(hk); free(hv);
+    return 0;
+}
+
+/* Smallest id that reaches each vertex along directed edges (itself         */
+/* included): what the WCC hooks leave when every vertex starts labelled by  */
+/* its id and active.  Sources in increasing order; a search stops at        */
+/* vertices already labelled (everything they reach is labelled already).    */
+int oracle_min_reaching_id(uint32_t V, const uint64_t *idx, const uint32_t *ngh, uint32_t *label)
+{
+    uint32_t *stack = (uint32_t *)malloc(sizeof(uint32_t) * ((size_t)V + 1));
+    if (!stack) return -1;
+    for (uint32_t v = 0; v < V; v++) label[v] = UINT32_MAX;
+    for (uint32_t s = 0; s < V; s++) {
+        if (label[s] != UINT32_MAX) continue;
+        size_t n = 0;
+        label[s] = s;
+        stack[n++] = s;
+        while (n) {
+            const uint32_t v = stack[--n];
+            for (uint64_t e = idx[v]; e < idx[v + 1]; e++) {
+                const uint32_t u = ngh[e];
+                if (label[u] == UINT32_MAX) { label[u] = s; stack[n++] = u; }
+            }
+        }
+    }
+    free(stack);
+    return 0;
+}

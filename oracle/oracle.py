@@ -54,6 +54,12 @@ def olib() -> C.CDLL:
         L.oracle_fit_zero_run.restype = i32
         L.oracle_set_run.argtypes = [u32, i32, i32, i32]
         L.oracle_set_run.restype = u32
+        L.oracle_hook_fixpoint.argtypes = [u32, vp, vp, vp, i32, vp, vp]
+        L.oracle_hook_fixpoint.restype = i64
+        L.oracle_sssp_dijkstra.argtypes = [u32, vp, vp, vp, u32, u32, vp]
+        L.oracle_sssp_dijkstra.restype = i32
+        L.oracle_min_reaching_id.argtypes = [u32, vp, vp, vp]
+        L.oracle_min_reaching_id.restype = i32
         _o = L
     return _o
 
@@ -156,3 +162,36 @@ def ref_bfs_check(idx32, ngh, src: int, values: np.ndarray):
     if rc != 0:
         raise RuntimeError("ref_bfs_check: could not parse the reference output")
     return err.value, sec.value
+
+
+HOOK_APPS = {"bfs": 0, "sssp": 1, "wcc": 2}
+
+
+def hook_fixpoint(idx, ngh, app: str, value, active, wgh=None) -> np.ndarray:
+    """Fixed point of an app's hooks (bfs / sssp / wcc) from the initial
+    values and active flags gpu_init() would leave; returns the values."""
+    idx, ngh = _csr(idx, ngh)
+    value = np.ascontiguousarray(value, np.uint32).copy()
+    active = np.ascontiguousarray(active, np.uint8)
+    w = None if wgh is None else np.ascontiguousarray(wgh, np.uint32)
+    n = olib().oracle_hook_fixpoint(len(idx) - 1, _p(idx), _p(ngh), _p(w), HOOK_APPS[app], _p(value), _p(active))
+    if n < 0:
+        raise ValueError("oracle_hook_fixpoint: bad arguments")
+    return value
+
+
+def sssp_dijkstra(idx, ngh, wgh, src: int, far: int = 0x7FFFFFFF) -> np.ndarray:
+    idx, ngh = _csr(idx, ngh)
+    wgh = np.ascontiguousarray(wgh, np.uint32)
+    out = np.zeros(len(idx) - 1, np.uint32)
+    if olib().oracle_sssp_dijkstra(len(idx) - 1, _p(idx), _p(ngh), _p(wgh), src, far, _p(out)) != 0:
+        raise ValueError("oracle_sssp_dijkstra failed")
+    return out
+
+
+def min_reaching_id(idx, ngh) -> np.ndarray:
+    idx, ngh = _csr(idx, ngh)
+    out = np.zeros(len(idx) - 1, np.uint32)
+    if olib().oracle_min_reaching_id(len(idx) - 1, _p(idx), _p(ngh), _p(out)) != 0:
+        raise ValueError("oracle_min_reaching_id failed")
+    return out

@@ -96,6 +96,8 @@ def lib() -> C.CDLL:
         "scaph_graph_page_list": ([vp], P(u32)),
         "scaph_graph_degree": ([vp], P(u32)),
         "scaph_graph_close": ([vp], None),
+        "scaph_graph_to_csr": ([vp, P(_Csr)], i32),
+        "scaph_csr_symmetric": ([P(_Csr)], i32),
         "scaph_engine_create": ([vp, vp, P(_Config), P(vp)], i32),
         "scaph_engine_destroy": ([vp], i32),
         "scaph_bfs": ([vp, u32, vp, vp, i32, P(_Stats)], i32),
@@ -223,6 +225,10 @@ class Csr:
         _check(lib().scaph_csr_read(prefix.encode(), int(with_weights), C.byref(g._c)))
         return g
 
+    def symmetric(self) -> bool:
+        """Whether every edge has its reverse (scaph_csr_symmetric)."""
+        return _check(lib().scaph_csr_symmetric(C.byref(self._c))) == 1
+
     def transpose(self) -> "Csr":
         t = Csr()
         _check(lib().scaph_csr_transpose(C.byref(self._c), C.byref(t._c)))
@@ -283,6 +289,12 @@ class PagedGraph:
 
     def degree(self) -> np.ndarray:
         return np.ctypeslib.as_array(lib().scaph_graph_degree(self._h), shape=(self.V,))
+
+    def to_csr(self) -> Csr:
+        """The flat CSR read back from the pages (scaph_graph_to_csr)."""
+        c = Csr()
+        _check(lib().scaph_graph_to_csr(self._h, C.byref(c._c)))
+        return c
 
 
 class Mlp:

@@ -380,4 +380,70 @@ const scaph_page_info *scaph_graph_page_list(const scaph_graph *g) { return g ? 
 const uint32_t *scaph_graph_degree(const scaph_graph *g) { return g ? g->degree.data() : nullptr; }
 void scaph_graph_close(scaph_graph *g) { delete g; }
 
-}  // extern "C"
+int scaph_graph_to_csr(const scaph_graph *g, scaph_csr *out)
+{
+    clear_error();
+    if (!g || !out) return set_error(SCAPH_EINVAL, "null argument");
+    memset(out, 0, sizeof(*out));
+    const uint32_t V = g->V;
+    const uint64_t E = g->E;
+    out->V = V;
+    out->E = E;
+    out->idx = (uint64_t *)malloc(sizeof(uint64_t) * ((size_t)V + 1));
+    out->ngh = (uint32_t *)malloc(sizeof(uint32_t) * std::max<uint64_t>(1, E));
+    if (g->weighted) out->wgh = (uint32_t *)malloc(sizeof(uint32_t) * std::max<uint64_t>(1, E));
+    if (!out->idx || !out->ngh || (g->weighted && !out->wgh)) {
+        scaph_csr_free(out);
+        return set_error(SCAPH_ENOMEM, "csr allocation");
+    }
+    out->idx[0] = 0;
+    for (uint32_t v = 0; v < V; v++) out->idx[v + 1] = out->idx[v] + g->degree[v];
+    if (out->idx[V] != E) {
+        scaph_csr_free(out);
+        return set_error(SCAPH_EFORMAT, "page degrees sum to %llu, graph.info says %llu",
+                         (unsigned long long)out->idx[V], (unsigned long long)E);
+    }
+    const uint32_t ew = g->weighted ? 2 : 1;
+    const int np = (int)g->pages.size();
+    #pragma omp parallel for schedule(dynamic, 1)
+    for (int p = 0; p < np; p++) {
+        const scaph_page_info &pi = g->pages[p];
+        const uint32_t *pg = g->page(p);
+        const uint32_t *edges = pg + 3ull * pi.nodenum;
+        for (uint32_t i = 0; i < pi.nodenum; i++) {
+            const uint32_t v = pg[3 * i], idx = pg[3 * i + 1], len = pg[3 * i + 2];
+            const uint64_t at = out->idx[v];
+            for (uint32_t k = 0; k < len; k++) {
+                out->ngh[at + k] = edges[(uint64_t)(idx + k) * ew];
+                if (ew == 2) out->wgh[at + k] = edges[(uint64_t)(idx + k) * 2 + 1];
+            }
+        }
+    }
+    return SCAPH_OK;
+}
+
+int scaph_csr_symmetric(const scaph_csr *csr)
+{
+    clear_error();
+    if (!csr || !csr->idx) return set_error(SCAPH_EINVAL, "null argument");
+    scaph_csr t;
+    int rc = scaph_csr_transpose(csr, &t);
+    if (rc) return rc;
+    int sym = 1;
+    for (uint32_t v = 0; v <= csr->V && sym; v++)
+        if (t.idx[v] != csr->idx[v]) sym = 0;
+    if (sym) {
+        // in-lists come out sorted: compare with each out-list sorted
+        #pragma omp parallel for schedule(dynamic, 1024) reduction(& : sym)
+        for (int64_t v = 0; v < (int64_t)csr->V; v++) {
+            const uint64_t b = csr->idx[v], e = csr->idx[v + 1];
+            std::vector<uint32_t> a(csr->ngh + b, csr->ngh + e);
+            std::sort(a.begin(), a.end());
+            if (!std::equal(a.begin(), a.end(), t.ngh + b)) sym = 0;
+        }
+    }
+    scaph_csr_free(&t);
+    return sym;
+}
+
+}  // extern "C""
