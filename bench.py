@@ -282,6 +282,63 @@ def extra_config4a(stream):
             "directions": "".join("p" if t["direction"] else "P" for t in tr)}
 
 
+def extra_config4b(stream):
+    """Mixed batch: 256 single-source queries over 32 RMAT graphs (scales
+    14-22, edge factors 8-32, drawn by seed) in one CUDA-graph launch with
+    autotuned parameters, against the plain engine running the same queries
+    one by one (one engine per graph, one graph launch per query)."""
+    import numpy as np
+    import torch
+
+    import scaph_b200 as S
+    from scaph_b200 import autotune, workloads
+
+    t0 = time.time()
+    graphs, queries, shapes = workloads.config4b()
+    gen_s = time.time() - t0
+    b = S.Batch(graphs, stream=stream.cuda_stream)
+    words = b.out_words(queries)
+    out = torch.empty(words, dtype=torch.int32, device="cuda")
+    with tempfile.TemporaryDirectory() as td:
+        tune = autotune.tune_batch(b, queries, out.data_ptr(), repeats=2, cache=os.path.join(td, "tune.json"))
+    runs = [b.run_device(queries, out.data_ptr()) for _ in range(5)]
+    ms_batch = min(r.ms for r in runs)
+    tr = b.trace()
+    # plain: one engine per graph, every query its own graph launch
+    engines = [S.Engine(S.PagedGraph.from_csr(g), stream=stream.cuda_stream) for g in graphs]
+    ref = torch.empty(words, dtype=torch.int32, device="cuda")
+    offs, o = [], 0
+    for gi, _ in queries:
+        offs.append(o)
+        o += graphs[gi].V
+    for (gi, s), off in zip(queries[:8], offs):
+        engines[gi].bfs_device(s, ref.data_ptr() + 4 * off)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for (gi, s), off in zip(queries, offs):
+        engines[gi].bfs_async(s, ref.data_ptr() + 4 * off)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms_plain = e0.elapsed_time(e1)
+    exact = bool(torch.equal(out, ref))
+    for e in engines:
+        e.close()
+    b.close()
+    teps = sum(graphs[gi].E for gi, _ in queries)
+    per_graph = np.bincount([gi for gi, _ in queries], minlength=len(graphs))
+    return {"graphs": len(graphs), "queries": len(queries), "V_total": sum(g.V for g in graphs),
+            "E_total": sum(g.E for g in graphs), "scales": [sc for sc, _ in shapes],
+            "edgefactors": [ef for _, ef in shapes], "max_queries_per_graph": int(per_graph.max()),
+            "graph_gen_s": round(gen_s, 1), "launches_per_batch": runs[-1].launches,
+            "batched_ms": ms_batch, "batched_gteps": teps / (ms_batch / 1e3) / 1e9,
+            "plain_ms": ms_plain, "plain_gteps": teps / (ms_plain / 1e3) / 1e9,
+            "speedup_vs_plain": ms_plain / ms_batch, "bit_exact_vs_plain": exact, "levels": len(tr),
+            "directions": "".join("p" if t["direction"] else "P" for t in tr),
+            "autotune": {"params": tune["params"], "default_ms": tune["default_ms"], "tuned_ms": tune["ms"],
+                         "candidates": tune["tried"], "seconds": round(tune["seconds"], 1)}}
+
+
 def _run_set(S, g, gt, srcs, pool, net=None, cold=False, warm_pass=True, **kw):
     """Times `srcs`; returns total ms, PCIe bytes, levels."""
     eng = S.Engine(g, gt, pool_bytes=pool, direction=S.DIR_LEARNED if net else 0, **kw)
@@ -481,6 +538,7 @@ def run_ours(args, world):
         extras = {}
         for name, fn in (("pcie", lambda: extra_pcie(stream)), ("config1", extra_config1),
                          ("config4a_batched", lambda: extra_config4a(stream)),
+                         ("config4b_mixed", lambda: extra_config4b(stream)),
                          ("config3_learned", extra_config3)):
             try:
                 extras[name] = fn()

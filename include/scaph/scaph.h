@@ -310,6 +310,47 @@ int scaph_msbfs(scaph_engine *e, const uint32_t *srcs, int nsrc, uint32_t *depth
  * nonzero mask; next = vertices newly reached by any source). */
 int scaph_msbfs_trace(scaph_engine *e, scaph_level_trace *out, int cap);
 
+/* ---- mixed query batches -------------------------------------------------- */
+
+/* No counterpart in the reference (one source of one graph per App::run,
+ * src/app.cuh:220-265).  A batch holds several graphs side by side on the
+ * device (their disjoint union, paged like any graph) and runs many
+ * single-source BFS queries over them in ONE launch of a CUDA graph:
+ * queries on the same graph share a bit-parallel traversal (one bit each,
+ * at most 128 per graph per launch), all graphs advance in one device-side
+ * level loop.  Depths are bit-exact with scaph_bfs on each graph alone.
+ * `transposed` (NULL when every graph is symmetric) gives each graph's
+ * in-edges for pull levels. */
+typedef struct scaph_batch scaph_batch;
+typedef struct scaph_query {
+    uint32_t graph;   /* index into the batch's graphs                      */
+    uint32_t source;  /* vertex id within that graph                        */
+} scaph_query;
+/* Tunables of the batch kernels (picked by scaph_b200/autotune.py). */
+typedef struct scaph_batch_params {
+    int32_t block_size;   /* threads per CTA of the level kernels: 256 or 512 */
+    int32_t ctas_per_sm;  /* grid = SMs x this                                 */
+    float   alpha, beta;  /* direction-switch thresholds                       */
+    int32_t _reserved;
+} scaph_batch_params;
+int scaph_batch_create(const scaph_csr *graphs, int ngraphs, const scaph_csr *transposed,
+                       uint32_t pagesize_words, const scaph_config *cfg, scaph_batch **b);
+int scaph_batch_destroy(scaph_batch *b);
+/* Union vertex ids of graph `graph`: first_vertex .. first_vertex+nvertices-1. */
+int scaph_batch_graph_range(const scaph_batch *b, int graph, uint32_t *first_vertex,
+                            uint32_t *nvertices);
+int scaph_batch_set_params(scaph_batch *b, const scaph_batch_params *p);
+int scaph_batch_get_params(const scaph_batch *b, scaph_batch_params *p);
+/* Runs nq queries.  depths: query i's row is u32[V of its graph], rows
+ * concatenated in query order (unreached = cfg.unreached); host or device
+ * memory per out_on_device.  stats->launches is 1: the traversal is one
+ * graph launch. */
+int scaph_batch_run(scaph_batch *b, const scaph_query *queries, int nq, uint32_t *depths,
+                    int out_on_device, scaph_bfs_stats *stats);
+/* Per-level trace of the last run (direction, frontier, time); returns the
+ * number of levels. */
+int scaph_batch_trace(const scaph_batch *b, scaph_level_trace *out, int cap);
+
 /* ---- page store for App-hook engines ------------------------------------ */
 
 /* The reference's apps supply a vertex program as device hooks

@@ -58,6 +58,15 @@ class _Stats(C.Structure):
                 ("launches", C.c_uint64), ("ms", C.c_double)]
 
 
+class _Query(C.Structure):
+    _fields_ = [("graph", C.c_uint32), ("source", C.c_uint32)]
+
+
+class _BatchParams(C.Structure):
+    _fields_ = [("block_size", C.c_int32), ("ctas_per_sm", C.c_int32), ("alpha", C.c_float), ("beta", C.c_float),
+                ("_reserved", C.c_int32)]
+
+
 class _Trace(C.Structure):
     _fields_ = [("level", C.c_int32), ("direction", C.c_int32), ("frontier", C.c_uint64),
                 ("frontier_edges", C.c_uint64), ("unvisited", C.c_uint64), ("unvisited_edges", C.c_uint64),
@@ -121,6 +130,13 @@ def lib() -> C.CDLL:
         "scaph_msbfs": ([vp, vp, i32, vp, i32, P(_Stats)], i32),
         "scaph_msbfs_trace": ([vp, P(_Trace), i32], i32),
         "scaph_bfs_page_hist": ([vp, i32, vp, vp, i32], i32),
+        "scaph_batch_create": ([vp, i32, vp, u32, P(_Config), P(vp)], i32),
+        "scaph_batch_destroy": ([vp], i32),
+        "scaph_batch_graph_range": ([vp, i32, P(u32), P(u32)], i32),
+        "scaph_batch_set_params": ([vp, P(_BatchParams)], i32),
+        "scaph_batch_get_params": ([vp, P(_BatchParams)], i32),
+        "scaph_batch_run": ([vp, vp, i32, vp, i32, P(_Stats)], i32),
+        "scaph_batch_trace": ([vp, vp, i32], i32),
         "scaph_host_alloc": ([C.c_size_t], vp),
         "scaph_host_free": ([vp], None),
         "scaph_device_count": ([], i32),
@@ -485,3 +501,85 @@ class Engine:
         d = np.zeros(self.graph.npages, np.uint32)
         _check(lib().scaph_bfs_page_hist(self._h, level, _ptr(n), _ptr(d), self.graph.npages))
         return n, d
+
+
+class Batch:
+    """Mixed query batch (scaph_batch_*): several graphs resident side by
+    side, many single-source queries per launch, one CUDA-graph launch per
+    run."""
+
+    def __init__(self, graphs: list, transposed: list | None = None, *, pagesize_words: int = 10 * 1024 * 1024,
+                 unreached: int = UNREACHED, direction: int = DIR_ALPHABETA, alpha: float = 14.0, beta: float = 24.0,
+                 device: int = 0, stream: int | None = None):
+        self.graphs = list(graphs)
+        arr = (_Csr * len(graphs))(*[g._c for g in graphs])
+        tarr = (_Csr * len(graphs))(*[g._c for g in transposed]) if transposed else None
+        cfg = _Config(0, unreached, direction, alpha, beta, 256, 0, 2, 0, 3, 0, device, stream, 0, 0, 0.0)
+        h = C.c_void_p()
+        _check(lib().scaph_batch_create(C.cast(arr, C.c_void_p), len(graphs),
+                                        C.cast(tarr, C.c_void_p) if tarr is not None else None, pagesize_words,
+                                        C.byref(cfg), C.byref(h)))
+        self._h = h
+        self.sizes = [int(g.V) for g in graphs]
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().scaph_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def graph_range(self, g: int) -> tuple[int, int]:
+        a, n = C.c_uint32(), C.c_uint32()
+        _check(lib().scaph_batch_graph_range(self._h, g, C.byref(a), C.byref(n)))
+        return a.value, n.value
+
+    @property
+    def params(self) -> dict:
+        p = _BatchParams()
+        _check(lib().scaph_batch_get_params(self._h, C.byref(p)))
+        return {"block_size": p.block_size, "ctas_per_sm": p.ctas_per_sm, "alpha": p.alpha, "beta": p.beta}
+
+    def set_params(self, block_size: int, ctas_per_sm: int, alpha: float, beta: float) -> None:
+        p = _BatchParams(block_size, ctas_per_sm, alpha, beta, 0)
+        _check(lib().scaph_batch_set_params(self._h, C.byref(p)))
+
+    def _queries(self, queries):
+        q = np.ascontiguousarray(np.asarray(queries, np.uint32).reshape(-1, 2))
+        if len(q) and int(q[:, 0].max()) >= len(self.sizes):
+            raise ScaphError(EINVAL, f"query graph {int(q[:, 0].max())} out of range ({len(self.sizes)} graphs)")
+        return q, sum(self.sizes[int(g)] for g in q[:, 0])
+
+    def run(self, queries) -> tuple[list, BfsStats]:
+        """queries: (graph, source) pairs.  Returns (one depth array per
+        query, over its graph's vertices; BfsStats)."""
+        q, total = self._queries(queries)
+        out = np.empty(total, np.uint32)
+        st = _Stats()
+        _check(lib().scaph_batch_run(self._h, _ptr(q), len(q), _ptr(out), 0, C.byref(st)))
+        rows, off = [], 0
+        for g in q[:, 0]:
+            n = self.sizes[int(g)]
+            rows.append(out[off:off + n])
+            off += n
+        return rows, _stats(st)
+
+    def run_device(self, queries, depth_ptr: int) -> BfsStats:
+        """Depth rows into device memory at depth_ptr (u32, concatenated in
+        query order)."""
+        q, _ = self._queries(queries)
+        st = _Stats()
+        _check(lib().scaph_batch_run(self._h, _ptr(q), len(q), C.c_void_p(depth_ptr), 1, C.byref(st)))
+        return _stats(st)
+
+    def out_words(self, queries) -> int:
+        return self._queries(queries)[1]
+
+    def trace(self) -> list[dict]:
+        buf = (_Trace * 4096)()
+        n = _check(lib().scaph_batch_trace(self._h, buf, 4096))
+        return [{f: getattr(buf[i], f) for f, _ in _Trace._fields_} for i in range(min(n, 4096))]

@@ -1,0 +1,127 @@
+"""Autotuner for the query-batch kernels (scaph_batch_*).
+
+The batch's level kernels take their CTA size (256 or 512 threads), the
+number of CTAs per SM, and the two direction-switch thresholds alpha / beta
+as run-time parameters (scaph_batch_set_params).  `tune_batch` times
+candidates on the caller's own batch - the device time of whole batch runs,
+best of `repeats` - by coordinate search: the launch shape first (every
+block size x CTAs-per-SM pair at the default thresholds), then alpha, then
+beta around the best shape.  Every parameter only changes the schedule, never
+the depths; the tuner still checks that the chosen parameters reproduce the
+depths of the starting parameters bit for bit (a checksum of the depth rows).
+
+Results are cached in a JSON file (default ~/.cache/scaph_b200/tune.json,
+or $SCAPH_TUNE_CACHE) keyed by the batch's shape, so a serving process tunes
+once per batch shape.
+"""
+from __future__ import annotations
+
+import json
+import os
+import time
+
+import numpy as np
+
+from . import Batch
+
+SHAPES = [(256, c) for c in (2, 3, 4, 6, 8)] + [(512, c) for c in (1, 2, 3, 4)]
+ALPHAS = (7.0, 10.0, 14.0, 20.0, 28.0)
+BETAS = (12.0, 24.0, 48.0, 96.0)
+
+
+def cache_path() -> str:
+    return os.environ.get("SCAPH_TUNE_CACHE", os.path.join(os.path.expanduser("~"), ".cache", "scaph_b200",
+                                                           "tune.json"))
+
+
+def batch_key(batch: Batch, queries) -> str:
+    q = np.asarray(queries, np.uint32).reshape(-1, 2)
+    per_graph = np.bincount(q[:, 0], minlength=len(batch.sizes))
+    V = sum(batch.sizes)
+    E = sum(int(g.E) for g in batch.graphs)
+    return f"batch|V={V}|E={E}|graphs={len(batch.sizes)}|queries={len(q)}|maxq={int(per_graph.max())}"
+
+
+def _load(path):
+    try:
+        with open(path) as f:
+            return json.load(f)
+    except (OSError, ValueError):
+        return {}
+
+
+def _store(path, data):
+    os.makedirs(os.path.dirname(path), exist_ok=True)
+    tmp = path + f".{os.getpid()}.tmp"
+    with open(tmp, "w") as f:
+        json.dump(data, f, indent=1, sort_keys=True)
+    os.replace(tmp, path)
+
+
+def _time(batch: Batch, queries, ptr: int, repeats: int) -> float:
+    best = float("inf")
+    for _ in range(repeats):
+        st = batch.run_device(queries, ptr)
+        best = min(best, st.ms)
+    return best
+
+
+def _checksum(batch: Batch, queries) -> int:
+    rows, _ = batch.run(queries)
+    h = 0
+    for i, r in enumerate(rows):
+        h = (h * 1000003 + int(np.bitwise_xor.reduce(r.astype(np.uint64) * np.uint64(2654435761) +
+                                                     np.arange(len(r), dtype=np.uint64))) + i) & (2**64 - 1)
+    return h
+
+
+def tune_batch(batch: Batch, queries, ptr: int, repeats: int = 3, cache: str | None = None,
+               force: bool = False) -> dict:
+    """Picks and sets the batch parameters for `queries`; `ptr` is a device
+    buffer of at least batch.out_words(queries) u32 words for the timed runs.
+    Returns {"params": ..., "ms": ..., "default_ms": ..., "tried": n,
+    "seconds": tuning time, "cached": bool}."""
+    path = cache or cache_path()
+    key = batch_key(batch, queries)
+    db = _load(path)
+    if key in db and not force:
+        p = db[key]["params"]
+        batch.set_params(p["block_size"], p["ctas_per_sm"], p["alpha"], p["beta"])
+        return dict(db[key], cached=True)
+    t0 = time.time()
+    start = batch.params
+    ref_sum = _checksum(batch, queries)
+    batch.run_device(queries, ptr)  # warm
+    default_ms = _time(batch, queries, ptr, repeats)
+    best = dict(start)
+    best_ms = default_ms
+    tried = 1
+
+    def trial(p):
+        nonlocal best, best_ms, tried
+        batch.set_params(p["block_size"], p["ctas_per_sm"], p["alpha"], p["beta"])
+        batch.run_device(queries, ptr)  # builds the graph for this shape
+        ms = _time(batch, queries, ptr, repeats)
+        tried += 1
+        if ms < best_ms:
+            best, best_ms = dict(p), ms
+
+    for b, c in SHAPES:
+        if (b, c) != (start["block_size"], start["ctas_per_sm"]):
+            trial(dict(start, block_size=b, ctas_per_sm=c))
+    for a in ALPHAS:
+        if a != best["alpha"]:
+            trial(dict(best, alpha=a))
+    for bt in BETAS:
+        if bt != best["beta"]:
+            trial(dict(best, beta=bt))
+    batch.set_params(best["block_size"], best["ctas_per_sm"], best["alpha"], best["beta"])
+    if _checksum(batch, queries) != ref_sum:
+        batch.set_params(start["block_size"], start["ctas_per_sm"], start["alpha"], start["beta"])
+        raise RuntimeError("tuned batch parameters changed the depths")
+    out = {"params": best, "ms": best_ms, "default_ms": default_ms, "tried": tried,
+           "seconds": time.time() - t0}
+    db = _load(path)
+    db[key] = out
+    _store(path, db)
+    return dict(out, cached=False)

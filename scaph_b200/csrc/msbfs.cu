@@ -1,21 +1,10 @@
-// Multi-source BFS: up to 128 single-source BFS traversals share one pass
-// over the edges (bit-parallel BFS in the manner of Then et al., "The More
-// the Merrier", VLDB 2014).  No reference counterpart: the reference runs one
-// source per App::run (src/app.cuh:220-265, app/bfs.cu:137-140).
-//
-// Per vertex u (NW = 1 or 2 64-bit words, bit i = source i):
-//   seen[u]    sources that have reached u (stored next to acc[u], the push
-//              accumulator, so one 16-byte load returns both)
-//   visit[u]   sources whose frontier holds u this level (valid where the
-//              `act` bitmap has u's bit)
-// push level: every active v sends visit[v] & ~seen[u] to its out-neighbours
-//   u with a fire-and-forget red.or into acc[u] (and marks u in `touched`);
-//   a finalize pass turns acc into the next frontier.
-// pull level: every incomplete u (seen[u] != all sources) ORs visit[v] over
-//   its in-neighbours v whose act bit is set, stopping as soon as every
-//   missing source has been found.
-// Depths are kept as bit planes (plane k, bit i = bit k of depth(i,u)) and
-// unpacked at the end into u32 depth[i][V], bit-exact with single-source BFS.
+// Multi-source BFS (scaph_msbfs): up to 128 single-source BFS traversals
+// share one pass over the edges, one bit per source in per-vertex masks (the
+// device side is in ms_kernels.cuh).  No reference counterpart: the
+// reference runs one source per App::run (src/app.cuh:220-265,
+// app/bfs.cu:137-140).  This file is the host loop: one launch per phase and
+// level, the direction rule between levels, depths unpacked at the end into
+// u32 depth[i][V], bit-exact with single-source BFS.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -24,123 +13,9 @@
 #include "engine.h"
 #include "kernel_common.cuh"
 
+#include "ms_kernels.cuh"
+
 namespace scaph {
-
-constexpr int kMsPlanes = 12;  // depths below 4096 = kMaxLevels
-constexpr int kMsBlock = 256;
-constexpr int kMsTileWords = 128;
-
-template <int NW>
-struct Mask {
-    unsigned long long w[NW];
-};
-
-template <int NW>
-__device__ __forceinline__ Mask<NW> ld_mask(const unsigned long long *a, uint32_t u)
-{
-    Mask<NW> m;
-    if constexpr (NW == 2) {
-        const ulonglong2 x = *reinterpret_cast<const ulonglong2 *>(a + 2ull * u);
-        m.w[0] = x.x;
-        m.w[1] = x.y;
-    } else {
-        m.w[0] = a[u];
-    }
-    return m;
-}
-
-template <int NW>
-__device__ __forceinline__ void st_mask(unsigned long long *a, uint32_t u, const Mask<NW> &m)
-{
-    if constexpr (NW == 2) {
-        *reinterpret_cast<ulonglong2 *>(a + 2ull * u) = make_ulonglong2(m.w[0], m.w[1]);
-    } else {
-        a[u] = m.w[0];
-    }
-}
-
-// seen and acc of vertex u are interleaved: sa[u] = {seen[NW], acc[NW]}
-template <int NW>
-__device__ __forceinline__ void ld_seen_acc(const unsigned long long *sa, uint32_t u, Mask<NW> &seen, Mask<NW> &acc)
-{
-    const ulonglong2 *p = reinterpret_cast<const ulonglong2 *>(sa + 2ull * NW * u);
-    if constexpr (NW == 1) {
-        const ulonglong2 x = *p;
-        seen.w[0] = x.x;
-        acc.w[0] = x.y;
-    } else {
-        const ulonglong2 x = p[0], y = p[1];
-        seen.w[0] = x.x;
-        seen.w[1] = x.y;
-        acc.w[0] = y.x;
-        acc.w[1] = y.y;
-    }
-}
-
-template <int NW>
-__device__ __forceinline__ Mask<NW> ld_seen(const unsigned long long *sa, uint32_t u)
-{
-    Mask<NW> m;
-    if constexpr (NW == 2) {
-        const ulonglong2 x = *reinterpret_cast<const ulonglong2 *>(sa + 4ull * u);
-        m.w[0] = x.x;
-        m.w[1] = x.y;
-    } else {
-        m.w[0] = sa[2ull * u];
-    }
-    return m;
-}
-
-template <int NW>
-__device__ __forceinline__ void st_seen(unsigned long long *sa, uint32_t u, const Mask<NW> &m)
-{
-    if constexpr (NW == 2) {
-        *reinterpret_cast<ulonglong2 *>(sa + 4ull * u) = make_ulonglong2(m.w[0], m.w[1]);
-    } else {
-        sa[2ull * u] = m.w[0];
-    }
-}
-
-template <int NW>
-__device__ __forceinline__ bool any(const Mask<NW> &m)
-{
-    bool r = false;
-#pragma unroll
-    for (int i = 0; i < NW; i++) r |= m.w[i] != 0;
-    return r;
-}
-
-template <int NW>
-__device__ __forceinline__ uint32_t popc(const Mask<NW> &m)
-{
-    uint32_t r = 0;
-#pragma unroll
-    for (int i = 0; i < NW; i++) r += __popcll(m.w[i]);
-    return r;
-}
-
-struct MsCounters {
-    unsigned long long active;        // vertices in the next frontier
-    unsigned long long active_edges;  // their out-degree sum
-    unsigned long long pairs;         // (source, vertex) pairs reached this level
-    unsigned long long inspected;     // adjacency entries examined
-    unsigned long long completed_edges;  // out-degree of vertices that became complete
-    unsigned int giant;
-    unsigned int error;
-};
-
-struct MsDev {
-    unsigned long long *sa;  // {seen, acc} per vertex
-    unsigned long long *visit_cur, *visit_nxt;
-    unsigned long long *planes[kMsPlanes];
-    uint32_t *act_cur, *act_nxt, *touched, *inc;
-    const uint32_t *degree;
-    MsCounters *ctr;
-    GiantChunk *giant;
-    uint32_t giant_cap;
-    uint32_t V, nwords, level;
-    unsigned long long all[2];  // source bits in use
-};
 
 struct MsState {
     int nw = 0;
@@ -172,486 +47,6 @@ void ms_release(MsState *m)
     cudaFree(m->d_src);
     cudaFree(m->out);
     delete m;
-}
-
-namespace {
-
-template <int NW>
-__device__ __forceinline__ Mask<NW> all_mask(const MsDev &s)
-{
-    Mask<NW> m;
-#pragma unroll
-    for (int i = 0; i < NW; i++) m.w[i] = s.all[i];
-    return m;
-}
-
-// depth planes: OR the newly reached bits into plane k for every bit k of d
-template <int NW>
-__device__ __forceinline__ void plane_or(const MsDev &s, uint32_t u, const Mask<NW> &nw, uint32_t d)
-{
-#pragma unroll 1
-    for (int k = 0; k < kMsPlanes; k++) {
-        if (!((d >> k) & 1u)) continue;
-        unsigned long long *p = s.planes[k];
-        Mask<NW> o = ld_mask<NW>(p, u);
-#pragma unroll
-        for (int i = 0; i < NW; i++) o.w[i] |= nw.w[i];
-        st_mask<NW>(p, u, o);
-    }
-}
-
-struct MsAcc {
-    unsigned long long active = 0, active_edges = 0, pairs = 0, inspected = 0, completed_edges = 0;
-};
-
-__device__ __forceinline__ void ms_flush(MsAcc a, MsCounters *c)
-{
-    a.active = kc::warp_sum64(a.active);
-    a.active_edges = kc::warp_sum64(a.active_edges);
-    a.pairs = kc::warp_sum64(a.pairs);
-    a.inspected = kc::warp_sum64(a.inspected);
-    a.completed_edges = kc::warp_sum64(a.completed_edges);
-    if ((threadIdx.x & 31) == 0) {
-        if (a.active) atomicAdd(&c->active, a.active);
-        if (a.active_edges) atomicAdd(&c->active_edges, a.active_edges);
-        if (a.pairs) atomicAdd(&c->pairs, a.pairs);
-        if (a.inspected) atomicAdd(&c->inspected, a.inspected);
-        if (a.completed_edges) atomicAdd(&c->completed_edges, a.completed_edges);
-    }
-}
-
-// Sends a frontier mask to up to four out-neighbours (on[j] marks the valid
-// ones): their seen masks are loaded first, all four at once, then the new
-// bits go out as reductions.
-template <int NW>
-__device__ __forceinline__ void ms_send4(const MsDev &s, const uint32_t (&u)[4], const bool (&on)[4],
-                                         const Mask<NW> &vis)
-{
-    Mask<NW> sn[4], ac[4];
-#pragma unroll
-    for (int j = 0; j < 4; j++) {
-        if (on[j] && u[j] < s.V) ld_seen_acc<NW>(s.sa, u[j], sn[j], ac[j]);
-    }
-#pragma unroll
-    for (int j = 0; j < 4; j++) {
-        if (!on[j]) continue;
-        if (u[j] >= s.V) {
-            atomicOr(&s.ctr->error, 1u);
-            continue;
-        }
-        bool hit = false;
-#pragma unroll
-        for (int i = 0; i < NW; i++) {
-            // bits some other sender already put in acc need not go again
-            const unsigned long long n = vis.w[i] & ~(sn[j].w[i] | ac[j].w[i]);
-            if (n) {
-                kc::red_or(s.sa + 2ull * NW * u[j] + NW + i, n);
-                hit = true;
-            }
-        }
-        if (hit) kc::red_or(s.touched + (u[j] >> 5), 1u << (u[j] & 31));
-    }
-}
-
-}  // namespace
-
-// ---------------------------------------------------------------------------
-// push: active vertices send their frontier masks to out-neighbours
-// ---------------------------------------------------------------------------
-template <int NW>
-__global__ void __launch_bounds__(kMsBlock) k_ms_push(GraphDev g, MsDev s)
-{
-    __shared__ PageDev lp[kLutPages];
-    __shared__ uint32_t lc[kLutCoarse];
-    __shared__ uint32_t q[kMsTileWords * 32];
-    __shared__ unsigned long long ebase[kMsBlock];
-    __shared__ uint32_t elen[kMsBlock], qoff[kMsBlock], wsum[kMsBlock / 32];
-    __shared__ Mask<NW> vis[kMsBlock];
-    const PageLut lut = kc::stage_lut<kMsBlock>(g, lp, lc);
-    __syncthreads();
-    MsAcc a;
-    const uint32_t ntiles = (s.nwords + kMsTileWords - 1) / kMsTileWords;
-    for (uint32_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-        const uint32_t w = tile * kMsTileWords + threadIdx.x;
-        uint32_t f = (threadIdx.x < kMsTileWords && w < s.nwords) ? s.act_cur[w] : 0u;
-        if (!__syncthreads_or(f != 0)) continue;
-        uint32_t total;
-        uint32_t off = kc::block_exclusive_scan<kMsBlock>(__popc(f), wsum, total);
-        while (f) {
-            q[off++] = (w << 5) + (__ffs(f) - 1);
-            f &= f - 1;
-        }
-        __syncthreads();
-        for (uint32_t c0 = 0; c0 < total; c0 += kMsBlock) {
-            const uint32_t k = c0 + threadIdx.x;
-            uint32_t nq = 0;
-            if (k < total) {
-                const uint32_t v = q[k];
-                const int p = lut.of(v);
-                const PageDev pd = lut.pages[p];
-                const uint32_t *node = g.pool + pd.base + 3ull * (v - pd.left);
-                uint32_t len = node[2];
-                const unsigned long long st = pd.base + 3ull * pd.nodenum + node[1];
-                const Mask<NW> m = ld_mask<NW>(s.visit_cur, v);
-                vis[threadIdx.x] = m;
-                a.inspected += len;
-                if (len > kGiantEdges) {
-                    const uint32_t nch = (len + kGiantEdges - 1) / kGiantEdges;
-                    const uint32_t at = atomicAdd(&s.ctr->giant, nch);
-                    if (at + nch <= s.giant_cap) {
-                        for (uint32_t c = 0; c < nch; c++) {
-                            GiantChunk gc;
-                            gc.start = st + (unsigned long long)c * kGiantEdges;
-                            gc.len = min(kGiantEdges, len - c * kGiantEdges);
-                            gc.src = v;
-                            s.giant[at + c] = gc;
-                        }
-                        len = 0;
-                    } else {
-                        atomicOr(&s.ctr->error, 2u);
-                    }
-                }
-                ebase[threadIdx.x] = st;
-                elen[threadIdx.x] = len;
-                nq = len ? (uint32_t)(((st + len + 3) >> 2) - (st >> 2)) : 0u;
-            }
-            uint32_t tq;
-            const uint32_t qo = kc::block_exclusive_scan<kMsBlock>(nq, wsum, tq);
-            qoff[threadIdx.x] = qo;
-            __syncthreads();
-            for (uint32_t i = threadIdx.x; i < tq; i += kMsBlock) {
-                int lo = 0, hi = kMsBlock - 1;
-                while (lo < hi) {
-                    const int mid = (lo + hi + 1) >> 1;
-                    if (qoff[mid] <= i) lo = mid; else hi = mid - 1;
-                }
-                const unsigned long long st = ebase[lo], en = st + elen[lo];
-                const unsigned long long quad = (st >> 2) + (i - qoff[lo]);
-                const uint4 val = ld_nc_v4(g.pool + quad * 4);
-                const uint32_t vals[4] = {val.x, val.y, val.z, val.w};
-                bool on[4];
-#pragma unroll
-                for (int j = 0; j < 4; j++) on[j] = quad * 4 + j >= st && quad * 4 + j < en;
-                ms_send4<NW>(s, vals, on, vis[lo]);
-            }
-            __syncthreads();
-        }
-    }
-    ms_flush(a, s.ctr);
-}
-
-template <int NW>
-__global__ void __launch_bounds__(kMsBlock) k_ms_push_giant(GraphDev g, MsDev s)
-{
-    const uint32_t n = min(*((volatile uint32_t *)&s.ctr->giant), s.giant_cap);
-    for (uint32_t c = blockIdx.x; c < n; c += gridDim.x) {
-        const GiantChunk gc = s.giant[c];
-        if (gc.len > kGiantEdges || gc.start + gc.len > g.pool_words || gc.src >= s.V) {
-            if (threadIdx.x == 0) atomicOr(&s.ctr->error, 8u);
-            continue;
-        }
-        const Mask<NW> m = ld_mask<NW>(s.visit_cur, gc.src);
-        const unsigned long long st = gc.start, en = gc.start + gc.len;
-        for (unsigned long long qd = (st >> 2) + threadIdx.x; qd < ((en + 3) >> 2); qd += kMsBlock) {
-            const uint4 val = ld_nc_v4(g.pool + qd * 4);
-            const uint32_t vals[4] = {val.x, val.y, val.z, val.w};
-            bool on[4];
-#pragma unroll
-            for (int j = 0; j < 4; j++) on[j] = qd * 4 + j >= st && qd * 4 + j < en;
-            ms_send4<NW>(s, vals, on, m);
-        }
-    }
-}
-
-// acc -> next frontier, seen, depth planes; one warp per touched word
-template <int NW>
-__global__ void __launch_bounds__(kMsBlock) k_ms_finalize(MsDev s)
-{
-    const int lane = threadIdx.x & 31;
-    const uint32_t wstride = (gridDim.x * kMsBlock) >> 5;
-    const Mask<NW> all = all_mask<NW>(s);
-    MsAcc a;
-    for (uint32_t w = (blockIdx.x * kMsBlock + threadIdx.x) >> 5; w < s.nwords; w += wstride) {
-        const uint32_t t = s.touched[w];
-        if (!t) continue;
-        const uint32_t u = (w << 5) + lane;
-        bool act = false, done = false;
-        if ((t >> lane) & 1u) {
-            Mask<NW> sn, ac, nw, ns;
-            ld_seen_acc<NW>(s.sa, u, sn, ac);
-            bool complete = true;
-#pragma unroll
-            for (int i = 0; i < NW; i++) {
-                nw.w[i] = ac.w[i] & ~sn.w[i] & all.w[i];
-                ns.w[i] = sn.w[i] | nw.w[i];
-                complete &= (ns.w[i] & all.w[i]) == all.w[i];
-            }
-            // seen |= new bits and acc = 0, in one store
-            ulonglong2 *p = reinterpret_cast<ulonglong2 *>(s.sa + 2ull * NW * u);
-            if constexpr (NW == 1) {
-                p[0] = make_ulonglong2(ns.w[0], 0ull);
-            } else {
-                p[0] = make_ulonglong2(ns.w[0], ns.w[1]);
-                p[1] = make_ulonglong2(0ull, 0ull);
-            }
-            if (any(nw)) {
-                st_mask<NW>(s.visit_nxt, u, nw);
-                plane_or<NW>(s, u, nw, s.level + 1);
-                const uint32_t d = __ldg(&s.degree[u]);
-                a.active++;
-                a.active_edges += d;
-                a.pairs += popc(nw);
-                act = true;
-                if (complete) {
-                    done = true;
-                    a.completed_edges += d;
-                }
-            }
-        }
-        const uint32_t am = __ballot_sync(0xFFFFFFFFu, act), dm = __ballot_sync(0xFFFFFFFFu, done);
-        if (lane == 0) {
-            s.touched[w] = 0;
-            if (am) s.act_nxt[w] = am;
-            if (dm) s.inc[w] &= ~dm;
-        }
-    }
-    ms_flush(a, s.ctr);
-}
-
-// ---------------------------------------------------------------------------
-// pull: incomplete vertices OR the frontier masks of their in-neighbours
-// ---------------------------------------------------------------------------
-template <int NW>
-__global__ void __launch_bounds__(kMsBlock) k_ms_pull(GraphDev g, MsDev s)
-{
-    __shared__ PageDev lp[kLutPages];
-    __shared__ uint32_t lc[kLutCoarse];
-    __shared__ uint32_t q[kMsTileWords * 32];
-    __shared__ uint32_t fnd[kMsTileWords], dne[kMsTileWords];
-    __shared__ uint32_t bq_u[kMsBlock], bq_len[kMsBlock];
-    __shared__ unsigned long long bq_st[kMsBlock];
-    __shared__ Mask<NW> bq_acc[kMsBlock];
-    __shared__ uint32_t bq_qoff[kMsBlock];
-    __shared__ uint32_t wsum[kMsBlock / 32];
-    const PageLut lut = kc::stage_lut<kMsBlock>(g, lp, lc);
-    const Mask<NW> all = all_mask<NW>(s);
-    __syncthreads();
-    MsAcc a;
-    const uint32_t ntiles = (s.nwords + kMsTileWords - 1) / kMsTileWords;
-    for (uint32_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-        const uint32_t wbase = tile * kMsTileWords;
-        const uint32_t w = wbase + threadIdx.x;
-        uint32_t f = 0;
-        if (threadIdx.x < kMsTileWords) {
-            fnd[threadIdx.x] = 0;
-            dne[threadIdx.x] = 0;
-            if (w < s.nwords) f = s.inc[w];
-        }
-        if (!__syncthreads_or(f != 0)) continue;
-        uint32_t total;
-        uint32_t off = kc::block_exclusive_scan<kMsBlock>(__popc(f), wsum, total);
-        while (f) {
-            q[off++] = (w << 5) + (__ffs(f) - 1);
-            f &= f - 1;
-        }
-        __syncthreads();
-        for (uint32_t c0 = 0; c0 < total; c0 += kMsBlock) {
-            const uint32_t k = c0 + threadIdx.x;
-            uint32_t u = 0, len = 0, need = 0;
-            unsigned long long st = 0;
-            Mask<NW> miss, acc;
-#pragma unroll
-            for (int i = 0; i < NW; i++) miss.w[i] = acc.w[i] = 0;
-            if (k < total) {
-                u = q[k];
-                const Mask<NW> sn = ld_seen<NW>(s.sa, u);
-#pragma unroll
-                for (int i = 0; i < NW; i++) miss.w[i] = all.w[i] & ~sn.w[i];
-                const int p = lut.of(u);
-                const PageDev pd = lut.pages[p];
-                const uint32_t *node = g.pool + pd.base + 3ull * (u - pd.left);
-                len = node[2];
-                st = pd.base + 3ull * pd.nodenum + node[1];
-                // first four in-edges: independent loads, act probes, masks
-                uint32_t v[4];
-#pragma unroll
-                for (int j = 0; j < 4; j++) v[j] = (uint32_t)j < len ? __ldg(&g.pool[st + j]) : 0xFFFFFFFFu;
-                bool on[4];
-#pragma unroll
-                for (int j = 0; j < 4; j++) on[j] = v[j] < s.V && test_bit(s.act_cur, v[j]);
-#pragma unroll
-                for (int j = 0; j < 4; j++) {
-                    if (on[j]) {
-                        const Mask<NW> m = ld_mask<NW>(s.visit_cur, v[j]);
-#pragma unroll
-                        for (int i = 0; i < NW; i++) acc.w[i] |= m.w[i];
-                    }
-                }
-                a.inspected += min(len, 4u);
-                bool full = true;
-#pragma unroll
-                for (int i = 0; i < NW; i++) full &= (acc.w[i] & miss.w[i]) == miss.w[i];
-                need = (!full && len > 4) ? 1u : 0u;
-            }
-            uint32_t nb;
-            const uint32_t bo = kc::block_exclusive_scan<kMsBlock>(need, wsum, nb);
-            if (need) {
-                bq_u[bo] = u;
-                bq_st[bo] = st;
-                bq_len[bo] = len;
-                bq_acc[bo] = acc;
-            }
-            __syncthreads();
-            // phase B: the remaining in-edges of the unresolved vertices,
-            // edge-balanced over the CTA by a scan over 16-byte quads; each
-            // quad's frontier masks are OR-ed into the vertex's shared
-            // accumulator (an OR-semiring SpMV over those rows)
-            uint32_t nq = 0;
-            if (threadIdx.x < nb) {
-                const unsigned long long a0 = bq_st[threadIdx.x] + 4, b0 = bq_st[threadIdx.x] + bq_len[threadIdx.x];
-                nq = (uint32_t)(((b0 + 3) >> 2) - (a0 >> 2));
-            }
-            uint32_t tq;
-            const uint32_t qo = kc::block_exclusive_scan<kMsBlock>(nq, wsum, tq);
-            bq_qoff[threadIdx.x] = qo;
-            __syncthreads();
-            for (uint32_t i = threadIdx.x; i < tq; i += kMsBlock) {
-                int lo = 0, hi = (int)nb - 1;
-                while (lo < hi) {
-                    const int mid = (lo + hi + 1) >> 1;
-                    if (bq_qoff[mid] <= i) lo = mid; else hi = mid - 1;
-                }
-                const unsigned long long aa = bq_st[lo] + 4, bb = bq_st[lo] + bq_len[lo];
-                const unsigned long long quad = (aa >> 2) + (i - bq_qoff[lo]);
-                const uint4 val = ld_nc_v4(g.pool + quad * 4);
-                const uint32_t vals[4] = {val.x, val.y, val.z, val.w};
-                bool in[4], on[4];
-#pragma unroll
-                for (int j = 0; j < 4; j++) {
-                    in[j] = quad * 4 + j >= aa && quad * 4 + j < bb;
-                    on[j] = in[j] && vals[j] < s.V && test_bit(s.act_cur, vals[j]);
-                    a.inspected += in[j] ? 1 : 0;
-                }
-                Mask<NW> part;
-#pragma unroll
-                for (int w2 = 0; w2 < NW; w2++) part.w[w2] = 0;
-#pragma unroll
-                for (int j = 0; j < 4; j++) {
-                    if (on[j]) {
-                        const Mask<NW> m = ld_mask<NW>(s.visit_cur, vals[j]);
-#pragma unroll
-                        for (int w2 = 0; w2 < NW; w2++) part.w[w2] |= m.w[w2];
-                    }
-                }
-                // the active lanes of a warp are a prefix and cover consecutive
-                // quads, so equal `lo` values are contiguous: a segmented OR by
-                // doubling leaves each segment's total in its first lane, which
-                // alone issues the shared atomic
-                const unsigned int am = __activemask();
-                const int lane = threadIdx.x & 31, nact = 32 - __clz(am);
-                const int lo_prev = __shfl_up_sync(am, lo, 1);
-                const bool head = lane == 0 || lo_prev != lo;
-#pragma unroll
-                for (int w2 = 0; w2 < NW; w2++) {
-                    unsigned long long v = part.w[w2];
-#pragma unroll
-                    for (int o = 1; o < 32; o <<= 1) {
-                        const unsigned long long x = __shfl_down_sync(am, v, o);
-                        const int lo2 = __shfl_down_sync(am, lo, o);
-                        if (lane + o < nact && lo2 == lo) v |= x;
-                    }
-                    if (head && v) atomicOr(&bq_acc[lo].w[w2], v);
-                }
-            }
-            __syncthreads();
-            // merge phase-B results back into the owning thread
-            if (need) acc = bq_acc[bo];
-            if (k < total) {
-                Mask<NW> nw;
-#pragma unroll
-                for (int i = 0; i < NW; i++) nw.w[i] = acc.w[i] & miss.w[i];
-                if (any(nw)) {
-                    const Mask<NW> sn = ld_seen<NW>(s.sa, u);
-                    Mask<NW> ns;
-                    bool complete = true;
-#pragma unroll
-                    for (int i = 0; i < NW; i++) {
-                        ns.w[i] = sn.w[i] | nw.w[i];
-                        complete &= (ns.w[i] & all.w[i]) == all.w[i];
-                    }
-                    st_seen<NW>(s.sa, u, ns);
-                    st_mask<NW>(s.visit_nxt, u, nw);
-                    plane_or<NW>(s, u, nw, s.level + 1);
-                    const uint32_t d = __ldg(&s.degree[u]);
-                    a.active++;
-                    a.active_edges += d;
-                    a.pairs += popc(nw);
-                    atomicOr(&fnd[(u >> 5) - wbase], 1u << (u & 31));
-                    if (complete) {
-                        a.completed_edges += d;
-                        atomicOr(&dne[(u >> 5) - wbase], 1u << (u & 31));
-                    }
-                }
-            }
-            __syncthreads();
-        }
-        if (threadIdx.x < kMsTileWords && w < s.nwords) {
-            if (fnd[threadIdx.x]) s.act_nxt[w] = fnd[threadIdx.x];
-            if (dne[threadIdx.x]) s.inc[w] &= ~dne[threadIdx.x];
-        }
-        __syncthreads();
-    }
-    ms_flush(a, s.ctr);
-}
-
-// clears the frontier masks of the source vertices (left over from an
-// earlier batch) before k_ms_sources sets their bits
-template <int NW>
-__global__ void k_ms_clear_sources(MsDev s, const uint32_t *srcs, int nsrc)
-{
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= nsrc || srcs[i] >= s.V) return;
-#pragma unroll
-    for (int j = 0; j < NW; j++) s.visit_cur[(size_t)srcs[i] * NW + j] = 0ull;
-}
-
-// sources into the state (setsrc of app/bfs.cu:32-37, one bit per source)
-template <int NW>
-__global__ void k_ms_sources(MsDev s, const uint32_t *srcs, int nsrc)
-{
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= nsrc) return;
-    const uint32_t v = srcs[i];
-    if (v >= s.V) {
-        atomicOr(&s.ctr->error, 32u);
-        return;
-    }
-    const int word = i >> 6;
-    const unsigned long long bit = 1ull << (i & 63);
-    atomicOr(s.sa + 2ull * NW * v + word, bit);
-    atomicOr(s.visit_cur + (size_t)v * NW + word, bit);
-    atomicOr(&s.act_cur[v >> 5], 1u << (v & 31));
-}
-
-// depth[i][u] from the bit planes; unreached where seen lacks bit i
-template <int NW>
-__global__ void k_ms_unpack(MsDev s, uint32_t *out, int nsrc, int nplanes, uint32_t unreached)
-{
-    const size_t stride = (size_t)gridDim.x * blockDim.x;
-    for (size_t u = (size_t)blockIdx.x * blockDim.x + threadIdx.x; u < s.V; u += stride) {
-        const Mask<NW> sn = ld_seen<NW>(s.sa, (uint32_t)u);
-        Mask<NW> pl[kMsPlanes];
-        for (int k = 0; k < nplanes; k++) pl[k] = ld_mask<NW>(s.planes[k], (uint32_t)u);
-        for (int i = 0; i < nsrc; i++) {
-            const int word = i >> 6, b = i & 63;
-            uint32_t d = unreached;
-            if ((sn.w[word] >> b) & 1ull) {
-                d = 0;
-                for (int k = 0; k < nplanes; k++) d |= (uint32_t)((pl[k].w[word] >> b) & 1ull) << k;
-            }
-            out[(size_t)i * s.V + u] = d;
-        }
-    }
 }
 
 }  // namespace scaph

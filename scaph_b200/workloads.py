@@ -54,6 +54,25 @@ def config4a(scale: int = 25):
     return csr, random_sources(csr, 64, SEED_BASE + 3)
 
 
+def config4b(ngraphs: int = 32, nqueries: int = 256, scales=(14, 22), edgefactors=(8, 32)):
+    """Mixed batch: ngraphs RMAT graphs with scale and edge factor drawn by
+    seed from the given ranges (inclusive), nqueries single-source queries
+    (graph uniform at random, source a random vertex with nonzero degree).
+    Returns (graphs, [(graph, source), ...], [(scale, edgefactor), ...])."""
+    rng = np.random.default_rng(SEED_BASE + 3 + 1000)
+    shapes = [(int(rng.integers(scales[0], scales[1] + 1)), int(rng.integers(edgefactors[0], edgefactors[1] + 1)))
+              for _ in range(ngraphs)]
+    a, b, c = RMAT_ABC
+    graphs = [Csr.rmat(s, ef, a, b, c, seed=SEED_BASE + 3 + 2000 + i, scramble=True)
+              for i, (s, ef) in enumerate(shapes)]
+    cands = [np.flatnonzero(g.degree() > 0) for g in graphs]
+    queries = []
+    for _ in range(nqueries):
+        gi = int(rng.integers(0, ngraphs))
+        queries.append((gi, int(rng.choice(cands[gi]))))
+    return graphs, queries, shapes
+
+
 def config5(V: int = 105_000_000, E: int = 3_700_000_000, max_degree: int = 1 << 20):
     """Directed web-crawl-like graph: out-degree power law s=2.1, 90 % of the
     edges inside the source's block of 4096 consecutive ids, the rest uniform;
