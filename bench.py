@@ -37,6 +37,11 @@ PEAKS_FILE = os.path.join(ROOT, "MEASURED_PEAKS.json")
 FALLBACK_HBM_GBS = 6650.0
 
 
+# Measured DRAM bytes (read + write) per k_pull launch on RMAT-24, mean over 200 launches;
+# see profiles/k_pull_rmat24_traffic.md for the ncu command.
+K_PULL_TRAFFIC_BYTES = 349_962_373
+
+
 def parse_args():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -50,6 +55,9 @@ def parse_args():
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the other configurations (rank 0, N=1 only anyway)")
     ap.add_argument("--config5", action="store_true", help="also run the 105M-vertex web graph (slow to generate)")
+    ap.add_argument("--host-loop", action="store_true",
+                    help="time the host-driven level loop (one launch per level kernel) instead of one "
+                         "CUDA-graph launch per BFS; for profilers that time kernels one launch at a time")
     return ap.parse_args()
 
 
@@ -447,7 +455,7 @@ def run_ours(args, world):
     # events below are recorded on it
     stream = torch.cuda.Stream()
     torch.cuda.set_stream(stream)
-    eng = S.Engine(g, device=local_rank, stream=stream.cuda_stream)
+    eng = S.Engine(g, device=local_rank, stream=stream.cuda_stream, use_graph=2 if args.host_loop else 0)
     depth = torch.empty(V, dtype=torch.int32, device="cuda")
 
     order = replicas.rank_sources(srcs, rank, max(args.steps, args.warmup))
@@ -518,7 +526,10 @@ def run_ours(args, world):
     roof = {"bound": "hbm", "kernel": "k_pull" if dom == 1 else "k_push(+k_push_giant)",
             "achieved": achieved, "peak": peak, "unit": "GB/s",
             "frac": achieved / peak if achieved else None, "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)",
-            "traffic": None, "launches_sampled": nl, "alg_bytes_per_launch": alg / nl if nl else None,
+            # DRAM read+write per k_pull launch, ncu over every k_pull launch of the same
+            # command with --host-loop (profiles/k_pull_rmat24_traffic.md)
+            "traffic": K_PULL_TRAFFIC_BYTES if dom == 1 and args.scale == 24 else None,
+            "launches_sampled": nl, "alg_bytes_per_launch": alg / nl if nl else None,
             "share_of_level_time": dms / (per_dir[0][1] + per_dir[1][1])}
 
     line = {"metric": METRIC, "value": value, "unit": "GTEPS", "n_gpus": world, "steps": args.steps,
