@@ -408,6 +408,69 @@ def extra_config3(nsrc_train=16, nsrc_eval=16):
     return res
 
 
+def extra_config5(stream, nsrc=128, nplain=8):
+    """Web-crawl-like graph 105M / 3.7B streamed out of core with a 24 GB page
+    pool: 128 sources per multi-source launch (alpha/beta, and with the
+    scheduler's out-of-core transfer rule) against the plain engine (one
+    source per launch, alpha/beta + demand paging), warm and cold pools."""
+    import torch
+
+    import scaph_b200 as S
+    from scaph_b200 import workloads
+
+    t0 = time.time()
+    csr, csr_t = workloads.config5()
+    g, gt = workloads.paged(csr), workloads.paged(csr_t)
+    srcs = workloads.random_sources(csr, nsrc, workloads.SEED_BASE + 4)
+    gen_s = time.time() - t0
+    V, E = csr.V, csr.E
+    del csr, csr_t  # the paged copies are what the engines use
+    pool = 24_000_000_000
+    out = {"graph": "web-like: power-law out-degree s=2.1, 90% of edges inside 4096-id blocks", "V": V, "E": E,
+           "out_pages": g.npages, "in_pages": gt.npages, "pool_bytes": pool,
+           "pool_pages": pool // (g.pagesize * 4), "graph_gen_s": round(gen_s, 1), "sources": nsrc}
+    depth = torch.empty((nsrc, V), dtype=torch.int32, device="cuda")
+    for name, direction in (("batched_alpha_beta", S.DIR_ALPHABETA), ("batched_transfer_rule", S.DIR_LEARNED)):
+        eng = S.Engine(g, gt, pool_bytes=pool, direction=direction, stream=stream.cuda_stream)
+        res = {}
+        for regime in ("cold", "warm"):
+            if regime == "cold":
+                eng.evict_all()
+            st = eng.msbfs_device(srcs, depth.data_ptr())
+            tr = eng.msbfs_trace()
+            res[regime] = {"ms": st.ms, "gteps_per_source": nsrc * E / (st.ms / 1e3) / 1e9,
+                           "h2d_bytes": st.h2d_bytes, "zero_copy_bytes": st.zc_bytes,
+                           "page_faults": st.page_faults, "levels": st.levels,
+                           "pcie_bytes_per_level": (st.h2d_bytes + st.zc_bytes) / max(1, st.levels),
+                           "directions": "".join("p" if t["direction"] else "P" for t in tr)}
+        out[name] = res
+        eng.close()
+    # plain engine, one source per launch, on the first sources
+    eng = S.Engine(g, gt, pool_bytes=pool, stream=stream.cuda_stream)
+    d1 = torch.empty(V, dtype=torch.int32, device="cuda")
+    plain = {}
+    for regime in ("cold", "warm"):
+        ms, h2d, zc, exact = 0.0, 0, 0, True
+        for i, s in enumerate(srcs[:nplain]):
+            if regime == "cold":
+                eng.evict_all()
+            st = eng.bfs_device(s, d1.data_ptr())
+            ms += st.ms
+            h2d += st.h2d_bytes
+            zc += st.zc_bytes
+            exact &= bool(torch.equal(d1, depth[i]))
+        plain[regime] = {"ms_per_source": ms / nplain, "gteps": E / (ms / nplain / 1e3) / 1e9,
+                         "pcie_bytes_per_source": (h2d + zc) / nplain, "batched_rows_equal": exact}
+    eng.close()
+    out["plain"] = plain
+    out["plain_sources_timed"] = nplain
+    for regime in ("cold", "warm"):
+        best = max(out["batched_alpha_beta"][regime]["gteps_per_source"],
+                   out["batched_transfer_rule"][regime]["gteps_per_source"])
+        out[f"speedup_vs_plain_{regime}"] = best / plain[regime]["gteps"]
+    return out
+
+
 def extra_pcie(stream):
     """Pinned host->device copy bandwidth (best of 5, 1 GiB)."""
     import torch
@@ -550,7 +613,8 @@ def run_ours(args, world):
         for name, fn in (("pcie", lambda: extra_pcie(stream)), ("config1", extra_config1),
                          ("config4a_batched", lambda: extra_config4a(stream)),
                          ("config4b_mixed", lambda: extra_config4b(stream)),
-                         ("config3_learned", extra_config3)):
+                         ("config3_learned", extra_config3)) + (
+                            (("config5_ooc_batched", lambda: extra_config5(stream)),) if args.config5 else ()):
             try:
                 extras[name] = fn()
             except Exception as exc:  # report, keep the headline line

@@ -171,7 +171,7 @@ __global__ void __launch_bounds__(B) k_bt_push(GraphDev g, const MsDev *ps, cons
 {
     const MsDev s = *ps;
     clear_ahead(s, ctl->act[(ctl->level + 2) % 3]);
-    ms_push_body<NW, B>(g, s);
+    ms_push_body<NW, B>(g, s, RangeList{nullptr, nullptr, nullptr, 0});
 }
 
 template <int NW, int B>
@@ -193,7 +193,7 @@ __global__ void __launch_bounds__(B) k_bt_pull(GraphDev g, const MsDev *ps, cons
 {
     const MsDev s = *ps;
     clear_ahead(s, ctl->act[(ctl->level + 2) % 3]);
-    ms_pull_body<NW, B>(g, s);
+    ms_pull_body<NW, B>(g, s, RangeList{nullptr, nullptr, nullptr, 0});
 }
 
 // End of a level: counters -> next direction, state rotation, loop control.

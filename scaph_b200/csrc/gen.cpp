@@ -274,15 +274,34 @@ int scaph_gen_web(uint32_t V, uint64_t E, double s, uint32_t max_degree, uint32_
     const uint64_t M = idx[V];
     std::unique_ptr<uint32_t[]> ngh(new (std::nothrow) uint32_t[std::max<uint64_t>(1, M)]);
     if (!ngh) return set_error(SCAPH_ENOMEM, "web adjacency buffer");
-    const uint64_t local_t = (uint64_t)(local_frac * 4294967296.0);
+    // Per vertex, round(local_frac * deg) DISTINCT neighbours inside its
+    // block (a walk with a random odd stride over the block's ids, skipping
+    // the vertex itself: a full cycle when the block size is a power of
+    // two, otherwise until the block is exhausted), the rest uniform over
+    // all vertices; local edges that do not fit the block become uniform
+    // ones.  So the deduplicated edge count stays close to E.
     #pragma omp parallel for schedule(dynamic, 1024)
     for (int64_t v = 0; v < (int64_t)V; v++) {
-        uint64_t base = ((uint64_t)v / block) * block;
-        uint64_t span = std::min<uint64_t>(block, V - base);
-        for (uint64_t e = idx[v]; e < idx[v + 1]; e++) {
-            uint64_t h = mix64(seed * 0x94D049BBull + e);
-            if ((h & 0xFFFFFFFFull) < local_t) ngh[e] = (uint32_t)(base + (h >> 32) % span);
-            else ngh[e] = (uint32_t)((h >> 32) % V);
+        const uint64_t base = ((uint64_t)v / block) * block;
+        const uint64_t span = std::min<uint64_t>(block, V - base);
+        const uint64_t d = idx[v + 1] - idx[v];
+        uint64_t k = (uint64_t)(local_frac * (double)d + 0.5);
+        if (k > span - 1) k = span - 1;
+        const uint64_t h0 = mix64(seed * 0xD6E8FEB86659FD93ull + (uint64_t)v);
+        const uint64_t off = (h0 >> 32) % span;
+        uint64_t stride = (h0 & 0xFFFFFFFFull) % span;
+        stride |= 1;  // odd: coprime with a power-of-two block
+        uint64_t e = idx[v], pos = off, steps = 0;
+        while (e < idx[v] + k && steps < span) {
+            const uint64_t u = base + pos;
+            pos = (pos + stride) % span;
+            steps++;
+            if (u == (uint64_t)v) continue;
+            ngh[e++] = (uint32_t)u;
+        }
+        for (; e < idx[v + 1]; e++) {
+            const uint64_t h = mix64(seed * 0x94D049BBull + e);
+            ngh[e] = (uint32_t)((h >> 32) % V);
         }
     }
     return finalize_csr(V, idx, ngh.get(), out);

@@ -227,7 +227,7 @@ __device__ __forceinline__ void ms_send4(const MsDev &s, const uint32_t (&u)[4],
 // push: active vertices send their frontier masks to out-neighbours
 // ---------------------------------------------------------------------------
 template <int NW, int B>
-__device__ __forceinline__ void ms_push_body(const GraphDev &g, const MsDev &s)
+__device__ __forceinline__ void ms_push_body(const GraphDev &g, const MsDev &s, const RangeList &rl)
 {
     __shared__ PageDev lp[kLutPages];
     __shared__ uint32_t lc[kLutCoarse];
@@ -238,10 +238,13 @@ __device__ __forceinline__ void ms_push_body(const GraphDev &g, const MsDev &s)
     const PageLut lut = kc::stage_lut<B>(g, lp, lc);
     __syncthreads();
     MsAcc a;
-    const uint32_t ntiles = (s.nwords + kMsTileWords - 1) / kMsTileWords;
+    const uint32_t ntiles = rl.n ? rl.tile0[rl.n] : (s.nwords + kMsTileWords - 1) / kMsTileWords;
     for (uint32_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-        const uint32_t w = tile * kMsTileWords + threadIdx.x;
-        uint32_t f = (threadIdx.x < kMsTileWords && w < s.nwords) ? s.act_cur[w] : 0u;
+        uint32_t rlo = 0, rhi = s.V, local;
+        range_of_tile(rl, tile, rlo, rhi, local);
+        const uint32_t rwhi = (uint32_t)(((unsigned long long)rhi + 31) >> 5);
+        const uint32_t w = (rlo >> 5) + local * kMsTileWords + threadIdx.x;
+        uint32_t f = (threadIdx.x < kMsTileWords && w < rwhi) ? s.act_cur[w] & range_mask(w, rlo, rhi) : 0u;
         if (!__syncthreads_or(f != 0)) continue;
         uint32_t total;
         uint32_t off = kc::block_exclusive_scan<B>(__popc(f), wsum, total);
@@ -390,7 +393,7 @@ __device__ __forceinline__ void ms_finalize_body(const MsDev &s)
 // pull: incomplete vertices OR the frontier masks of their in-neighbours
 // ---------------------------------------------------------------------------
 template <int NW, int B>
-__device__ __forceinline__ void ms_pull_body(const GraphDev &g, const MsDev &s)
+__device__ __forceinline__ void ms_pull_body(const GraphDev &g, const MsDev &s, const RangeList &rl)
 {
     __shared__ PageDev lp[kLutPages];
     __shared__ uint32_t lc[kLutCoarse];
@@ -405,15 +408,18 @@ __device__ __forceinline__ void ms_pull_body(const GraphDev &g, const MsDev &s)
     const Mask<NW> all = all_mask<NW>(s);
     __syncthreads();
     MsAcc a;
-    const uint32_t ntiles = (s.nwords + kMsTileWords - 1) / kMsTileWords;
+    const uint32_t ntiles = rl.n ? rl.tile0[rl.n] : (s.nwords + kMsTileWords - 1) / kMsTileWords;
     for (uint32_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-        const uint32_t wbase = tile * kMsTileWords;
+        uint32_t rlo = 0, rhi = s.V, local;
+        range_of_tile(rl, tile, rlo, rhi, local);
+        const uint32_t rwhi = (uint32_t)(((unsigned long long)rhi + 31) >> 5);
+        const uint32_t wbase = (rlo >> 5) + local * kMsTileWords;
         const uint32_t w = wbase + threadIdx.x;
         uint32_t f = 0;
         if (threadIdx.x < kMsTileWords) {
             fnd[threadIdx.x] = 0;
             dne[threadIdx.x] = 0;
-            if (w < s.nwords) f = s.inc[w];
+            if (w < rwhi) f = s.inc[w] & range_mask(w, rlo, rhi);
         }
         if (!__syncthreads_or(f != 0)) continue;
         uint32_t total;
@@ -563,9 +569,11 @@ __device__ __forceinline__ void ms_pull_body(const GraphDev &g, const MsDev &s)
             }
             __syncthreads();
         }
-        if (threadIdx.x < kMsTileWords && w < s.nwords) {
-            if (fnd[threadIdx.x]) s.act_nxt[w] = fnd[threadIdx.x];
-            if (dne[threadIdx.x]) s.inc[w] &= ~dne[threadIdx.x];
+        if (threadIdx.x < kMsTileWords && w < rwhi) {
+            // OR / AND-NOT: the word may be shared with a range of another
+            // page batch of this level
+            if (fnd[threadIdx.x]) atomicOr(&s.act_nxt[w], fnd[threadIdx.x]);
+            if (dne[threadIdx.x]) atomicAnd(&s.inc[w], ~dne[threadIdx.x]);
         }
         __syncthreads();
     }
@@ -574,9 +582,9 @@ __device__ __forceinline__ void ms_pull_body(const GraphDev &g, const MsDev &s)
 
 // host-loop kernels (MsDev by value, one launch per phase and level)
 template <int NW>
-__global__ void __launch_bounds__(kMsBlock) k_ms_push(GraphDev g, MsDev s)
+__global__ void __launch_bounds__(kMsBlock) k_ms_push(GraphDev g, MsDev s, RangeList rl)
 {
-    ms_push_body<NW, kMsBlock>(g, s);
+    ms_push_body<NW, kMsBlock>(g, s, rl);
 }
 
 template <int NW>
@@ -592,9 +600,9 @@ __global__ void __launch_bounds__(kMsBlock) k_ms_finalize(MsDev s)
 }
 
 template <int NW>
-__global__ void __launch_bounds__(kMsBlock) k_ms_pull(GraphDev g, MsDev s)
+__global__ void __launch_bounds__(kMsBlock) k_ms_pull(GraphDev g, MsDev s, RangeList rl)
 {
-    ms_pull_body<NW, kMsBlock>(g, s);
+    ms_pull_body<NW, kMsBlock>(g, s, rl);
 }
 
 // clears the frontier masks of the source vertices (left over from an

@@ -28,6 +28,7 @@ struct MsState {
     uint32_t *out = nullptr;  // internal depth output [128][V] when the caller wants host memory
     size_t out_words = 0;
     std::vector<scaph_level_trace> trace;
+    std::vector<uint64_t> h2d;  // out of core: page bytes copied or read zero-copy per level
 };
 
 void ms_release(MsState *m)
@@ -95,6 +96,68 @@ int ms_alloc(scaph_engine *e, int nw)
 
 }  // namespace
 
+// Page traffic (ms) a push over `act` and a pull over `inc` would cause.
+static int ms_transfer_ms(scaph_engine *e, const uint32_t *act, const uint32_t *inc, int grid, double &t_push,
+                          double &t_pull)
+{
+    const int gin = e->symmetric ? 0 : 1;
+    for (int d = 0; d < 2; d++) {
+        std::vector<int> need;
+        std::vector<uint32_t> datas;
+        const int gid = d == 0 ? 0 : gin;
+        int rc = pager_page_counts(e->pager, gid, d == 0 ? act : inc, false,
+                                   d == 0 || !e->d_indeg ? e->d_degree : e->d_indeg, 1, grid, e->st, need, datas);
+        if (rc) return rc;
+        std::vector<uint32_t> cnt(datas.size(), 0);
+        for (int p : need) cnt[p] = 1;
+        (d == 0 ? t_push : t_pull) =
+            pager_transfer_ms(e->pager, gid, cnt.data(), datas.data(), (int)cnt.size(), e->cfg.compact_threshold);
+    }
+    return SCAPH_OK;
+}
+
+// One out-of-core level: push sends from the pages holding frontier
+// vertices (giant chunks after each page batch, whose pool they address),
+// then one finalize; pull reads the in-pages holding incomplete vertices.
+template <int NW>
+static int ms_ooc_level(scaph_engine *e, const MsDev &s, int dir, int level, int grid, uint64_t &launches,
+                        std::vector<uint64_t> &h2d)
+{
+    cudaStream_t st = e->st;
+    const int gid = (dir == 0 || e->symmetric) ? 0 : 1;
+    std::vector<int> needed;
+    std::vector<uint32_t> datas;
+    int rc = pager_page_counts(e->pager, gid, dir == 0 ? s.act_cur : s.inc, false,
+                               dir == 0 || !e->d_indeg ? e->d_degree : e->d_indeg, 1, grid, st, needed, datas);
+    if (rc) return rc;
+    PageLaunch fn;
+    fn.run = [&](const GraphDev &gv, int, const RangeList &rl, uint32_t, cudaStream_t cs) -> int {
+        if (dir == 0) {
+            k_ms_push<NW><<<grid, kMsBlock, 0, cs>>>(gv, s, rl);
+            k_ms_push_giant<NW><<<grid, kMsBlock, 0, cs>>>(gv, s);
+            SCAPH_CUDA(cudaMemsetAsync(&s.ctr->giant, 0, sizeof(unsigned int), cs));
+            launches += 2;
+        } else {
+            k_ms_pull<NW><<<grid, kMsBlock, 0, cs>>>(gv, s, rl);
+            launches += 1;
+        }
+        SCAPH_CUDA(cudaGetLastError());
+        return SCAPH_OK;
+    };
+    uint64_t h0, z0, f0, pf, hits, lh;
+    pager_counters(e->pager, &h0, &z0, &f0, &pf, &hits, &lh);
+    if ((rc = pager_run_level(e->pager, gid, needed, datas, e->cfg.compact_threshold, fn, st))) return rc;
+    if (dir == 0) {
+        k_ms_finalize<NW><<<grid, kMsBlock, 0, st>>>(s);
+        launches += 1;
+    }
+    uint64_t h1, z1, f1;
+    pager_counters(e->pager, &h1, &z1, &f1, &pf, &hits, &lh);
+    if ((size_t)level >= h2d.size()) h2d.resize(level + 1, 0);
+    h2d[level] = (h1 - h0) + (z1 - z0);
+    return SCAPH_OK;
+}
+
 template <int NW>
 static int ms_run(scaph_engine *e, const uint32_t *srcs, int nsrc, uint32_t *out, scaph_bfs_stats *stats)
 {
@@ -144,12 +207,24 @@ static int ms_run(scaph_engine *e, const uint32_t *srcs, int nsrc, uint32_t *out
     int dir = 0, cur = 0, level = 0, npush = 0, npull = 0, planes_used = 0;
     uint32_t err = 0;
     m->trace.clear();
+    m->h2d.clear();
+    if (e->pager) pager_reset_counters(e->pager);
     while (nf > 0 && level < kMaxLevels && (uint64_t)level + 1 < e->unreached) {
         const uint64_t mu = e->E > done_e ? e->E - done_e : 0;
         switch (e->cfg.direction) {
         case SCAPH_DIR_PUSH: dir = 0; break;
         case SCAPH_DIR_PULL: dir = level == 0 ? 0 : 1; break;
         default: dir = level == 0 ? 0 : alpha_beta_next(dir, nf, prev_nf, mf, mu, V, alpha, beta); break;
+        }
+        if (e->pager && e->cfg.direction == SCAPH_DIR_LEARNED && level > 0) {
+            // the scheduler's out-of-core rule: the page traffic each
+            // direction would cause is known exactly; it overrides the
+            // kernel-time choice when one side clearly dominates
+            double tp = 0, tq = 0;
+            int rc = ms_transfer_ms(e, m->act[cur], m->inc, grid, tp, tq);
+            if (rc) return rc;
+            if (tp > 2 * tq + 1.0) dir = 1;
+            else if (tq > 2 * tp + 1.0) dir = 0;
         }
         const uint32_t d = (uint32_t)level + 1;
         for (int k = 0; k < kMsPlanes; k++) {
@@ -167,14 +242,22 @@ static int ms_run(scaph_engine *e, const uint32_t *srcs, int nsrc, uint32_t *out
         s.act_nxt = m->act[cur ^ 1];
         s.ctr = m->d_ctr + level;
         s.level = (uint32_t)level;
-        if (dir == 0) {
-            k_ms_push<NW><<<grid, kMsBlock, 0, st>>>(e->dout.view, s);
+        const RangeList whole{nullptr, nullptr, nullptr, 0};
+        if (e->pager) {
+            // out of core: the pages holding frontier vertices (push) or
+            // incomplete vertices (pull), in batches the pager makes ready
+            // (resident, zero-copy, demand copies)
+            int rc = ms_ooc_level<NW>(e, s, dir, level, grid, launches, m->h2d);
+            if (rc) return rc;
+            if (dir == 0) npush++; else npull++;
+        } else if (dir == 0) {
+            k_ms_push<NW><<<grid, kMsBlock, 0, st>>>(e->dout.view, s, whole);
             k_ms_push_giant<NW><<<grid, kMsBlock, 0, st>>>(e->dout.view, s);
             k_ms_finalize<NW><<<grid, kMsBlock, 0, st>>>(s);
             launches += 3;
             npush++;
         } else {
-            k_ms_pull<NW><<<grid, kMsBlock, 0, st>>>(e->gin(), s);
+            k_ms_pull<NW><<<grid, kMsBlock, 0, st>>>(e->gin(), s, whole);
             launches += 1;
             npull++;
         }
@@ -192,10 +275,11 @@ static int ms_run(scaph_engine *e, const uint32_t *srcs, int nsrc, uint32_t *out
         t.unvisited_edges = mu;
         t.next = c.active;
         t.edges_inspected = c.inspected;
-        // SURVEY 8(d) unit for MS-BFS: headers + adjacency of the vertices
-        // with a nonzero frontier mask, plus a read and a write of a mask per
-        // vertex per level
+        // algorithmic bytes of an MS-BFS level: headers + adjacency of the
+        // vertices with a nonzero frontier mask (push) or the in-edges read
+        // (pull), plus a read and a write of a mask per vertex
         t.alg_bytes = dir == 0 ? nf * 12 + mf * 4 + 2ull * NW * 8 * V : c.inspected * 4 + 2ull * NW * 8 * V;
+        if ((size_t)level < m->h2d.size()) t.h2d_bytes = m->h2d[level];
         m->trace.push_back(t);
         alg += t.alg_bytes;
         insp += c.inspected;
@@ -223,6 +307,13 @@ static int ms_run(scaph_engine *e, const uint32_t *srcs, int nsrc, uint32_t *out
         float ms = 0;
         cudaEventElapsedTime(&ms, e->ev_start, e->ev_stop);
         stats->ms = ms;
+        if (e->pager) {
+            uint64_t h2d, zc, faults, pf, hits, lh;
+            pager_counters(e->pager, &h2d, &zc, &faults, &pf, &hits, &lh);
+            stats->h2d_bytes = h2d;
+            stats->zc_bytes = zc;
+            stats->page_faults = faults;
+        }
         stats->levels = level;
         stats->push_levels = npush;
         stats->pull_levels = npull;
@@ -243,7 +334,6 @@ extern "C" int scaph_msbfs(scaph_engine *e, const uint32_t *srcs, int nsrc, uint
     if (nsrc < 1 || nsrc > SCAPH_MSBFS_MAX) return set_error(SCAPH_EINVAL, "nsrc %d outside 1..%d", nsrc, SCAPH_MSBFS_MAX);
     for (int i = 0; i < nsrc; i++)
         if (srcs[i] >= e->V) return set_error(SCAPH_EINVAL, "source %u out of range (V=%u)", srcs[i], e->V);
-    if (e->pager) return set_error(SCAPH_EUNSUPPORTED, "multi-source BFS needs the graph resident");
     SCAPH_CUDA(cudaSetDevice(e->device));
     const int nw = nsrc > 64 ? 2 : 1;
     int rc = ms_alloc(e, nw);

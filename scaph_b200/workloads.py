@@ -73,10 +73,13 @@ def config4b(ngraphs: int = 32, nqueries: int = 256, scales=(14, 22), edgefactor
     return graphs, queries, shapes
 
 
-def config5(V: int = 105_000_000, E: int = 3_700_000_000, max_degree: int = 1 << 20):
+def config5(V: int = 105_000_000, E: int = 3_700_000_000, max_degree: int = 4096):
     """Directed web-crawl-like graph: out-degree power law s=2.1, 90 % of the
-    edges inside the source's block of 4096 consecutive ids, the rest uniform;
-    returns (out-edge CSR, in-edge CSR)."""
+    edges inside the source's block of 4096 consecutive ids (distinct ids),
+    the rest uniform; returns (out-edge CSR, in-edge CSR).  Out-degrees are
+    capped at the block size so that a vertex's local edges fit its block
+    (with a higher cap the hubs' surplus would have to leave the block and the
+    local share would fall below 90 %)."""
     csr = Csr.web(V, E, 2.1, max_degree, 4096, 0.9, seed=SEED_BASE + 4)
     return csr, csr.transpose()
 

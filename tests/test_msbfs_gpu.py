@@ -84,3 +84,34 @@ def test_msbfs_matches_single_source_engine_and_trace():
     tr = eng.msbfs_trace()
     assert len(tr) == st.levels and st.reached == int((d != S.UNREACHED).sum())
     eng.close()
+
+
+@pytest.mark.parametrize("direction", [S.DIR_ALPHABETA, S.DIR_PUSH, S.DIR_PULL, S.DIR_LEARNED])
+def test_msbfs_out_of_core(direction):
+    """Pool of a third of the out+in pages: the multi-source levels run on
+    page batches (resident, zero-copy, demand copies); depths still exact.
+    DIR_LEARNED adds the out-of-core transfer rule to alpha/beta."""
+    csr = S.Csr.powerlaw(30000, 400000, 1.9, 3000, seed=G.SEED + 23)
+    g = S.PagedGraph.from_csr(csr, pagesize_words=1 << 12)
+    gt = S.PagedGraph.from_csr(csr.transpose(), pagesize_words=1 << 12)
+    total = g.npages + gt.npages
+    pool = (total // 3) * g.pagesize * 4
+    eng = S.Engine(g, gt, pool_bytes=pool, direction=direction, compact_threshold=2)
+    srcs = G.sources(csr, 100, 23)
+    for cold in (True, False):
+        if cold:
+            eng.evict_all()
+        _, st = check_batch(csr, eng, srcs)
+        assert st.h2d_bytes + st.zc_bytes > 0
+        assert st.push_levels + st.pull_levels == st.levels
+    tr = eng.msbfs_trace()
+    assert sum(t["h2d_bytes"] for t in tr) > 0 or not cold
+    eng.close()
+
+
+def test_msbfs_out_of_core_symmetric_64():
+    csr = S.Csr.rmat(14, 16, seed=G.SEED + 24)
+    g = S.PagedGraph.from_csr(csr, pagesize_words=1 << 13)
+    eng = S.Engine(g, pool_bytes=(g.npages // 2) * g.pagesize * 4)
+    check_batch(csr, eng, G.sources(csr, 64, 24))
+    eng.close()
