@@ -54,7 +54,9 @@ def parse_args():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the other configurations (rank 0, N=1 only anyway)")
-    ap.add_argument("--config5", action="store_true", help="also run the 105M-vertex web graph (slow to generate)")
+    ap.add_argument("--no-config5", action="store_true",
+                    help="skip the 105M-vertex / 3.7B-edge web graph (about a minute to generate)")
+    ap.add_argument("--only-extra", default=None, help=argparse.SUPPRESS)
     ap.add_argument("--host-loop", action="store_true",
                     help="time the host-driven level loop (one launch per level kernel) instead of one "
                          "CUDA-graph launch per BFS; for profilers that time kernels one launch at a time")
@@ -609,14 +611,19 @@ def run_ours(args, world):
     eng_h.close()
     eng.close()
     if rank == 0 and world == 1 and not args.no_extras:
+        # each configuration in its own process: a fresh host heap for the big
+        # generated graphs, and a failure there cannot take the headline down
         extras = {}
-        for name, fn in (("pcie", lambda: extra_pcie(stream)), ("config1", extra_config1),
-                         ("config4a_batched", lambda: extra_config4a(stream)),
-                         ("config4b_mixed", lambda: extra_config4b(stream)),
-                         ("config3_learned", extra_config3)) + (
-                            (("config5_ooc_batched", lambda: extra_config5(stream)),) if args.config5 else ()):
+        names = ["pcie", "config1", "config4a_batched", "config4b_mixed", "config3_learned"]
+        if not args.no_config5:
+            names.append("config5_ooc_batched")
+        for name in names:
             try:
-                extras[name] = fn()
+                r = subprocess.run([sys.executable, os.path.abspath(__file__), "--only-extra", name],
+                                   capture_output=True, text=True, timeout=1200)
+                last = [l for l in r.stdout.splitlines() if l.startswith("{")]
+                extras[name] = json.loads(last[-1]) if r.returncode == 0 and last else \
+                    {"error": f"exit {r.returncode}: {r.stderr[-400:]}"}
             except Exception as exc:  # report, keep the headline line
                 extras[name] = {"error": f"{type(exc).__name__}: {exc}"}
             print(f"[bench] {name}: {json.dumps(extras[name])[:300]}", file=sys.stderr, flush=True)
@@ -628,9 +635,30 @@ def run_ours(args, world):
         print(json.dumps(line), flush=True)
 
 
+EXTRAS = {
+    "pcie": lambda st: extra_pcie(st),
+    "config1": lambda st: extra_config1(),
+    "config4a_batched": lambda st: extra_config4a(st),
+    "config4b_mixed": lambda st: extra_config4b(st),
+    "config3_learned": lambda st: extra_config3(),
+    "config5_ooc_batched": lambda st: extra_config5(st),
+}
+
+
+def run_extra(name):
+    import torch
+
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    print(json.dumps(EXTRAS[name](stream)), flush=True)
+
+
 def main():
     args = parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
+    if args.only_extra:
+        run_extra(args.only_extra)
+        return
     if args.impl == "reference":
         run_reference(args, world)
     else:
