@@ -40,8 +40,13 @@ namespace {
 #define SCAPH_PULL_SERIAL 4
 #endif
 constexpr int kPushTileWords = 128;                  // frontier-bitmap words per push tile
-constexpr int kPullTileWords = 128;                  // visited-bitmap words per pull tile
+#ifndef SCAPH_PULL_MINB
+#define SCAPH_PULL_MINB 1280
+#endif
+constexpr int kPullTileWords = 128;                  // visited-bitmap words per pull tile (the range-list tile)
+constexpr int kPullMinThreads = SCAPH_PULL_MINB;     // resident threads per SM the pull kernel is compiled for
 constexpr uint32_t kPullSerial = SCAPH_PULL_SERIAL;  // in-edges each lane probes before the warp helps
+static_assert(kPullSerial == kPullHead, "phase A reads one dense head row of in-edges");
 
 template <int BLOCK>
 __device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t x, uint32_t *wsum, uint32_t &total)
@@ -415,17 +420,35 @@ __device__ __forceinline__ void pull_body(const GraphDev &g, const BfsDev &s, ui
             int p = 0;
             if (k < total) {
                 v = q[k];
-                p = lut.of(v);
-                const PageDev pd = lut.pages[p];
-                if (pd.base != kNotResident) {
-                    const uint32_t *node = g.pool + pd.base + 3ull * (v - pd.left);
-                    const uint32_t pos = node[1];
-                    len = node[2];
-                    st = pd.base + 3ull * pd.nodenum + pos;
-                    t.headers++;
-                    uint32_t u[kPullSerial];
+                uint32_t u[kPullSerial];
+                bool ok = true;
+                if (s.head) {
+                    // dense rows: the in-degree and the first in-edges of
+                    // consecutive vertices, two independent coalesced loads;
+                    // the page is read only if these do not decide
+                    len = __ldg(&s.indeg[v]);
+                    const uint4 h = ld_nc_v4(s.head + (size_t)kPullHead * v);
+                    u[0] = h.x;
+                    u[1] = h.y;
+                    u[2] = h.z;
+                    u[3] = h.w;
+                } else {
+                    p = lut.of(v);
+                    const PageDev pd = lut.pages[p];
+                    if (pd.base != kNotResident) {
+                        const uint32_t *node = g.pool + pd.base + 3ull * (v - pd.left);
+                        len = node[2];
+                        st = pd.base + 3ull * pd.nodenum + node[1];
+                        t.headers++;
 #pragma unroll
-                    for (uint32_t j = 0; j < kPullSerial; j++) u[j] = j < len ? __ldg(&g.pool[st + j]) : 0xFFFFFFFFu;
+                        for (uint32_t j = 0; j < kPullSerial; j++)
+                            u[j] = j < len ? __ldg(&g.pool[st + j]) : 0xFFFFFFFFu;
+                    } else {
+                        atomicOr(&s.ctr->error, 4u);
+                        ok = false;
+                    }
+                }
+                if (ok) {
                     uint32_t hit = 0;
 #pragma unroll
                     for (uint32_t j = 0; j < kPullSerial; j++)
@@ -440,13 +463,27 @@ __device__ __forceinline__ void pull_body(const GraphDev &g, const BfsDev &s, ui
                         const uint32_t dv = __ldg(&s.degree[v]);
                         t.next++;
                         t.next_edges += dv;
-                        if (s.page_nodes) hist_add(sm, s, hist_same ? p : page_of(s.hg, v), dv + 3);
+                        if (s.page_nodes) {
+                            if (s.head && hist_same) p = lut.of(v);
+                            hist_add(sm, s, hist_same ? p : page_of(s.hg, v), dv + 3);
+                        }
                     } else {
                         t.inspected += min(len, kPullSerial);
                         need = len > kPullSerial;
+                        if (need && s.head) {
+                            // phase B needs where the list lives
+                            p = lut.of(v);
+                            const PageDev pd = lut.pages[p];
+                            if (pd.base != kNotResident) {
+                                const uint32_t *node = g.pool + pd.base + 3ull * (v - pd.left);
+                                st = pd.base + 3ull * pd.nodenum + node[1];
+                                t.headers++;
+                            } else {
+                                atomicOr(&s.ctr->error, 4u);
+                                need = 0;
+                            }
+                        }
                     }
-                } else {
-                    atomicOr(&s.ctr->error, 4u);
                 }
             }
             uint32_t nb;
@@ -464,7 +501,7 @@ __device__ __forceinline__ void pull_body(const GraphDev &g, const BfsDev &s, ui
                 const bool mine = e < nb;
                 unsigned long long a = 0, b = 0;
                 if (mine) {
-                    a = bq_st[e] + kPullSerial;
+                    a = bq_st[e] + (s.head_ranked ? 0u : kPullSerial);
                     b = bq_st[e] + bq_len[e];
                 }
                 const unsigned long long qa = a >> 2, qb = (b + 3) >> 2;
@@ -588,7 +625,7 @@ __global__ void __launch_bounds__(BLOCK) k_push_giant(GraphDev g, BfsDev s)
 }
 
 template <int BLOCK>
-__global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) k_pull(GraphDev g, BfsDev s, uint32_t vlo, uint32_t vhi,
+__global__ void __launch_bounds__(BLOCK, kPullMinThreads / BLOCK) k_pull(GraphDev g, BfsDev s, uint32_t vlo, uint32_t vhi,
                                                             RangeList rl)
 {
     pull_body<BLOCK>(g, s, vlo, vhi, rl);
@@ -612,7 +649,7 @@ __global__ void __launch_bounds__(BLOCK) k_push_giant_g(GraphDev g, BfsGraphArgs
 }
 
 template <int BLOCK>
-__global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) k_pull_g(GraphDev g, BfsGraphArgs a)
+__global__ void __launch_bounds__(BLOCK, kPullMinThreads / BLOCK) k_pull_g(GraphDev g, BfsGraphArgs a)
 {
     const BfsDev s = level_state(a);
     clear_third(a, s.level);

@@ -49,6 +49,11 @@ struct Graph {
 bool page_cut(const uint64_t *idx, uint32_t V, uint32_t left, uint32_t pagesize,
               int weighted, uint32_t *right);
 
+// Rows of `width` adjacency entries of every vertex of a paged graph
+// (out[v*width + j], 0xFFFFFFFF past the vertex's degree): the first ones,
+// or, with rank != null, the ones with the largest rank[] (ties: list order).
+void adjacency_heads(const Graph &g, uint32_t width, uint32_t *out, const uint32_t *rank = nullptr);
+
 uint32_t *alloc_words(size_t words);  // zeroed, 4 KiB aligned
 void free_words(uint32_t *p);
 

@@ -6,6 +6,7 @@
 
 namespace scaph {
 
+constexpr uint32_t kPullHead = 4;  // dense in-edge row per vertex read by pull phase A
 constexpr unsigned long long kNotResident = ~0ull;
 constexpr uint32_t kNoParent = 0xFFFFFFFFu;
 constexpr int kHistCap = 512;           // pages histogrammed in shared memory
@@ -72,6 +73,14 @@ struct BfsDev {
     uint32_t V;
     uint32_t nwords;           // (V + 31) / 32
     GraphDev hg;               // out-edge graph whose pages the histogram counts
+    // pull: kPullHead in-edges of every vertex (the first ones, or the ones
+    // of largest out-degree), kPullHead words per vertex (16-byte aligned
+    // rows, 0xFFFFFFFF past the in-degree), and the in-degrees; null when
+    // the caller keeps no such copy
+    const uint32_t *head;
+    const uint32_t *indeg;
+    uint32_t head_ranked;      // head rows are not the list's first edges:
+                               // phase B scans the whole list
 };
 
 // Graph mode: state of one traversal kept on the device, so a whole BFS runs

@@ -24,7 +24,14 @@
 #include "engine.h"
 #include "kernels.h"
 
-using namespace scaph;
+using // Pull phase A's first probes: 0 = the first in-edges, read from the pages;
+// 1 = the same edges from dense per-vertex rows (16 B per vertex of device
+// memory); 2 = dense rows of the in-neighbours with the largest out-degree.
+#ifndef SCAPH_PULL_HEAD
+#define SCAPH_PULL_HEAD 2
+#endif
+
+namespace scaph;
 
 namespace scaph {
 
@@ -115,6 +122,9 @@ BfsDev scaph_engine::base_state(uint32_t *dd, uint32_t *dp) const
     s.V = V;
     s.nwords = nwords;
     s.hg = out_view();
+    s.head = d_head;
+    s.indeg = d_indeg;
+    s.head_ranked = head_ranked ? 1u : 0u;
     return s;
 }
 
@@ -163,6 +173,19 @@ int scaph_engine::create(const Graph *g_, const Graph *gt_, const scaph_config *
         const size_t npi = (gt ? gt->pages.size() : g->pages.size()) + 1;
         SCAPH_CUDA(cudaMalloc(&d_pcnt, npi * 4));
         SCAPH_CUDA(cudaMalloc(&d_pdatas, npi * 4));
+    }
+
+    if (SCAPH_PULL_HEAD) {
+        // pull phase A's dense rows: the first in-edges of every vertex
+        // in-neighbours of largest out-degree first: the likeliest to be in
+        // a frontier (hubs join it early), so most vertices settle on the
+        // first probe
+        const Graph &gi = gt ? *gt : *g;
+        std::vector<uint32_t> head((size_t)V * kPullHead);
+        adjacency_heads(gi, kPullHead, head.data(), SCAPH_PULL_HEAD == 2 ? g->degree.data() : nullptr);
+        head_ranked = SCAPH_PULL_HEAD == 2;
+        SCAPH_CUDA(cudaMalloc(&d_head, head.size() * 4));
+        SCAPH_CUDA(cudaMemcpy(d_head, head.data(), head.size() * 4, cudaMemcpyHostToDevice));
     }
 
     // vertices no edge reaches (in-degree 0) are never discovered: they start
@@ -215,6 +238,7 @@ void scaph_engine::destroy()
     pager_release(pager);
     pager = nullptr;
     cudaFree(d_indeg);
+    cudaFree(d_head);
     cudaFree(d_snap);
     cudaFree(d_pcnt);
     cudaFree(d_pdatas);

@@ -142,6 +142,8 @@ struct scaph_engine {
     scaph::MsState *ms = nullptr;  // allocated by the first scaph_msbfs call
     scaph::Pager *pager = nullptr;  // out-of-core mode: pool smaller than the graph
     uint32_t *d_indeg = nullptr;    // in-degree per vertex (pull page statistics)
+    uint32_t *d_head = nullptr;     // kPullHead in-edges per vertex (pull phase A)
+    bool head_ranked = false;       // d_head holds the top in-neighbours by out-degree
     std::vector<uint64_t> level_h2d;  // page bytes copied per level of the last run
     scaph_bfs_stats pager_stats{};
     // learned scheduler / training traces

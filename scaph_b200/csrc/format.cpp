@@ -8,6 +8,7 @@
 #include <sys/stat.h>
 
 #include <algorithm>
+#include <functional>
 #include <cstdlib>
 #include <cstring>
 #include <memory>
@@ -151,6 +152,47 @@ static int cut_pages(const scaph_csr *csr, uint32_t pagesize, int weighted,
     }
     return SCAPH_OK;
 }
+
+namespace scaph {
+
+void adjacency_heads(const Graph &g, uint32_t width, uint32_t *out, const uint32_t *rank)
+{
+    const uint32_t ew = g.weighted ? 2 : 1;
+    const int np = (int)g.pages.size();
+    #pragma omp parallel for schedule(dynamic, 1)
+    for (int p = 0; p < np; p++) {
+        const scaph_page_info &pi = g.pages[p];
+        const uint32_t *pg = g.page(p);
+        const uint32_t *edges = pg + 3ull * pi.nodenum;
+        std::vector<std::pair<uint32_t, uint32_t>> top;  // (rank, neighbour)
+        for (uint32_t i = 0; i < pi.nodenum; i++) {
+            const uint32_t v = pi.left + i, idx = pg[3 * i + 1], len = pg[3 * i + 2];
+            uint32_t *row = out + (size_t)v * width;
+            if (!rank || len <= width) {
+                for (uint32_t j = 0; j < width; j++) row[j] = j < len ? edges[(uint64_t)(idx + j) * ew] : 0xFFFFFFFFu;
+                continue;
+            }
+            // the `width` neighbours of largest rank, largest first
+            top.clear();
+            for (uint32_t k = 0; k < len; k++) {
+                const uint32_t u = edges[(uint64_t)(idx + k) * ew];
+                const uint32_t r = rank[u];
+                if (top.size() < width) {
+                    top.emplace_back(r, u);
+                    std::push_heap(top.begin(), top.end(), std::greater<>());
+                } else if (r > top.front().first) {
+                    std::pop_heap(top.begin(), top.end(), std::greater<>());
+                    top.back() = {r, u};
+                    std::push_heap(top.begin(), top.end(), std::greater<>());
+                }
+            }
+            std::sort(top.begin(), top.end(), std::greater<>());
+            for (uint32_t j = 0; j < width; j++) row[j] = top[j].second;
+        }
+    }
+}
+
+}  // namespace scaph
 
 extern "C" {
 
