@@ -40,6 +40,9 @@ namespace {
 #define SCAPH_PULL_SERIAL 4
 #endif
 constexpr int kPushTileWords = 128;                  // frontier-bitmap words per push tile
+#ifndef SCAPH_PULL_FIRST_PROBE
+#define SCAPH_PULL_FIRST_PROBE 1
+#endif
 #ifndef SCAPH_PULL_MINB
 #define SCAPH_PULL_MINB 1280
 #endif
@@ -450,9 +453,23 @@ __device__ __forceinline__ void pull_body(const GraphDev &g, const BfsDev &s, ui
                 }
                 if (ok) {
                     uint32_t hit = 0;
+#if SCAPH_PULL_FIRST_PROBE
+                    // ranked rows: the top in-neighbour alone first (it
+                    // settles most vertices), the other three only on a miss
+                    if (s.head_ranked) {
+                        if (u[0] < s.V && test_bit(s.front, u[0])) hit = 1u;
+                        else {
 #pragma unroll
-                    for (uint32_t j = 0; j < kPullSerial; j++)
-                        if (u[j] < s.V && test_bit(s.front, u[j])) hit |= 1u << j;
+                            for (uint32_t j = 1; j < kPullSerial; j++)
+                                if (u[j] < s.V && test_bit(s.front, u[j])) hit |= 1u << j;
+                        }
+                    } else
+#endif
+                    {
+#pragma unroll
+                        for (uint32_t j = 0; j < kPullSerial; j++)
+                            if (u[j] < s.V && test_bit(s.front, u[j])) hit |= 1u << j;
+                    }
                     if (hit) {
                         const uint32_t j = __ffs(hit) - 1;
                         t.inspected += j + 1;
