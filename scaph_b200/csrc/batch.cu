@@ -442,6 +442,9 @@ int scaph_batch::build_graph(uint32_t *out)
     base.level = 0;
     base.all[0] = ~0ull;
     base.all[1] = nw == 2 ? ~0ull : 0ull;
+    base.head = e->d_head;
+    base.indeg = e->d_indeg;
+    base.head_ranked = e->head_ranked ? 1u : 0u;
 
     SCAPH_CUDA(cudaGraphCreate(&graph, 0));
     cudaGraphConditionalHandle h_loop, h_push, h_pull;

@@ -139,6 +139,12 @@ struct MsDev {
     uint32_t giant_cap;
     uint32_t V, nwords, level;
     unsigned long long all[2];  // source bits in use
+    // pull phase A: dense rows of four in-neighbours per vertex (the first
+    // ones, or - head_ranked - the ones of largest out-degree) and the
+    // in-degrees; null: read from the pages
+    const uint32_t *head;
+    const uint32_t *indeg;
+    uint32_t head_ranked;
 };
 
 
@@ -441,15 +447,24 @@ __device__ __forceinline__ void ms_pull_body(const GraphDev &g, const MsDev &s, 
                 const Mask<NW> sn = ld_seen<NW>(s.sa, u);
 #pragma unroll
                 for (int i = 0; i < NW; i++) miss.w[i] = all.w[i] & ~sn.w[i];
-                const int p = lut.of(u);
-                const PageDev pd = lut.pages[p];
-                const uint32_t *node = g.pool + pd.base + 3ull * (u - pd.left);
-                len = node[2];
-                st = pd.base + 3ull * pd.nodenum + node[1];
-                // first four in-edges: independent loads, act probes, masks
+                // four in-edges: independent loads, act probes, masks
                 uint32_t v[4];
+                if (s.head) {
+                    len = __ldg(&s.indeg[u]);
+                    const uint4 h = ld_nc_v4(s.head + 4ull * u);
+                    v[0] = h.x;
+                    v[1] = h.y;
+                    v[2] = h.z;
+                    v[3] = h.w;
+                } else {
+                    const int p = lut.of(u);
+                    const PageDev pd = lut.pages[p];
+                    const uint32_t *node = g.pool + pd.base + 3ull * (u - pd.left);
+                    len = node[2];
+                    st = pd.base + 3ull * pd.nodenum + node[1];
 #pragma unroll
-                for (int j = 0; j < 4; j++) v[j] = (uint32_t)j < len ? __ldg(&g.pool[st + j]) : 0xFFFFFFFFu;
+                    for (int j = 0; j < 4; j++) v[j] = (uint32_t)j < len ? __ldg(&g.pool[st + j]) : 0xFFFFFFFFu;
+                }
                 bool on[4];
 #pragma unroll
                 for (int j = 0; j < 4; j++) on[j] = v[j] < s.V && test_bit(s.act_cur, v[j]);
@@ -466,6 +481,13 @@ __device__ __forceinline__ void ms_pull_body(const GraphDev &g, const MsDev &s, 
 #pragma unroll
                 for (int i = 0; i < NW; i++) full &= (acc.w[i] & miss.w[i]) == miss.w[i];
                 need = (!full && len > 4) ? 1u : 0u;
+                if (need && s.head) {
+                    // phase B needs where the list lives
+                    const int p = lut.of(u);
+                    const PageDev pd = lut.pages[p];
+                    const uint32_t *node = g.pool + pd.base + 3ull * (u - pd.left);
+                    st = pd.base + 3ull * pd.nodenum + node[1];
+                }
             }
             uint32_t nb;
             const uint32_t bo = kc::block_exclusive_scan<B>(need, wsum, nb);
@@ -482,7 +504,8 @@ __device__ __forceinline__ void ms_pull_body(const GraphDev &g, const MsDev &s, 
             // accumulator (an OR-semiring SpMV over those rows)
             uint32_t nq = 0;
             if (threadIdx.x < nb) {
-                const unsigned long long a0 = bq_st[threadIdx.x] + 4, b0 = bq_st[threadIdx.x] + bq_len[threadIdx.x];
+                const unsigned long long a0 = bq_st[threadIdx.x] + (s.head_ranked ? 0u : 4u),
+                                         b0 = bq_st[threadIdx.x] + bq_len[threadIdx.x];
                 nq = (uint32_t)(((b0 + 3) >> 2) - (a0 >> 2));
             }
             uint32_t tq;
@@ -495,7 +518,7 @@ __device__ __forceinline__ void ms_pull_body(const GraphDev &g, const MsDev &s, 
                     const int mid = (lo + hi + 1) >> 1;
                     if (bq_qoff[mid] <= i) lo = mid; else hi = mid - 1;
                 }
-                const unsigned long long aa = bq_st[lo] + 4, bb = bq_st[lo] + bq_len[lo];
+                const unsigned long long aa = bq_st[lo] + (s.head_ranked ? 0u : 4u), bb = bq_st[lo] + bq_len[lo];
                 const unsigned long long quad = (aa >> 2) + (i - bq_qoff[lo]);
                 const uint4 val = ld_nc_v4(g.pool + quad * 4);
                 const uint32_t vals[4] = {val.x, val.y, val.z, val.w};

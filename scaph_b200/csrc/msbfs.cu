@@ -176,6 +176,9 @@ static int ms_run(scaph_engine *e, const uint32_t *srcs, int nsrc, uint32_t *out
     s.nwords = e->nwords;
     s.all[0] = nsrc >= 64 ? ~0ull : ((1ull << nsrc) - 1);
     s.all[1] = nsrc > 64 ? (nsrc >= 128 ? ~0ull : ((1ull << (nsrc - 64)) - 1)) : 0ull;
+    s.head = e->d_head;
+    s.indeg = e->d_indeg;
+    s.head_ranked = e->head_ranked ? 1u : 0u;
     for (int k = 0; k < kMsPlanes; k++) s.planes[k] = m->planes[k];
 
     uint32_t *d_src = m->d_src;
