@@ -264,6 +264,7 @@ void scaph_engine::destroy()
     for (auto &ev : ev_dual)
         if (ev) cudaEventDestroy(ev);
     for (auto &e : ev_level) if (e) cudaEventDestroy(e);
+    cudaFreeHost(h_fstage);
     if (own_stream && st) cudaStreamDestroy(st);
 }
 
@@ -278,25 +279,32 @@ int scaph_engine::features(int level, uint32_t src, uint64_t nf, uint64_t mf, ui
     const int npi = (int)gi.npages;
     // frontier histogram over out-pages, counts then active words (level 0:
     // the source alone)
+    // both read-backs land in pinned staging and wait on one synchronisation
+    if (!h_fstage) SCAPH_CUDA(cudaMallocHost(&h_fstage, sizeof(uint32_t) * 2 * (np + (size_t)npi)));
+    uint32_t *hh = h_fstage, *hp = h_fstage + 2 * np;
+    const bool hist_dev = level > 0 && level - 1 < kHistLevels;
+    if (hist_dev)
+        SCAPH_CUDA(cudaMemcpyAsync(hh, d_hist + (size_t)(level - 1) * 2 * np, 2 * np * 4, cudaMemcpyDeviceToHost, st));
+    // unvisited vertices per in-edge page (only needed out of core, for the
+    // residency features, and for training traces)
+    const bool pull_dev = pager || cfg.record_features;
+    if (pull_dev) {
+        SCAPH_CUDA(page_unvisited(gi, d_visited, d_indeg, d_pcnt, d_pdatas, num_sms * 8, st));
+        SCAPH_CUDA(cudaMemcpyAsync(hp, d_pcnt, npi * 4, cudaMemcpyDeviceToHost, st));
+        SCAPH_CUDA(cudaMemcpyAsync(hp + npi, d_pdatas, npi * 4, cudaMemcpyDeviceToHost, st));
+    }
+    if (hist_dev || pull_dev) SCAPH_CUDA(cudaStreamSynchronize(st));
     hist.assign(2 * np, 0);
     if (level == 0) {
         size_t p = 0;
         while (p + 1 < np && g->pages[p + 1].left <= src) p++;
         hist[p] = 1;
         hist[np + p] = g->degree[src] + 3;
-    } else if (level - 1 < kHistLevels) {
-        SCAPH_CUDA(cudaMemcpyAsync(hist.data(), d_hist + (size_t)(level - 1) * 2 * np, 2 * np * 4,
-                                   cudaMemcpyDeviceToHost, st));
+    } else if (hist_dev) {
+        hist.assign(hh, hh + 2 * np);
     }
-    // unvisited vertices per in-edge page (only needed out of core, for the
-    // residency features, and for training traces)
     pull_cnt.assign(2 * (size_t)npi, 0);  // counts, then active words
-    if (pager || cfg.record_features) {
-        SCAPH_CUDA(page_unvisited(gi, d_visited, d_indeg, d_pcnt, d_pdatas, num_sms * 4, st));
-        SCAPH_CUDA(cudaMemcpyAsync(pull_cnt.data(), d_pcnt, npi * 4, cudaMemcpyDeviceToHost, st));
-        SCAPH_CUDA(cudaMemcpyAsync(pull_cnt.data() + npi, d_pdatas, npi * 4, cudaMemcpyDeviceToHost, st));
-    }
-    SCAPH_CUDA(cudaStreamSynchronize(st));
+    if (pull_dev) pull_cnt.assign(hp, hp + 2 * (size_t)npi);
     auto lg = [](double x, double d) { return (float)(std::log2(1.0 + x) / d); };
     f[0] = lg((double)nf, 32);
     f[1] = lg((double)mf, 40);
@@ -361,6 +369,12 @@ int scaph_engine::run_host_loop(uint32_t src, uint32_t *dd, uint32_t *dp)
     uint64_t vis_n = 1, vis_e = mf;
     int dir = 0, cur = 0, level = 0;
     std::vector<float> f(feat_dim), y;
+    if (learned) {
+        int rc = mlp_host_snapshot(sched, sched_host);
+        if (rc) return rc;
+    }
+    // page counts of the last feature pass, reused by the pager
+    std::vector<uint32_t> feat_pc, feat_hist;
     while (nf > 0 && level < kMaxLevels && (uint64_t)level + 1 < unreached) {
         const uint64_t used = vis_e + dead_edges;
         const uint64_t mu = E > used ? E - used : 0;
@@ -382,7 +396,7 @@ int scaph_engine::run_host_loop(uint32_t src, uint32_t *dd, uint32_t *dp)
                 int in = 0, out = 0;
                 mlp_dims(sched, &in, &out);
                 y.resize(out);
-                if ((rc = mlp_forward1(sched, f.data(), y.data(), st))) return rc;
+                mlp_forward_host(sched_host, f.data(), y.data());
                 if (level > 0) {
                     // the network models kernel time (trained resident);
                     // out of core the page traffic each direction would
@@ -404,6 +418,8 @@ int scaph_engine::run_host_loop(uint32_t src, uint32_t *dd, uint32_t *dp)
                 for (int p = 0; p + 1 < out && p < (int)np; p++)
                     if (y[1 + p] > 2.f) prefetch_pages.push_back(p);
             }
+            feat_pc = pc;
+            feat_hist = std::move(hist);
             pull_log.push_back(std::move(pc));
         }
         uint32_t *next = bm[cur ^ 1];
@@ -440,7 +456,20 @@ int scaph_engine::run_host_loop(uint32_t src, uint32_t *dd, uint32_t *dp)
         if (pager) {
             std::vector<int> needed;
             std::vector<uint32_t> datas;
-            int rc = pager_needs(this, pager, run_dir, level, src, needed, datas);
+            int rc = SCAPH_OK;
+            if (want_feat && (run_dir == 0 ? !feat_hist.empty() : !feat_pc.empty())) {
+                // the feature pass of this level already counted these pages
+                const std::vector<uint32_t> &c = run_dir == 0 ? feat_hist : feat_pc;
+                const size_t n = c.size() / 2;
+                datas.assign(n, 0);
+                for (size_t p = 0; p < n; p++)
+                    if (c[p]) {
+                        needed.push_back((int)p);
+                        datas[p] = c[n + p];
+                    }
+            } else {
+                rc = pager_needs(this, pager, run_dir, level, src, needed, datas);
+            }
             if (!rc) rc = pager_run_level(this, pager, run_dir, s, needed, datas);
             if (!rc && !prefetch_pages.empty() && run_dir == 0) rc = pager_prefetch(this, pager, 0, prefetch_pages);
             if (rc) return rc;

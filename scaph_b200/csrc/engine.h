@@ -7,6 +7,7 @@
 #include <vector>
 
 #include "common.h"
+#include "mlp_host.h"
 #include "device.cuh"
 #include "scaph/scaph.h"
 
@@ -84,6 +85,7 @@ int mlp_forward_device(scaph_mlp *m, const float *hX, int n, float *hY);
 int mlp_dims(const scaph_mlp *m, int *in, int *out);
 int mlp_device_view(const scaph_mlp *m, MlpDev *v);
 int mlp_forward1(scaph_mlp *m, const float *hX, float *hY, cudaStream_t st);
+int mlp_host_snapshot(const scaph_mlp *m, MlpHost &h);
 }  // namespace scaph
 
 // The engine behind the opaque C-ABI handle.
@@ -148,11 +150,13 @@ struct scaph_engine {
     scaph_bfs_stats pager_stats{};
     // learned scheduler / training traces
     scaph_mlp *sched = nullptr;
+    scaph::MlpHost sched_host;  // snapshot of sched taken at each host-loop run
     std::vector<float> feat_log;                    // levels x feat_dim
     int feat_dim = 0;
     std::vector<std::vector<uint32_t>> pull_log;    // unvisited per in-page, per level
     std::vector<std::pair<double, double>> dual_ms; // (push, pull) per level
     uint32_t *d_snap = nullptr, *d_pcnt = nullptr, *d_pdatas = nullptr;
+    uint32_t *h_fstage = nullptr;  // pinned: the feature pass's page counts
 
     static constexpr int kHistLevels = 256;
 

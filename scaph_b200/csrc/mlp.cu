@@ -313,6 +313,39 @@ int mlp_forward1(scaph_mlp *m, const float *hX, float *hY, cudaStream_t st)
     return SCAPH_OK;
 }
 
+// Round to the nearest bfloat16, ties to even (NaN stays NaN).
+static inline float bf16_round_host(float x)
+{
+    uint32_t u;
+    memcpy(&u, &x, 4);
+    if ((u & 0x7F800000u) == 0x7F800000u && (u & 0x007FFFFFu)) return x;
+    u = (u + 0x7FFFu + ((u >> 16) & 1u)) & 0xFFFF0000u;
+    float r;
+    memcpy(&r, &u, 4);
+    return r;
+}
+
+int mlp_host_snapshot(const scaph_mlp *m, MlpHost &h)
+{
+    h.in = m->in;
+    h.out = m->out;
+    h.w.resize(m->nparams);
+    SCAPH_CUDA(cudaMemcpy(h.w.data(), m->w, sizeof(float) * m->nparams, cudaMemcpyDeviceToHost));
+    // the device rounds every weight to bf16 where it reads it; biases stay
+    // in fp32
+    const size_t off[3] = {m->off_w1, m->off_w2, m->off_w3};
+    const size_t len[3] = {(size_t)m->in * kH, (size_t)kH * kH, (size_t)kH * m->out};
+    for (int l = 0; l < 3; l++)
+        for (size_t i = 0; i < len[l]; i++) h.w[off[l] + i] = bf16_round_host(h.w[off[l] + i]);
+    h.off_w1 = m->off_w1;
+    h.off_b1 = m->off_b1;
+    h.off_w2 = m->off_w2;
+    h.off_b2 = m->off_b2;
+    h.off_w3 = m->off_w3;
+    h.off_b3 = m->off_b3;
+    return SCAPH_OK;
+}
+
 int mlp_device_view(const scaph_mlp *m, MlpDev *v)
 {
     v->w = m->w;

@@ -55,11 +55,16 @@ __global__ void k_table_update(PageDev *tab, TableUpdate u)
 // words sum(deg*ew+3).  flip = 0: active vertices and their out-degrees, i.e.
 // get_page_info (src/gpu_engine.cuh:397-441, ew = 2 for weighted pages);
 // flip = ~0 over the visited bitmap: unvisited vertices (dead ones start
-// visited) with their in-degrees, the pull-side counterpart.  A warp
-// takes one visited word at a time (lane = vertex, coalesced in-degree
-// reads); a word spans at most two pages (pages hold >= 32 vertices or the
-// word is split lane by lane); per-CTA shared counters, one global atomic per
-// page per CTA.  cnt/datas must be zeroed by the caller.
+// visited) with their in-degrees, the pull-side counterpart.
+//
+// A warp takes a chunk of 32 bitmap words (1024 vertices): one coalesced
+// load gives every lane a word; the words are then walked eight at a time,
+// lane = vertex, with the eight degree loads issued together, and each lane
+// keeps its own count and sum for the chunk's first page.  A chunk rarely
+// crosses a page boundary; the vertices past it take the slow path (their
+// page looked up, one shared atomic each).  One shared atomic per page per
+// warp-chunk, one global atomic per page per CTA.  cnt/datas must be zeroed
+// by the caller.
 __global__ void k_page_counts(const uint32_t *bits, uint32_t flip, GraphDev g, const uint32_t *deg, uint32_t ew,
                               uint32_t *cnt, uint32_t *datas)
 {
@@ -68,47 +73,53 @@ __global__ void k_page_counts(const uint32_t *bits, uint32_t flip, GraphDev g, c
     if (local)
         for (uint32_t i = threadIdx.x; i < g.npages; i += blockDim.x) sc[i] = sd[i] = 0;
     __syncthreads();
+    uint32_t *const pc = local ? sc : cnt;
+    uint32_t *const pd = local ? sd : datas;
     const int lane = threadIdx.x & 31;
     const uint32_t nwords = (g.V + 31) / 32;
-    const uint32_t wstride = (gridDim.x * blockDim.x) >> 5;
-    for (uint32_t w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < nwords; w += wstride) {
-        const uint32_t m = (bits[w] ^ flip) & range_mask(w, 0, g.V);
-        if (!m) continue;
-        const uint32_t v = (w << 5) + lane;
-        const bool on = (m >> lane) & 1u;
-        const int p = on ? page_of(g, v) : -1;
-        const uint32_t d = on ? deg[v] * ew + 3 : 0;
-        const int p0 = __shfl_sync(0xFFFFFFFFu, p, __ffs(m) - 1);
-        const bool first = on && p == p0;
-        const uint32_t c0 = __popc(__ballot_sync(0xFFFFFFFFu, first));
-        uint32_t d0 = first ? d : 0, d1 = (on && !first) ? d : 0;
+    const uint32_t nchunks = (nwords + 31) / 32;
+    const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+    for (uint32_t ch = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; ch < nchunks; ch += nwarps) {
+        const uint32_t w = ch * 32 + lane;
+        const uint32_t mine = w < nwords ? (bits[w] ^ flip) & range_mask(w, 0, g.V) : 0u;
+        if (!__any_sync(0xFFFFFFFFu, mine != 0)) continue;
+        const uint32_t v0 = ch << 10;
+        const int p0 = page_of(g, v0);
+        const uint32_t lim = __ldg(&g.pages[p0 + 1].left);  // first vertex past page p0
+        uint32_t c = 0, dsum = 0;
+#pragma unroll 1
+        for (int j0 = 0; j0 < 32; j0 += 8) {
+            uint32_t m[8], d[8];
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-            d0 += __shfl_xor_sync(0xFFFFFFFFu, d0, o);
-            d1 += __shfl_xor_sync(0xFFFFFFFFu, d1, o);
-        }
-        const uint32_t rest = __ballot_sync(0xFFFFFFFFu, on && !first);
-        if (lane == 0) {
-            if (local) {
-                atomicAdd(&sc[p0], c0);
-                atomicAdd(&sd[p0], d0);
-            } else {
-                atomicAdd(&cnt[p0], c0);
-                atomicAdd(&datas[p0], d0);
+            for (int k = 0; k < 8; k++) m[k] = __shfl_sync(0xFFFFFFFFu, mine, j0 + k);
+#pragma unroll
+            for (int k = 0; k < 8; k++) {
+                const uint32_t v = v0 + ((uint32_t)(j0 + k) << 5) + lane;
+                d[k] = ((m[k] >> lane) & 1u) ? __ldg(&deg[v]) : 0u;
             }
-        }
-        if (rest) {
-            // the lanes past the page boundary: rare, one atomic per lane
-            if (on && !first) {
-                if (local) {
-                    atomicAdd(&sc[p], 1u);
-                    atomicAdd(&sd[p], d);
+#pragma unroll
+            for (int k = 0; k < 8; k++) {
+                if (!((m[k] >> lane) & 1u)) continue;
+                const uint32_t v = v0 + ((uint32_t)(j0 + k) << 5) + lane;
+                const uint32_t wd = d[k] * ew + 3;
+                if (v < lim) {
+                    c++;
+                    dsum += wd;
                 } else {
-                    atomicAdd(&cnt[p], 1u);
-                    atomicAdd(&datas[p], d);
+                    const int p = page_of(g, v);
+                    atomicAdd(&pc[p], 1u);
+                    atomicAdd(&pd[p], wd);
                 }
             }
-            (void)d1;
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            c += __shfl_xor_sync(0xFFFFFFFFu, c, o);
+            dsum += __shfl_xor_sync(0xFFFFFFFFu, dsum, o);
+        }
+        if (lane == 0 && c) {
+            atomicAdd(&pc[p0], c);
+            atomicAdd(&pd[p0], dsum);
         }
     }
     __syncthreads();
@@ -534,7 +545,7 @@ int pager_needs(scaph_engine *e, Pager *pg, int dir, int level, uint32_t src, st
         SCAPH_CUDA(cudaMemcpyAsync(G.h_cnt, h, np * 4, cudaMemcpyDeviceToHost, e->st));
         SCAPH_CUDA(cudaMemcpyAsync(G.h_datas, h + np, np * 4, cudaMemcpyDeviceToHost, e->st));
     } else {
-        SCAPH_CUDA(page_unvisited(G.view, e->d_visited, e->d_indeg, G.d_cnt, G.d_datas, e->num_sms * 4, e->st));
+        SCAPH_CUDA(page_unvisited(G.view, e->d_visited, e->d_indeg, G.d_cnt, G.d_datas, e->num_sms * 8, e->st));
         SCAPH_CUDA(cudaMemcpyAsync(G.h_cnt, G.d_cnt, np * 4, cudaMemcpyDeviceToHost, e->st));
         SCAPH_CUDA(cudaMemcpyAsync(G.h_datas, G.d_datas, np * 4, cudaMemcpyDeviceToHost, e->st));
     }
