@@ -121,6 +121,7 @@ __device__ __forceinline__ void flush_acc(CtaAcc *acc, ThreadAcc t, LevelCounter
 // Shared-memory working set common to the level kernels.
 struct LevelSmem {
     uint32_t hn[kHistCap], hd[kHistCap];
+    uint32_t hni[kHistCap], hdi[kHistCap];  // in-page histogram (page_nodes_in)
     PageDev lut_pages[kLutPages];
     uint32_t lut_coarse[kLutCoarse];
     CtaAcc acc;
@@ -150,6 +151,13 @@ __device__ __forceinline__ void level_prologue(LevelSmem &sm, const BfsDev &s)
             sm.hd[i] = 0;
         }
     }
+    if (s.page_nodes_in) {
+        const int n = s.hgi.npages < (uint32_t)kHistCap ? (int)s.hgi.npages : kHistCap;
+        for (int i = threadIdx.x; i < n; i += BLOCK) {
+            sm.hni[i] = 0;
+            sm.hdi[i] = 0;
+        }
+    }
 }
 
 template <int BLOCK>
@@ -166,6 +174,15 @@ __device__ __forceinline__ void level_epilogue(LevelSmem &sm, const BfsDev &s, c
             }
         }
     }
+    if (s.page_nodes_in) {
+        const int n = s.hgi.npages < (uint32_t)kHistCap ? (int)s.hgi.npages : kHistCap;
+        for (int i = threadIdx.x; i < n; i += BLOCK) {
+            if (sm.hni[i]) {
+                atomicAdd(&s.page_nodes_in[i], sm.hni[i]);
+                atomicAdd(&s.page_datas_in[i], sm.hdi[i]);
+            }
+        }
+    }
 }
 
 // Adds a discovered vertex (page p of the histogram graph; out-degree + 3
@@ -178,6 +195,21 @@ __device__ __forceinline__ void hist_add(LevelSmem &sm, const BfsDev &s, int p, 
     } else {
         atomicAdd(&s.page_nodes[p], 1u);
         atomicAdd(&s.page_datas[p], datas);
+    }
+}
+
+// Adds discovered vertex v to the in-page histogram (in-degree + 3 words).
+__device__ __forceinline__ void hist_in_add(LevelSmem &sm, const BfsDev &s, uint32_t v)
+{
+    if (!s.page_nodes_in) return;
+    const int p = page_of(s.hgi, v);
+    const uint32_t d = __ldg(&s.indeg[v]) + 3;
+    if (p < kHistCap) {
+        atomicAdd(&sm.hni[p], 1u);
+        atomicAdd(&sm.hdi[p], d);
+    } else {
+        atomicAdd(&s.page_nodes_in[p], 1u);
+        atomicAdd(&s.page_datas_in[p], d);
     }
 }
 
@@ -218,6 +250,7 @@ __device__ __forceinline__ void visit4(LevelSmem &sm, const BfsDev &s, ThreadAcc
         const uint32_t du = __ldg(&s.degree[u[j]]);
         t.next_edges += du;
         if (s.page_nodes) hist_add(sm, s, hist_same ? lut.of(u[j]) : page_of(s.hg, u[j]), du + 3);
+        hist_in_add(sm, s, u[j]);
     }
 }
 
@@ -484,6 +517,7 @@ __device__ __forceinline__ void pull_body(const GraphDev &g, const BfsDev &s, ui
                             if (s.head && hist_same) p = lut.of(v);
                             hist_add(sm, s, hist_same ? p : page_of(s.hg, v), dv + 3);
                         }
+                        hist_in_add(sm, s, v);
                     } else {
                         t.inspected += min(len, kPullSerial);
                         need = len > kPullSerial;
@@ -570,6 +604,7 @@ __device__ __forceinline__ void pull_body(const GraphDev &g, const BfsDev &s, ui
                         t.next++;
                         t.next_edges += dv;
                         if (s.page_nodes) hist_add(sm, s, hist_same ? bq_p[e] : page_of(s.hg, vv), dv + 3);
+                        hist_in_add(sm, s, vv);
                     }
                 }
             }
@@ -772,7 +807,7 @@ __global__ void __launch_bounds__(64) k_decide_learned(BfsGraphArgs a, DecideArg
     constexpr int kG = 16;
     __shared__ float f[kG + kHistCap];
     __shared__ float h1[64], h2[64];
-    __shared__ int s_stop, s_ab;
+    __shared__ int s_stop, s_ab, s_guard;
     BfsCtl *c = a.ctl;
     const uint32_t L = c->level;
     const int t = threadIdx.x;
@@ -793,6 +828,7 @@ __global__ void __launch_bounds__(64) k_decide_learned(BfsGraphArgs a, DecideArg
         const unsigned long long src_dead = (d.dead_bm[src >> 5] >> (src & 31)) & 1u;
         const unsigned long long unv = (unsigned long long)d.V - d.dead - c->vis_n + src_dead;
         s_ab = alpha_beta_next(c->dir, c->nf, c->prev_nf, c->mf, mu, d.V, d.alpha, d.beta);
+        s_guard = alpha_beta_confident(c->dir, c->nf, c->mf, mu, d.V, d.alpha, d.beta);
         f[0] = log2f(1.f + (float)c->nf) / 32.f;
         f[1] = log2f(1.f + (float)c->mf) / 40.f;
         f[2] = log2f(1.f + (float)unv) / 32.f;
@@ -839,7 +875,7 @@ __global__ void __launch_bounds__(64) k_decide_learned(BfsGraphArgs a, DecideArg
     if (t == 0) {
         float y = net.w[net.off_b3];
         for (int j = 0; j < 64; j++) y += bf(h2[j]) * bf(W3[(size_t)j * net.out]);
-        const int nd = d.mode == 1 ? 0 : d.mode == 2 ? 1 : (y > 0.f ? 1 : 0);
+        const int nd = d.mode == 1 ? 0 : d.mode == 2 ? 1 : s_guard >= 0 ? s_guard : (y > 0.f ? 1 : 0);
         c->dir = nd;
         c->level = L + 1;
         cudaGraphSetConditional(h_push, nd == 0 ? 1 : 0);

@@ -81,6 +81,12 @@ struct BfsDev {
     const uint32_t *indeg;
     uint32_t head_ranked;      // head rows are not the list's first edges:
                                // phase B scans the whole list
+    // histogram of the discovered vertices over the IN-edge graph's pages
+    // (count, sum(indeg+3)): keeps the pull-side page counts current without
+    // a pass over all vertices (directed graphs; null when not wanted)
+    uint32_t *page_nodes_in;
+    uint32_t *page_datas_in;
+    GraphDev hgi;
 };
 
 // Graph mode: state of one traversal kept on the device, so a whole BFS runs
@@ -136,6 +142,28 @@ __host__ __device__ inline int alpha_beta_next(int cur_dir, unsigned long long n
 {
     if (cur_dir == 0) return (double)mf > (double)mu / alpha ? 1 : 0;
     return ((double)nf < (double)V / beta && nf < prev_nf) ? 0 : 1;
+}
+
+// The learned direction is taken only near the alpha/beta switch point:
+// where the rule's own ratio is more than kLearnedBand times past (or short
+// of) its threshold, the rule decides.  From push (cur_dir 0) the ratio is
+// mf / (mu / alpha), from pull it is nf / (V / beta).  Returns the rule's
+// direction when it is that clear, -1 when the network decides.
+constexpr float kLearnedBand = 4.f;
+__host__ __device__ inline int alpha_beta_confident(int cur_dir, unsigned long long nf, unsigned long long mf,
+                                                    unsigned long long mu, unsigned long long V, float alpha,
+                                                    float beta)
+{
+    if (cur_dir == 0) {
+        const double r = (double)mf * alpha / (double)(mu ? mu : 1);
+        if (r > kLearnedBand) return 1;
+        if (r * kLearnedBand < 1.0) return 0;
+        return -1;
+    }
+    const double r = (double)nf * beta / (double)(V ? V : 1);
+    if (r > kLearnedBand) return 1;
+    if (r * kLearnedBand < 1.0) return 0;
+    return -1;
 }
 
 // Page lookup (page table + coarse index), in global or shared memory.

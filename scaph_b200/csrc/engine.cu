@@ -265,11 +265,16 @@ void scaph_engine::destroy()
         if (ev) cudaEventDestroy(ev);
     for (auto &e : ev_level) if (e) cudaEventDestroy(e);
     cudaFreeHost(h_fstage);
+    cudaFreeHost(h_inc);
+    cudaFree(d_hist_in);
     if (own_stream && st) cudaStreamDestroy(st);
 }
 
-// Scheduler features of the coming level (layout in scaph.h /
-// DESIGN.md): 16 globals, then the frontier's share of every out-edge page.
+// Scheduler features of the coming level (layout in scaph.h): 16 globals,
+// then the frontier's share of every out-edge page.  The frontier histogram
+// and the pull-side page counts come from the incremental copies the host
+// loop keeps (inc_hist / inc_pull) when they are current, else from the
+// device.
 int scaph_engine::features(int level, uint32_t src, uint64_t nf, uint64_t mf, uint64_t unvis, uint64_t mu,
                            int prev_dir, int ab_dir, float *f, std::vector<uint32_t> &pull_cnt,
                            std::vector<uint32_t> &hist)
@@ -282,12 +287,14 @@ int scaph_engine::features(int level, uint32_t src, uint64_t nf, uint64_t mf, ui
     // both read-backs land in pinned staging and wait on one synchronisation
     if (!h_fstage) SCAPH_CUDA(cudaMallocHost(&h_fstage, sizeof(uint32_t) * 2 * (np + (size_t)npi)));
     uint32_t *hh = h_fstage, *hp = h_fstage + 2 * np;
-    const bool hist_dev = level > 0 && level - 1 < kHistLevels;
+    const bool hist_inc = level > 0 && inc_hist_level == level;
+    const bool hist_dev = level > 0 && level - 1 < kHistLevels && !hist_inc;
     if (hist_dev)
         SCAPH_CUDA(cudaMemcpyAsync(hh, d_hist + (size_t)(level - 1) * 2 * np, 2 * np * 4, cudaMemcpyDeviceToHost, st));
     // unvisited vertices per in-edge page (only needed out of core, for the
     // residency features, and for training traces)
-    const bool pull_dev = pager || cfg.record_features;
+    const bool pull_inc = inc_pull_valid;
+    const bool pull_dev = (pager || cfg.record_features) && !pull_inc;
     if (pull_dev) {
         SCAPH_CUDA(page_unvisited(gi, d_visited, d_indeg, d_pcnt, d_pdatas, num_sms * 8, st));
         SCAPH_CUDA(cudaMemcpyAsync(hp, d_pcnt, npi * 4, cudaMemcpyDeviceToHost, st));
@@ -300,11 +307,14 @@ int scaph_engine::features(int level, uint32_t src, uint64_t nf, uint64_t mf, ui
         while (p + 1 < np && g->pages[p + 1].left <= src) p++;
         hist[p] = 1;
         hist[np + p] = g->degree[src] + 3;
+    } else if (hist_inc) {
+        hist.assign(inc_hist.begin(), inc_hist.end());
     } else if (hist_dev) {
         hist.assign(hh, hh + 2 * np);
     }
     pull_cnt.assign(2 * (size_t)npi, 0);  // counts, then active words
-    if (pull_dev) pull_cnt.assign(hp, hp + 2 * (size_t)npi);
+    if (pull_inc) pull_cnt.assign(inc_pull.begin(), inc_pull.end());
+    else if (pull_dev) pull_cnt.assign(hp, hp + 2 * (size_t)npi);
     auto lg = [](double x, double d) { return (float)(std::log2(1.0 + x) / d); };
     f[0] = lg((double)nf, 32);
     f[1] = lg((double)mf, 40);
@@ -373,6 +383,27 @@ int scaph_engine::run_host_loop(uint32_t src, uint32_t *dd, uint32_t *dp)
         int rc = mlp_host_snapshot(sched, sched_host);
         if (rc) return rc;
     }
+    // out of core, the learned scheduler's per-level page counts are kept
+    // incrementally: the pull side starts from one pass over the vertices
+    // and loses each level's discoveries (the in-page histogram the level
+    // kernels record), the push side is the level's out-page histogram; both
+    // arrive with the level's counters, so a level needs no extra pass
+    const bool incr = pager && learned && !dual;
+    const GraphDev &gview_in = gin();
+    const size_t npi = gview_in.npages;
+    inc_pull_valid = false;
+    inc_hist_level = -1;
+    if (incr) {
+        if (!h_inc) SCAPH_CUDA(cudaMallocHost(&h_inc, sizeof(uint32_t) * 2 * (np + npi)));
+        if (!symmetric && !d_hist_in) SCAPH_CUDA(cudaMalloc(&d_hist_in, sizeof(uint32_t) * 2 * npi * kHistLevels));
+        if (d_hist_in) SCAPH_CUDA(cudaMemsetAsync(d_hist_in, 0, sizeof(uint32_t) * 2 * npi * kHistLevels, st));
+        SCAPH_CUDA(page_unvisited(gview_in, d_visited, d_indeg, d_pcnt, d_pdatas, num_sms * 8, st));
+        SCAPH_CUDA(cudaMemcpyAsync(h_inc, d_pcnt, npi * 4, cudaMemcpyDeviceToHost, st));
+        SCAPH_CUDA(cudaMemcpyAsync(h_inc + npi, d_pdatas, npi * 4, cudaMemcpyDeviceToHost, st));
+        SCAPH_CUDA(cudaStreamSynchronize(st));
+        inc_pull.assign(h_inc, h_inc + 2 * npi);
+        inc_pull_valid = true;
+    }
     // page counts of the last feature pass, reused by the pager
     std::vector<uint32_t> feat_pc, feat_hist;
     while (nf > 0 && level < kMaxLevels && (uint64_t)level + 1 < unreached) {
@@ -403,6 +434,9 @@ int scaph_engine::run_host_loop(uint32_t src, uint32_t *dd, uint32_t *dp)
                     // cause is known exactly and overrides it when it
                     // clearly dominates
                     dir = y[0] > 0.f ? 1 : 0;
+                    // far from the alpha/beta threshold the rule decides
+                    const int sure = alpha_beta_confident(prev_dir, nf, mf, mu, V, cfg.alpha, cfg.beta);
+                    if (sure >= 0) dir = sure;
                     if (pager) {
                         const int npi = (int)pc.size() / 2;
                         const double t_push = pager_transfer_ms(pager, 0, hist.data(), hist.data() + np, (int)np,
@@ -432,6 +466,12 @@ int scaph_engine::run_host_loop(uint32_t src, uint32_t *dd, uint32_t *dp)
             s.page_datas = s.page_nodes + np;
         } else {
             s.page_nodes = s.page_datas = nullptr;
+        }
+        s.page_nodes_in = s.page_datas_in = nullptr;
+        if (incr && d_hist_in && level < kHistLevels) {
+            s.page_nodes_in = d_hist_in + (size_t)level * 2 * npi;
+            s.page_datas_in = s.page_nodes_in + npi;
+            s.hgi = gview_in;
         }
         double dual_push = 0, dual_pull = 0;
         if (dual && level > 0) {
@@ -482,7 +522,23 @@ int scaph_engine::run_host_loop(uint32_t src, uint32_t *dd, uint32_t *dp)
         }
         SCAPH_CUDA(cudaEventRecord(ev_level[2 * level + 1], st));
         SCAPH_CUDA(cudaMemcpyAsync(h_ctr + level, d_ctr + level, sizeof(LevelCounters), cudaMemcpyDeviceToHost, st));
+        const bool inc_now = incr && level < kHistLevels;
+        if (inc_now) {
+            SCAPH_CUDA(cudaMemcpyAsync(h_inc, d_hist + (size_t)level * 2 * np, 2 * np * 4, cudaMemcpyDeviceToHost, st));
+            if (d_hist_in)
+                SCAPH_CUDA(cudaMemcpyAsync(h_inc + 2 * np, d_hist_in + (size_t)level * 2 * npi, 2 * npi * 4,
+                                           cudaMemcpyDeviceToHost, st));
+        }
         SCAPH_CUDA(cudaStreamSynchronize(st));
+        if (inc_now) {
+            inc_hist.assign(h_inc, h_inc + 2 * np);
+            inc_hist_level = level + 1;
+            const uint32_t *hin = d_hist_in ? h_inc + 2 * np : h_inc;  // symmetric: in-pages are the out-pages
+            for (size_t p = 0; p < 2 * npi; p++) inc_pull[p] -= hin[p];
+        } else if (incr) {
+            inc_pull_valid = false;
+            inc_hist_level = -1;
+        }
         if (dual) {
             float ms = 0;
             cudaEventElapsedTime(&ms, ev_level[2 * level], ev_level[2 * level + 1]);

@@ -157,6 +157,12 @@ struct scaph_engine {
     std::vector<std::pair<double, double>> dual_ms; // (push, pull) per level
     uint32_t *d_snap = nullptr, *d_pcnt = nullptr, *d_pdatas = nullptr;
     uint32_t *h_fstage = nullptr;  // pinned: the feature pass's page counts
+    // incremental page counts of the learned host loop (out of core)
+    uint32_t *d_hist_in = nullptr;  // [kHistLevels][2][in-pages]: discoveries by in-page
+    uint32_t *h_inc = nullptr;      // pinned read-back of a level's histograms
+    std::vector<uint32_t> inc_hist, inc_pull;
+    int inc_hist_level = -1;        // level whose frontier histogram inc_hist holds
+    bool inc_pull_valid = false;
 
     static constexpr int kHistLevels = 256;
 

@@ -64,3 +64,38 @@ def test_ooc_matches_in_hbm_trace():
         assert [(t["direction"], t["next"]) for t in ta] == [(t["direction"], t["next"]) for t in tb]
     a.close()
     b.close()
+
+
+@pytest.mark.parametrize("directed", [False, True])
+def test_learned_ooc_incremental_page_counts(directed):
+    """Out of core the learned loop keeps the pull-side page counts
+    incrementally (in-page histograms of each level's discoveries); at every
+    level they must equal a recount over the vertices: unvisited vertices per
+    in-page and their sum(indeg+3)."""
+    if directed:
+        csr = S.Csr.powerlaw(30000, 300000, 1.9, 3000, seed=G.SEED + 33)
+        gt_csr = csr.transpose()
+    else:
+        csr = S.Csr.rmat(14, 16, seed=G.SEED + 34)
+        gt_csr = csr
+    g = S.PagedGraph.from_csr(csr, pagesize_words=1 << 12)
+    gt = S.PagedGraph.from_csr(gt_csr, pagesize_words=1 << 12) if directed else None
+    gin = gt or g
+    net = S.Mlp(16 + g.npages, 1 + g.npages, seed=3)
+    total = g.npages + (gt.npages if gt else 0)
+    eng = S.Engine(g, gt, pool_bytes=(total // 2) * g.pagesize * 4, direction=S.DIR_LEARNED, record_features=1)
+    eng.set_scheduler(net)
+    indeg = gt_csr.degree()
+    pl = gin.page_list()
+    for src in G.sources(csr, 2, 35):
+        depth = run_check(csr, eng, src)
+        depth, _, st = eng.bfs(src)
+        for lvl in range(st.levels):
+            cnt, datas = eng.pull_pages(lvl, gin.npages)
+            unv = (depth > lvl) & (indeg > 0)  # visited before level `lvl` runs: depth <= lvl, or no in-edge
+            for p in range(gin.npages):
+                lo, hi = int(pl[p, 0]), int(pl[p, 1]) + 1
+                m = unv[lo:hi]
+                assert cnt[p] == m.sum(), (lvl, p)
+                assert datas[p] == (indeg[lo:hi][m].astype(np.int64) + 3).sum(), (lvl, p)
+    eng.close()
