@@ -39,7 +39,7 @@ FALLBACK_HBM_GBS = 6650.0
 
 # Measured DRAM bytes (read + write) per k_pull launch on RMAT-24, mean over 200 launches;
 # see profiles/k_pull_rmat24_traffic.md for the ncu command.
-K_PULL_TRAFFIC_BYTES = 349_962_373
+K_PULL_TRAFFIC_BYTES = 295_719_334
 
 
 def parse_args():
