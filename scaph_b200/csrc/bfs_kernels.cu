@@ -686,9 +686,13 @@ __global__ void __launch_bounds__(BLOCK, kPullMinThreads / BLOCK) k_pull(GraphDe
 // ---------------------------------------------------------------------------
 // kernels: graph mode
 // ---------------------------------------------------------------------------
+// The three level kernels of a graph-mode level run back to back; the one
+// the level's direction (decided on the device) does not select leaves at
+// once, which costs less than a conditional node per direction.
 template <int BLOCK>
 __global__ void __launch_bounds__(BLOCK) k_push_g(GraphDev g, BfsGraphArgs a)
 {
+    if (a.ctl->dir != 0) return;
     const BfsDev s = level_state(a);
     clear_third(a, s.level);
     push_body<BLOCK>(g, s, 0, s.V, RangeList{nullptr, nullptr, nullptr, 0});
@@ -697,12 +701,14 @@ __global__ void __launch_bounds__(BLOCK) k_push_g(GraphDev g, BfsGraphArgs a)
 template <int BLOCK>
 __global__ void __launch_bounds__(BLOCK) k_push_giant_g(GraphDev g, BfsGraphArgs a)
 {
+    if (a.ctl->dir != 0) return;
     giant_body<BLOCK>(g, level_state(a));
 }
 
 template <int BLOCK>
 __global__ void __launch_bounds__(BLOCK, kPullMinThreads / BLOCK) k_pull_g(GraphDev g, BfsGraphArgs a)
 {
+    if (a.ctl->dir != 1) return;
     const BfsDev s = level_state(a);
     clear_third(a, s.level);
     pull_body<BLOCK>(g, s, 0, s.V, RangeList{nullptr, nullptr, nullptr, 0});
@@ -760,8 +766,7 @@ __global__ void k_graph_start(BfsGraphArgs a)
 
 // Last node of each level: counters -> next direction (Beamer alpha/beta, or
 // the forced direction) and the conditionals of the next iteration.
-__global__ void k_decide(BfsGraphArgs a, DecideArgs d, cudaGraphConditionalHandle h_loop,
-                         cudaGraphConditionalHandle h_push, cudaGraphConditionalHandle h_pull)
+__global__ void k_decide(BfsGraphArgs a, DecideArgs d, cudaGraphConditionalHandle h_loop)
 {
     BfsCtl *c = a.ctl;
     const uint32_t L = c->level;
@@ -778,8 +783,6 @@ __global__ void k_decide(BfsGraphArgs a, DecideArgs d, cudaGraphConditionalHandl
     if (stop) {
         c->done = 1;
         cudaGraphSetConditional(h_loop, 0);
-        cudaGraphSetConditional(h_push, 0);
-        cudaGraphSetConditional(h_pull, 0);
         return;
     }
     const unsigned long long used = c->vis_e + d.dead_edges;
@@ -790,8 +793,6 @@ __global__ void k_decide(BfsGraphArgs a, DecideArgs d, cudaGraphConditionalHandl
     else nd = alpha_beta_next(c->dir, c->nf, c->prev_nf, c->mf, mu, d.V, d.alpha, d.beta);
     c->dir = nd;
     c->level = L + 1;
-    cudaGraphSetConditional(h_push, nd == 0 ? 1 : 0);
-    cudaGraphSetConditional(h_pull, nd == 1 ? 1 : 0);
     cudaGraphSetConditional(h_loop, 1);
 }
 
@@ -800,9 +801,7 @@ __global__ void k_decide(BfsGraphArgs a, DecideArgs d, cudaGraphConditionalHandl
 // page residency 1 (graph resident), then the new frontier's share of every
 // out-page - through the network's three layers; output 0 > 0 means pull.
 __global__ void __launch_bounds__(64) k_decide_learned(BfsGraphArgs a, DecideArgs d, MlpDev net,
-                                                       cudaGraphConditionalHandle h_loop,
-                                                       cudaGraphConditionalHandle h_push,
-                                                       cudaGraphConditionalHandle h_pull)
+                                                       cudaGraphConditionalHandle h_loop)
 {
     constexpr int kG = 16;
     __shared__ float f[kG + kHistCap];
@@ -855,8 +854,6 @@ __global__ void __launch_bounds__(64) k_decide_learned(BfsGraphArgs a, DecideArg
         if (t == 0) {
             c->done = 1;
             cudaGraphSetConditional(h_loop, 0);
-            cudaGraphSetConditional(h_push, 0);
-            cudaGraphSetConditional(h_pull, 0);
         }
         return;
     }
@@ -878,8 +875,6 @@ __global__ void __launch_bounds__(64) k_decide_learned(BfsGraphArgs a, DecideArg
         const int nd = d.mode == 1 ? 0 : d.mode == 2 ? 1 : s_guard >= 0 ? s_guard : (y > 0.f ? 1 : 0);
         c->dir = nd;
         c->level = L + 1;
-        cudaGraphSetConditional(h_push, nd == 0 ? 1 : 0);
-        cudaGraphSetConditional(h_pull, nd == 1 ? 1 : 0);
         cudaGraphSetConditional(h_loop, 1);
     }
 }
@@ -988,6 +983,27 @@ cudaError_t run_level_graph(int dir, int block, int grid, const GraphDev &g, con
     case 128: return launch_level_g<128>(dir, grid, g, a, st);
     case 512: return launch_level_g<512>(dir, grid, g, a, st);
     default: return launch_level_g<256>(dir, grid, g, a, st);
+    }
+}
+
+void level_graph_kernels(int block, const void **push, const void **giant, const void **pull)
+{
+    switch (block) {
+    case 128:
+        *push = (const void *)k_push_g<128>;
+        *giant = (const void *)k_push_giant_g<128>;
+        *pull = (const void *)k_pull_g<128>;
+        break;
+    case 512:
+        *push = (const void *)k_push_g<512>;
+        *giant = (const void *)k_push_giant_g<512>;
+        *pull = (const void *)k_pull_g<512>;
+        break;
+    default:
+        *push = (const void *)k_push_g<256>;
+        *giant = (const void *)k_push_giant_g<256>;
+        *pull = (const void *)k_pull_g<256>;
+        break;
     }
 }
 

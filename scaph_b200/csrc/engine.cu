@@ -565,12 +565,9 @@ int scaph_engine::run_host_loop(uint32_t src, uint32_t *dd, uint32_t *dp)
 
 int scaph_engine::build_graph()
 {
-    SCAPH_CUDA(cudaStreamCreateWithFlags(&cap_st, cudaStreamNonBlocking));
     SCAPH_CUDA(cudaGraphCreate(&graph, 0));
-    cudaGraphConditionalHandle h_loop, h_push, h_pull;
+    cudaGraphConditionalHandle h_loop;
     SCAPH_CUDA(cudaGraphConditionalHandleCreate(&h_loop, graph, 1, cudaGraphCondAssignDefault));
-    SCAPH_CUDA(cudaGraphConditionalHandleCreate(&h_push, graph, 1, cudaGraphCondAssignDefault));
-    SCAPH_CUDA(cudaGraphConditionalHandleCreate(&h_pull, graph, 0, cudaGraphCondAssignDefault));
 
     const size_t np = g->pages.size();
     gargs.base = base_state(d_depth, nullptr);
@@ -610,7 +607,8 @@ int scaph_engine::build_graph()
     cudaGraphNode_t n_start;
     SCAPH_CUDA(cudaGraphAddKernelNode(&n_start, graph, &n_init, 1, &sp));
 
-    // WHILE(loop) { IF(push){push, giant}; IF(pull){pull}; decide }
+    // WHILE(loop) { push; giant; pull; decide }: the level kernel the level's
+    // direction does not select leaves at once (cheaper than IF nodes)
     cudaGraphNodeParams wp{};
     wp.type = cudaGraphNodeTypeConditional;
     wp.conditional.handle = h_loop;
@@ -620,45 +618,37 @@ int scaph_engine::build_graph()
     SCAPH_CUDA(cudaGraphAddNode(&n_while, graph, &n_start, 1, &wp));
     cudaGraph_t body = wp.conditional.phGraph_out[0];
 
-    cudaGraphNodeParams ip{};
-    ip.type = cudaGraphNodeTypeConditional;
-    ip.conditional.handle = h_push;
-    ip.conditional.type = cudaGraphCondTypeIf;
-    ip.conditional.size = 1;
-    cudaGraphNode_t n_ifpush;
-    SCAPH_CUDA(cudaGraphAddNode(&n_ifpush, body, nullptr, 0, &ip));
-    cudaGraph_t bpush = ip.conditional.phGraph_out[0];
-
-    cudaGraphNodeParams iq{};
-    iq.type = cudaGraphNodeTypeConditional;
-    iq.conditional.handle = h_pull;
-    iq.conditional.type = cudaGraphCondTypeIf;
-    iq.conditional.size = 1;
-    cudaGraphNode_t n_ifpull;
-    SCAPH_CUDA(cudaGraphAddNode(&n_ifpull, body, &n_ifpush, 1, &iq));
-    cudaGraph_t bpull = iq.conditional.phGraph_out[0];
+    const void *f_push, *f_giant, *f_pull;
+    level_graph_kernels(block, &f_push, &f_giant, &f_pull);
+    GraphDev gout = dout.view, gpull = gin();
+    void *push_args[] = {&gout, &gargs};
+    void *pull_args[] = {&gpull, &gargs};
+    cudaGraphNode_t n_push, n_giant, n_pull;
+    cudaKernelNodeParams lp{};
+    lp.func = const_cast<void *>(f_push);
+    lp.gridDim = dim3(grid_push);
+    lp.blockDim = dim3(block);
+    lp.kernelParams = push_args;
+    SCAPH_CUDA(cudaGraphAddKernelNode(&n_push, body, nullptr, 0, &lp));
+    lp.func = const_cast<void *>(f_giant);
+    SCAPH_CUDA(cudaGraphAddKernelNode(&n_giant, body, &n_push, 1, &lp));
+    lp.func = const_cast<void *>(f_pull);
+    lp.gridDim = dim3(grid_pull);
+    lp.kernelParams = pull_args;
+    SCAPH_CUDA(cudaGraphAddKernelNode(&n_pull, body, &n_giant, 1, &lp));
 
     const bool learned = cfg.direction == SCAPH_DIR_LEARNED && sched;
     MlpDev net{};
     if (learned) mlp_device_view(sched, &net);
-    void *dec_args[] = {&gargs, &dargs, &h_loop, &h_push, &h_pull};
-    void *dec_learned_args[] = {&gargs, &dargs, &net, &h_loop, &h_push, &h_pull};
+    void *dec_args[] = {&gargs, &dargs, &h_loop};
+    void *dec_learned_args[] = {&gargs, &dargs, &net, &h_loop};
     cudaKernelNodeParams dp{};
     dp.func = const_cast<void *>(learned ? decide_learned_kernel() : decide_kernel());
     dp.gridDim = dim3(1);
     dp.blockDim = dim3(learned ? 64 : 1);
     dp.kernelParams = learned ? dec_learned_args : dec_args;
     cudaGraphNode_t n_decide;
-    SCAPH_CUDA(cudaGraphAddKernelNode(&n_decide, body, &n_ifpull, 1, &dp));
-
-    SCAPH_CUDA(cudaStreamBeginCaptureToGraph(cap_st, bpush, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
-    cudaError_t e1 = run_level_graph(0, block, grid_push, dout.view, gargs, cap_st);
-    SCAPH_CUDA(cudaStreamEndCapture(cap_st, &bpush));
-    SCAPH_CUDA(e1);
-    SCAPH_CUDA(cudaStreamBeginCaptureToGraph(cap_st, bpull, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
-    cudaError_t e2 = run_level_graph(1, block, grid_pull, gin(), gargs, cap_st);
-    SCAPH_CUDA(cudaStreamEndCapture(cap_st, &bpull));
-    SCAPH_CUDA(e2);
+    SCAPH_CUDA(cudaGraphAddKernelNode(&n_decide, body, &n_pull, 1, &dp));
     SCAPH_CUDA(cudaGraphInstantiate(&gexec, graph, 0));
     return SCAPH_OK;
 }

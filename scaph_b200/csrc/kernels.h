@@ -18,6 +18,9 @@ cudaError_t run_giant(int block, int grid, const GraphDev &g, const BfsDev &s, c
 // Graph mode: the same level kernels reading the level from a BfsCtl.
 cudaError_t run_level_graph(int dir, int block, int grid, const GraphDev &g, const BfsGraphArgs &a, cudaStream_t st);
 // k_graph_init(BfsGraphArgs, u32* depth, u32* parent, u32 src, u32 unreached, const u32* dead, u32 nlevels_clear)
+// Graph mode: the push, giant-chunk and pull kernels of a level (each leaves
+// at once unless the level's direction selects it).
+void level_graph_kernels(int block, const void **push, const void **giant, const void **pull);
 const void *graph_init_kernel();
 // k_graph_start(BfsGraphArgs)
 const void *graph_start_kernel();
