@@ -11,12 +11,15 @@
 //   exact.  Adjacency longer than kGiantEdges is cut into chunks that a
 //   second kernel spreads over the whole GPU.
 // pull (bottom-up): has no reference counterpart (gpu_pull_iteration is a
-//   stub, src/app.cuh:365-369).  A warp owns one word (32 vertices) of the
-//   visited bitmap, so visited/next words are written without atomics.  Each
-//   unvisited vertex issues its first four in-edge loads and frontier probes
-//   at once; longer lists are then scanned by the whole warp, 128 edges per
-//   step with 128-bit loads, stopping at the first frontier hit.  Warps take
-//   words from a per-CTA shared counter, so heavy words do not stall a CTA.
+//   stub, src/app.cuh:365-369).  A CTA takes a tile of visited-bitmap words
+//   and compacts the tile's unvisited vertices into a shared queue.  Phase A:
+//   each thread takes two of them at a time, reads their in-degrees and
+//   dense head rows (in-neighbours ranked by out-degree) with all loads
+//   issued before any frontier probe, and probes the top-ranked neighbour
+//   first.  Vertices still unresolved are scanned by groups of eight lanes,
+//   32 in-edges per step with 128-bit loads, up to the first frontier hit
+//   (phase B).  Found vertices are collected in a shared bitmap and written
+//   back once per tile word.
 // Both stage the page table and coarse index in shared memory, and fold the
 // per-page frontier statistics of get_page_info (src/gpu_engine.cuh:397-441)
 // into their epilogue: a shared-memory histogram of the next frontier by
@@ -43,9 +46,13 @@ constexpr int kPushTileWords = 128;                  // frontier-bitmap words pe
 #ifndef SCAPH_PULL_FIRST_PROBE
 #define SCAPH_PULL_FIRST_PROBE 1
 #endif
-#ifndef SCAPH_PULL_MINB
-#define SCAPH_PULL_MINB 1280
+#ifndef SCAPH_PULL_PER_THREAD
+#define SCAPH_PULL_PER_THREAD 2
 #endif
+#ifndef SCAPH_PULL_MINB
+#define SCAPH_PULL_MINB 1024
+#endif
+constexpr int kPullPerThread = SCAPH_PULL_PER_THREAD;  // unvisited vertices each thread takes per pull round
 constexpr int kPullTileWords = 128;                  // visited-bitmap words per pull tile (the range-list tile)
 constexpr int kPullMinThreads = SCAPH_PULL_MINB;     // resident threads per SM the pull kernel is compiled for
 constexpr uint32_t kPullSerial = SCAPH_PULL_SERIAL;  // in-edges each lane probes before the warp helps
@@ -119,9 +126,11 @@ __device__ __forceinline__ void flush_acc(CtaAcc *acc, ThreadAcc t, LevelCounter
 }
 
 // Shared-memory working set common to the level kernels.
+constexpr int kHistInCap = 256;  // in-pages counted in shared memory (the rest: global atomics)
+
 struct LevelSmem {
     uint32_t hn[kHistCap], hd[kHistCap];
-    uint32_t hni[kHistCap], hdi[kHistCap];  // in-page histogram (page_nodes_in)
+    uint32_t hni[kHistInCap], hdi[kHistInCap];  // in-page histogram (page_nodes_in)
     PageDev lut_pages[kLutPages];
     uint32_t lut_coarse[kLutCoarse];
     CtaAcc acc;
@@ -152,7 +161,7 @@ __device__ __forceinline__ void level_prologue(LevelSmem &sm, const BfsDev &s)
         }
     }
     if (s.page_nodes_in) {
-        const int n = s.hgi.npages < (uint32_t)kHistCap ? (int)s.hgi.npages : kHistCap;
+        const int n = s.hgi.npages < (uint32_t)kHistInCap ? (int)s.hgi.npages : kHistInCap;
         for (int i = threadIdx.x; i < n; i += BLOCK) {
             sm.hni[i] = 0;
             sm.hdi[i] = 0;
@@ -175,7 +184,7 @@ __device__ __forceinline__ void level_epilogue(LevelSmem &sm, const BfsDev &s, c
         }
     }
     if (s.page_nodes_in) {
-        const int n = s.hgi.npages < (uint32_t)kHistCap ? (int)s.hgi.npages : kHistCap;
+        const int n = s.hgi.npages < (uint32_t)kHistInCap ? (int)s.hgi.npages : kHistInCap;
         for (int i = threadIdx.x; i < n; i += BLOCK) {
             if (sm.hni[i]) {
                 atomicAdd(&s.page_nodes_in[i], sm.hni[i]);
@@ -204,7 +213,7 @@ __device__ __forceinline__ void hist_in_add(LevelSmem &sm, const BfsDev &s, uint
     if (!s.page_nodes_in) return;
     const int p = page_of(s.hgi, v);
     const uint32_t d = __ldg(&s.indeg[v]) + 3;
-    if (p < kHistCap) {
+    if (p < kHistInCap) {
         atomicAdd(&sm.hni[p], 1u);
         atomicAdd(&sm.hdi[p], d);
     } else {
@@ -407,9 +416,9 @@ __device__ __forceinline__ void pull_body(const GraphDev &g, const BfsDev &s, ui
     __shared__ LevelSmem sm;
     __shared__ uint32_t q[kPullTileWords * 32];
     __shared__ uint32_t fnd[kPullTileWords];
-    __shared__ uint32_t bq_v[BLOCK], bq_len[BLOCK];
-    __shared__ unsigned long long bq_st[BLOCK];
-    __shared__ int bq_p[BLOCK];
+    constexpr int kPPT = BLOCK >= 512 ? 1 : kPullPerThread;  // shared memory bounds the 512-thread CTA
+    __shared__ uint32_t bq_v[kPPT * BLOCK], bq_len[kPPT * BLOCK];
+    __shared__ unsigned long long bq_st[kPPT * BLOCK];
     __shared__ uint32_t wsum[BLOCK / 32];
 
     level_prologue<BLOCK>(sm, s);
@@ -448,102 +457,123 @@ __device__ __forceinline__ void pull_body(const GraphDev &g, const BfsDev &s, ui
             }
         }
         __syncthreads();
-        for (uint32_t c0 = 0; c0 < total; c0 += BLOCK) {
-            // ---- phase A: one unvisited vertex per thread
-            const uint32_t k = c0 + threadIdx.x;
-            uint32_t v = 0, len = 0, need = 0;
-            unsigned long long st = 0;
-            int p = 0;
-            if (k < total) {
-                v = q[k];
-                uint32_t u[kPullSerial];
-                bool ok = true;
+        for (uint32_t c0 = 0; c0 < total; c0 += kPPT * BLOCK) {
+            // ---- phase A: kPPT unvisited vertices per thread, all
+            // their row (or header and first in-edge) loads issued before
+            // any of their frontier probes
+            uint32_t vv[kPPT], len[kPPT], need[kPPT];
+            unsigned long long st[kPPT];
+            int p[kPPT];
+            uint32_t u[kPPT][kPullSerial];
+            bool ok[kPPT];
+#pragma unroll
+            for (int i = 0; i < kPPT; i++) {
+                const uint32_t k = c0 + i * BLOCK + threadIdx.x;
+                vv[i] = 0;
+                len[i] = 0;
+                need[i] = 0;
+                st[i] = 0;
+                p[i] = 0;
+                ok[i] = k < total;
+#pragma unroll
+                for (uint32_t j = 0; j < kPullSerial; j++) u[i][j] = 0xFFFFFFFFu;
+                if (!ok[i]) continue;
+                const uint32_t v = q[k];
+                vv[i] = v;
                 if (s.head) {
                     // dense rows: the in-degree and the first in-edges of
-                    // consecutive vertices, two independent coalesced loads;
-                    // the page is read only if these do not decide
-                    len = __ldg(&s.indeg[v]);
+                    // consecutive vertices, independent coalesced loads; the
+                    // page is read only if these do not decide
+                    len[i] = __ldg(&s.indeg[v]);
                     const uint4 h = ld_nc_v4(s.head + (size_t)kPullHead * v);
-                    u[0] = h.x;
-                    u[1] = h.y;
-                    u[2] = h.z;
-                    u[3] = h.w;
+                    u[i][0] = h.x;
+                    u[i][1] = h.y;
+                    u[i][2] = h.z;
+                    u[i][3] = h.w;
                 } else {
-                    p = lut.of(v);
-                    const PageDev pd = lut.pages[p];
+                    p[i] = lut.of(v);
+                    const PageDev pd = lut.pages[p[i]];
                     if (pd.base != kNotResident) {
                         const uint32_t *node = g.pool + pd.base + 3ull * (v - pd.left);
-                        len = node[2];
-                        st = pd.base + 3ull * pd.nodenum + node[1];
+                        len[i] = node[2];
+                        st[i] = pd.base + 3ull * pd.nodenum + node[1];
                         t.headers++;
 #pragma unroll
                         for (uint32_t j = 0; j < kPullSerial; j++)
-                            u[j] = j < len ? __ldg(&g.pool[st + j]) : 0xFFFFFFFFu;
+                            u[i][j] = j < len[i] ? __ldg(&g.pool[st[i] + j]) : 0xFFFFFFFFu;
                     } else {
                         atomicOr(&s.ctr->error, 4u);
-                        ok = false;
+                        ok[i] = false;
                     }
                 }
-                if (ok) {
-                    uint32_t hit = 0;
+            }
+#pragma unroll
+            for (int i = 0; i < kPPT; i++) {
+                if (!ok[i]) continue;
+                const uint32_t v = vv[i];
+                uint32_t hit = 0;
 #if SCAPH_PULL_FIRST_PROBE
-                    // ranked rows: the top in-neighbour alone first (it
-                    // settles most vertices), the other three only on a miss
-                    if (s.head_ranked) {
-                        if (u[0] < s.V && test_bit(s.front, u[0])) hit = 1u;
-                        else {
+                // ranked rows: the top in-neighbour alone first (it settles
+                // most vertices), the other three only on a miss
+                if (s.head_ranked) {
+                    if (u[i][0] < s.V && test_bit(s.front, u[i][0])) hit = 1u;
+                    else {
 #pragma unroll
-                            for (uint32_t j = 1; j < kPullSerial; j++)
-                                if (u[j] < s.V && test_bit(s.front, u[j])) hit |= 1u << j;
-                        }
-                    } else
-#endif
-                    {
-#pragma unroll
-                        for (uint32_t j = 0; j < kPullSerial; j++)
-                            if (u[j] < s.V && test_bit(s.front, u[j])) hit |= 1u << j;
+                        for (uint32_t j = 1; j < kPullSerial; j++)
+                            if (u[i][j] < s.V && test_bit(s.front, u[i][j])) hit |= 1u << j;
                     }
-                    if (hit) {
-                        const uint32_t j = __ffs(hit) - 1;
-                        t.inspected += j + 1;
-                        const uint32_t par = u[j];
-                        s.depth[v] = s.level + 1;
-                        if (s.parent) s.parent[v] = par;
-                        atomicOr(&fnd[(v >> 5) - tbase], 1u << (v & 31));
-                        const uint32_t dv = __ldg(&s.degree[v]);
-                        t.next++;
-                        t.next_edges += dv;
-                        if (s.page_nodes) {
-                            if (s.head && hist_same) p = lut.of(v);
-                            hist_add(sm, s, hist_same ? p : page_of(s.hg, v), dv + 3);
-                        }
-                        hist_in_add(sm, s, v);
-                    } else {
-                        t.inspected += min(len, kPullSerial);
-                        need = len > kPullSerial;
-                        if (need && s.head) {
-                            // phase B needs where the list lives
-                            p = lut.of(v);
-                            const PageDev pd = lut.pages[p];
-                            if (pd.base != kNotResident) {
-                                const uint32_t *node = g.pool + pd.base + 3ull * (v - pd.left);
-                                st = pd.base + 3ull * pd.nodenum + node[1];
-                                t.headers++;
-                            } else {
-                                atomicOr(&s.ctr->error, 4u);
-                                need = 0;
-                            }
+                } else
+#endif
+                {
+#pragma unroll
+                    for (uint32_t j = 0; j < kPullSerial; j++)
+                        if (u[i][j] < s.V && test_bit(s.front, u[i][j])) hit |= 1u << j;
+                }
+                if (hit) {
+                    const uint32_t j = __ffs(hit) - 1;
+                    t.inspected += j + 1;
+                    const uint32_t par = u[i][j];
+                    s.depth[v] = s.level + 1;
+                    if (s.parent) s.parent[v] = par;
+                    atomicOr(&fnd[(v >> 5) - tbase], 1u << (v & 31));
+                    const uint32_t dv = __ldg(&s.degree[v]);
+                    t.next++;
+                    t.next_edges += dv;
+                    if (s.page_nodes) {
+                        if (s.head && hist_same) p[i] = lut.of(v);
+                        hist_add(sm, s, hist_same ? p[i] : page_of(s.hg, v), dv + 3);
+                    }
+                    hist_in_add(sm, s, v);
+                } else {
+                    t.inspected += min(len[i], kPullSerial);
+                    need[i] = len[i] > kPullSerial;
+                    if (need[i] && s.head) {
+                        // phase B needs where the list lives
+                        p[i] = lut.of(v);
+                        const PageDev pd = lut.pages[p[i]];
+                        if (pd.base != kNotResident) {
+                            const uint32_t *node = g.pool + pd.base + 3ull * (v - pd.left);
+                            st[i] = pd.base + 3ull * pd.nodenum + node[1];
+                            t.headers++;
+                        } else {
+                            atomicOr(&s.ctr->error, 4u);
+                            need[i] = 0;
                         }
                     }
                 }
             }
+            uint32_t nneed = 0;
+#pragma unroll
+            for (int i = 0; i < kPPT; i++) nneed += need[i];
             uint32_t nb;
-            const uint32_t bo = block_exclusive_scan<BLOCK>(need, wsum, nb);
-            if (need) {
-                bq_v[bo] = v;
-                bq_st[bo] = st;
-                bq_len[bo] = len;
-                bq_p[bo] = p;
+            uint32_t bo = block_exclusive_scan<BLOCK>(nneed, wsum, nb);
+#pragma unroll
+            for (int i = 0; i < kPPT; i++) {
+                if (!need[i]) continue;
+                bq_v[bo] = vv[i];
+                bq_st[bo] = st[i];
+                bq_len[bo] = len[i];
+                bo++;
             }
             __syncthreads();
             // ---- phase B: groups of kGroup lanes, one vertex per group
@@ -603,7 +633,7 @@ __device__ __forceinline__ void pull_body(const GraphDev &g, const BfsDev &s, ui
                         const uint32_t dv = __ldg(&s.degree[vv]);
                         t.next++;
                         t.next_edges += dv;
-                        if (s.page_nodes) hist_add(sm, s, hist_same ? bq_p[e] : page_of(s.hg, vv), dv + 3);
+                        if (s.page_nodes) hist_add(sm, s, hist_same ? lut.of(vv) : page_of(s.hg, vv), dv + 3);
                         hist_in_add(sm, s, vv);
                     }
                 }
