@@ -49,6 +49,9 @@ constexpr int kPushTileWords = 128;                  // frontier-bitmap words pe
 #ifndef SCAPH_PULL_PER_THREAD
 #define SCAPH_PULL_PER_THREAD 2
 #endif
+#ifndef SCAPH_PULL_GROUP
+#define SCAPH_PULL_GROUP 8  // lanes per unresolved vertex in pull phase B
+#endif
 #ifndef SCAPH_PULL_MINB
 #define SCAPH_PULL_MINB 1024
 #endif
@@ -411,7 +414,7 @@ __device__ __forceinline__ void pull_body(const GraphDev &g, const BfsDev &s, ui
     // 128-bit loads, up to the first frontier hit (phase B).  Found vertices
     // are collected in a shared bitmap and the tile's visited/next words are
     // then written once, without global atomics.
-    constexpr int kGroup = 8;
+    constexpr int kGroup = SCAPH_PULL_GROUP;
     constexpr int kGroups = BLOCK / kGroup;
     __shared__ LevelSmem sm;
     __shared__ uint32_t q[kPullTileWords * 32];
