@@ -437,29 +437,19 @@ __device__ __forceinline__ void pull_body(const GraphDev &g, const BfsDev &s, ui
                                  : (((uint32_t)(((unsigned long long)vhi + 31) >> 5)) - (vlo >> 5) + kPullTileWords - 1) /
                                        kPullTileWords;
 
-    for (uint32_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-        uint32_t rlo = vlo, rhi = vhi, local;
-        range_of_tile(rl, tile, rlo, rhi, local);
-        const uint32_t rwhi = (uint32_t)(((unsigned long long)rhi + 31) >> 5);
-        const uint32_t tbase = (rlo >> 5) + local * kPullTileWords;  // first word of the tile
-        const uint32_t w = tbase + threadIdx.x;
-        uint32_t unv = 0;
-        if (threadIdx.x < kPullTileWords) {
-            fnd[threadIdx.x] = 0;
-            if (w < rwhi) unv = ~s.visited[w] & range_mask(w, rlo, rhi);
-        }
-        if (!__syncthreads_or(unv != 0)) continue;
-        uint32_t total;
-        uint32_t off = block_exclusive_scan<BLOCK>(__popc(unv), wsum, total);
-        if (total == 0) continue;
-        {
-            uint32_t m = unv;
-            while (m) {
-                q[off++] = (w << 5) + (__ffs(m) - 1);
-                m &= m - 1;
+    // Runs phases A and B over q[0, total): found vertices go to the tile's
+    // shared bitmap fnd (tbase = the tile's first word), or, gathering
+    // several sparse tiles, straight to the visited / next words.
+    auto run_queue = [&](uint32_t total, uint32_t tbase, bool gathered) {
+        auto mark_found = [&](uint32_t v) {
+            const uint32_t bit = 1u << (v & 31);
+            if (gathered) {
+                atomicOr(&s.visited[v >> 5], bit);
+                atomicOr(&s.next[v >> 5], bit);
+            } else {
+                atomicOr(&fnd[(v >> 5) - tbase], bit);
             }
-        }
-        __syncthreads();
+        };
         for (uint32_t c0 = 0; c0 < total; c0 += kPPT * BLOCK) {
             // ---- phase A: kPPT unvisited vertices per thread, all
             // their row (or header and first in-edge) loads issued before
@@ -538,7 +528,7 @@ __device__ __forceinline__ void pull_body(const GraphDev &g, const BfsDev &s, ui
                     const uint32_t par = u[i][j];
                     s.depth[v] = s.level + 1;
                     if (s.parent) s.parent[v] = par;
-                    atomicOr(&fnd[(v >> 5) - tbase], 1u << (v & 31));
+                    mark_found(v);
                     const uint32_t dv = __ldg(&s.degree[v]);
                     t.next++;
                     t.next_edges += dv;
@@ -632,7 +622,7 @@ __device__ __forceinline__ void pull_body(const GraphDev &g, const BfsDev &s, ui
                         const uint32_t vv = bq_v[e];
                         s.depth[vv] = s.level + 1;
                         if (s.parent) s.parent[vv] = hit_par;
-                        atomicOr(&fnd[(vv >> 5) - tbase], 1u << (vv & 31));
+                        mark_found(vv);
                         const uint32_t dv = __ldg(&s.degree[vv]);
                         t.next++;
                         t.next_edges += dv;
@@ -643,6 +633,55 @@ __device__ __forceinline__ void pull_body(const GraphDev &g, const BfsDev &s, ui
             }
             __syncthreads();
         }
+    };
+
+    // Sparse levels (few unvisited vertices, a handful per tile): the
+    // vertices of several tiles are gathered into one queue before phases A
+    // and B run, so that every thread has a vertex in each round.
+    const bool gather = s.pull_gather != 0;
+    uint32_t qn = 0;  // gathered vertices (uniform across the CTA)
+    for (uint32_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        uint32_t rlo = vlo, rhi = vhi, local;
+        range_of_tile(rl, tile, rlo, rhi, local);
+        const uint32_t rwhi = (uint32_t)(((unsigned long long)rhi + 31) >> 5);
+        const uint32_t tbase = (rlo >> 5) + local * kPullTileWords;  // first word of the tile
+        const uint32_t w = tbase + threadIdx.x;
+        uint32_t unv = 0;
+        if (threadIdx.x < kPullTileWords) {
+            if (!gather) fnd[threadIdx.x] = 0;
+            if (w < rwhi) unv = ~s.visited[w] & range_mask(w, rlo, rhi);
+        }
+        if (!__syncthreads_or(unv != 0)) continue;
+        uint32_t total;
+        uint32_t off = block_exclusive_scan<BLOCK>(__popc(unv), wsum, total);
+        if (total == 0) continue;
+        if (gather) {
+            if (qn + total > (uint32_t)kPullTileWords * 32) {
+                run_queue(qn, 0, true);
+                qn = 0;
+            }
+            uint32_t m = unv, at = qn + off;
+            while (m) {
+                q[at++] = (w << 5) + (__ffs(m) - 1);
+                m &= m - 1;
+            }
+            qn += total;
+            __syncthreads();
+            if (qn >= (uint32_t)kPPT * BLOCK) {
+                run_queue(qn, 0, true);
+                qn = 0;
+            }
+            continue;
+        }
+        {
+            uint32_t m = unv;
+            while (m) {
+                q[off++] = (w << 5) + (__ffs(m) - 1);
+                m &= m - 1;
+            }
+        }
+        __syncthreads();
+        run_queue(total, tbase, false);
         // ---- the tile's visited / next words, written once (atomically:
         // a word at a range boundary may belong to two tiles)
         if (threadIdx.x < kPullTileWords && w < rwhi) {
@@ -654,6 +693,7 @@ __device__ __forceinline__ void pull_body(const GraphDev &g, const BfsDev &s, ui
         }
         __syncthreads();
     }
+    if (gather && qn) run_queue(qn, 0, true);
     level_epilogue<BLOCK>(sm, s, t);
 }
 
@@ -669,6 +709,7 @@ __device__ __forceinline__ BfsDev level_state(const BfsGraphArgs &a)
     s.front = a.bm3 + (size_t)(L % 3) * s.nwords;
     s.next = a.bm3 + (size_t)((L + 1) % 3) * s.nwords;
     s.ctr = a.ctr0 + L;
+    s.pull_gather = c->pull_gather;
     if (a.hist0 && L < a.hist_levels) {
         s.page_nodes = a.hist0 + (size_t)L * 2 * a.npages_h;
         s.page_datas = s.page_nodes + a.npages_h;
@@ -761,6 +802,7 @@ __global__ void k_graph_init(BfsGraphArgs a, uint32_t *depth, uint32_t *parent, 
         c->level = 0;
         c->dir = 0;
         c->done = 0;
+        c->pull_gather = 0;
         c->t_start = globaltimer();
     }
     const size_t stride = (size_t)gridDim.x * blockDim.x;
@@ -825,6 +867,12 @@ __global__ void k_decide(BfsGraphArgs a, DecideArgs d, cudaGraphConditionalHandl
     else if (d.mode == 2) nd = 1;
     else nd = alpha_beta_next(c->dir, c->nf, c->prev_nf, c->mf, mu, d.V, d.alpha, d.beta);
     c->dir = nd;
+    {
+        const uint32_t src = c->src;
+        const unsigned long long src_dead = (d.dead_bm[src >> 5] >> (src & 31)) & 1u;
+        const unsigned long long unv = (unsigned long long)d.V - d.dead - c->vis_n + src_dead;
+        c->pull_gather = unv * kPullGatherRatio < d.V ? 1u : 0u;
+    }
     c->level = L + 1;
     cudaGraphSetConditional(h_loop, 1);
 }
@@ -840,6 +888,7 @@ __global__ void __launch_bounds__(64) k_decide_learned(BfsGraphArgs a, DecideArg
     __shared__ float f[kG + kHistCap];
     __shared__ float h1[64], h2[64];
     __shared__ int s_stop, s_ab, s_guard;
+    __shared__ unsigned long long s_unv;
     BfsCtl *c = a.ctl;
     const uint32_t L = c->level;
     const int t = threadIdx.x;
@@ -859,6 +908,7 @@ __global__ void __launch_bounds__(64) k_decide_learned(BfsGraphArgs a, DecideArg
         const uint32_t src = c->src;
         const unsigned long long src_dead = (d.dead_bm[src >> 5] >> (src & 31)) & 1u;
         const unsigned long long unv = (unsigned long long)d.V - d.dead - c->vis_n + src_dead;
+        s_unv = unv;
         s_ab = alpha_beta_next(c->dir, c->nf, c->prev_nf, c->mf, mu, d.V, d.alpha, d.beta);
         s_guard = alpha_beta_confident(c->dir, c->nf, c->mf, mu, d.V, d.alpha, d.beta);
         f[0] = log2f(1.f + (float)c->nf) / 32.f;
@@ -907,6 +957,7 @@ __global__ void __launch_bounds__(64) k_decide_learned(BfsGraphArgs a, DecideArg
         for (int j = 0; j < 64; j++) y += bf(h2[j]) * bf(W3[(size_t)j * net.out]);
         const int nd = d.mode == 1 ? 0 : d.mode == 2 ? 1 : s_guard >= 0 ? s_guard : (y > 0.f ? 1 : 0);
         c->dir = nd;
+        c->pull_gather = s_unv * kPullGatherRatio < d.V ? 1u : 0u;
         c->level = L + 1;
         cudaGraphSetConditional(h_loop, 1);
     }

@@ -87,7 +87,12 @@ struct BfsDev {
     uint32_t *page_nodes_in;
     uint32_t *page_datas_in;
     GraphDev hgi;
+    uint32_t pull_gather;      // sparse pull level: gather several tiles per queue
 };
+
+// A pull level gathers the vertices of several tiles into one queue when the
+// unvisited vertices are this sparse (fewer than one per kPullGatherRatio).
+constexpr unsigned long long kPullGatherRatio = 64;
 
 // Graph mode: state of one traversal kept on the device, so a whole BFS runs
 // as one CUDA-graph launch with the level loop in a conditional WHILE node.
@@ -98,6 +103,8 @@ struct BfsCtl {
     uint32_t level;            // level being run
     int32_t dir;               // 0 push, 1 pull
     int32_t done;
+    uint32_t pull_gather;      // the level is a sparse pull (BfsDev::pull_gather)
+    uint32_t _pad;
     unsigned long long nf, prev_nf, mf, vis_n, vis_e;
     unsigned long long t_start;
 };

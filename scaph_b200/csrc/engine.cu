@@ -467,6 +467,10 @@ int scaph_engine::run_host_loop(uint32_t src, uint32_t *dd, uint32_t *dp)
         } else {
             s.page_nodes = s.page_datas = nullptr;
         }
+        {
+            const uint64_t unv_now = (uint64_t)V - n_dead - vis_n + (src_dead ? 1 : 0);
+            s.pull_gather = unv_now * kPullGatherRatio < V ? 1u : 0u;
+        }
         s.page_nodes_in = s.page_datas_in = nullptr;
         if (incr && d_hist_in && level < kHistLevels) {
             s.page_nodes_in = d_hist_in + (size_t)level * 2 * npi;
