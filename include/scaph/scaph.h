@@ -228,6 +228,16 @@ int scaph_engine_evict_all(scaph_engine *e);
  * traversal on the engine's stream and returns; scaph_engine_sync waits,
  * and scaph_bfs_trace / scaph_bfs_page_hist wait for the last run. */
 int scaph_engine_sync(scaph_engine *e);
+/* Pipelined traversals with host output, for serving many sources: enqueues
+ * the traversal of `src` and the copy of its depths into `host_depths`
+ * (V words; page-locked memory from scaph_host_alloc for the copy to run
+ * asynchronously) and returns.  The copy of one run overlaps the next run's
+ * traversal (two device buffers, a copy stream); the caller keeps each host
+ * buffer untouched until scaph_engine_sync returns.  Resident graphs in graph
+ * mode only (SCAPH_EUNSUPPORTED otherwise).  Same depths as scaph_bfs
+ * (App::run, src/app.cuh:220-265, with the copy-back of check(),
+ * src/app.cuh:262-264). */
+int scaph_bfs_enqueue(scaph_engine *e, uint32_t src, uint32_t *host_depths);
 
 /* Per-level trace of the last scaph_bfs (direction, frontier, edges, time,
  * per-page histogram).  Writes up to `cap` records, returns the count. */

@@ -112,6 +112,7 @@ def lib() -> C.CDLL:
         "scaph_bfs": ([vp, u32, vp, vp, i32, P(_Stats)], i32),
         "scaph_bfs_trace": ([vp, P(_Trace), i32], i32),
         "scaph_engine_sync": ([vp], i32),
+        "scaph_bfs_enqueue": ([vp, u32, vp], i32),
         "scaph_engine_evict_all": ([vp], i32),
         "scaph_mlp_create": ([i32, i32, u64, i32, P(vp)], i32),
         "scaph_mlp_destroy": ([vp], None),
@@ -161,6 +162,30 @@ def _ptr(a: np.ndarray | None) -> C.c_void_p | None:
 
 def device_count() -> int:
     return lib().scaph_device_count()
+
+
+class PinnedArray:
+    """Page-locked host array (scaph_host_alloc) viewed as numpy; the target
+    of asynchronous device->host copies (Engine.bfs_enqueue)."""
+
+    def __init__(self, n: int, dtype=np.uint32):
+        dt = np.dtype(dtype)
+        self._p = lib().scaph_host_alloc(max(1, n) * dt.itemsize)
+        if not self._p:
+            raise ScaphError(ENOMEM, f"scaph_host_alloc({n * dt.itemsize}) failed")
+        self.array = np.ctypeslib.as_array((C.c_uint8 * (max(1, n) * dt.itemsize)).from_address(self._p)).view(dt)[:n]
+
+    def close(self) -> None:
+        if self._p:
+            self.array = None
+            lib().scaph_host_free(self._p)
+            self._p = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 # ---------------------------------------------------------------------------
@@ -438,6 +463,14 @@ class Engine:
         _check(lib().scaph_bfs(self._h, src, C.c_void_p(depth_ptr), C.c_void_p(parent_ptr) if parent_ptr else None,
                                1, C.byref(st)))
         return _stats(st)
+
+    def bfs_enqueue(self, src: int, host_depth: np.ndarray) -> None:
+        """Pipelined traversal with host output (scaph_bfs_enqueue): returns
+        at once; host_depth (uint32[V], page-locked for overlap) is filled by
+        the time sync() returns."""
+        if host_depth.dtype != np.uint32 or host_depth.size < self.V or not host_depth.flags.c_contiguous:
+            raise ScaphError(EINVAL, "host_depth must be a contiguous uint32 array of V entries")
+        _check(lib().scaph_bfs_enqueue(self._h, src, _ptr(host_depth)))
 
     def bfs_async(self, src: int, depth_ptr: int, parent_ptr: int | None = None) -> None:
         """Enqueues one BFS writing into device buffers; returns at once."""

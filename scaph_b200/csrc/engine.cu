@@ -233,6 +233,18 @@ int scaph_engine::create(const Graph *g_, const Graph *gt_, const scaph_config *
 void scaph_engine::destroy()
 {
     if (st) cudaStreamSynchronize(st);
+    if (copy_st) {
+        cudaStreamSynchronize(copy_st);
+        cudaStreamDestroy(copy_st);
+        copy_st = nullptr;
+    }
+    for (int i = 0; i < 2; i++) {
+        cudaFree(d_pipe[i]);
+        d_pipe[i] = nullptr;
+        if (ev_run[i]) cudaEventDestroy(ev_run[i]);
+        if (ev_copied[i]) cudaEventDestroy(ev_copied[i]);
+        ev_run[i] = ev_copied[i] = nullptr;
+    }
     ms_release(ms);
     ms = nullptr;
     pager_release(pager);
@@ -804,7 +816,47 @@ int scaph_engine::bfs(uint32_t src, uint32_t *depths, uint32_t *parents, int out
     return rc;
 }
 
+// Pipelined traversal into host memory: run i writes device buffer i % 2 on
+// the engine stream; its copy to the host runs on a second stream after the
+// run, so it overlaps run i+1; run i+2 reuses the buffer once that copy is
+// done.  Graph mode only (the traversal is one launch).
+int scaph_engine::enqueue(uint32_t src, uint32_t *host_depths)
+{
+    if (src >= V) return set_error(SCAPH_EINVAL, "source %u out of range (V=%u)", src, V);
+    if (!host_depths) return set_error(SCAPH_EINVAL, "null output");
+    if (!graph_mode()) return set_error(SCAPH_EUNSUPPORTED, "pipelined runs need graph mode (resident graph)");
+    SCAPH_CUDA(cudaSetDevice(device));
+    if (!copy_st) {
+        SCAPH_CUDA(cudaStreamCreateWithFlags(&copy_st, cudaStreamNonBlocking));
+        for (int i = 0; i < 2; i++) {
+            SCAPH_CUDA(cudaMalloc(&d_pipe[i], (size_t)V * 4));
+            SCAPH_CUDA(cudaEventCreateWithFlags(&ev_run[i], cudaEventDisableTiming));
+            SCAPH_CUDA(cudaEventCreateWithFlags(&ev_copied[i], cudaEventDisableTiming));
+        }
+    }
+    const int b = (int)(pipe_runs & 1);
+    SCAPH_CUDA(cudaStreamWaitEvent(st, ev_copied[b], 0));  // the buffer's previous copy is done
+    pending_src = src;
+    pending_parent = false;
+    int rc = launch_graph(src, d_pipe[b], nullptr);
+    if (rc) return rc;
+    pending = true;
+    SCAPH_CUDA(cudaEventRecord(ev_run[b], st));
+    SCAPH_CUDA(cudaStreamWaitEvent(copy_st, ev_run[b], 0));
+    SCAPH_CUDA(cudaMemcpyAsync(host_depths, d_pipe[b], (size_t)V * 4, cudaMemcpyDeviceToHost, copy_st));
+    SCAPH_CUDA(cudaEventRecord(ev_copied[b], copy_st));
+    pipe_runs++;
+    return SCAPH_OK;
+}
+
 extern "C" {
+
+int scaph_bfs_enqueue(scaph_engine *e, uint32_t src, uint32_t *host_depths)
+{
+    clear_error();
+    if (!e) return set_error(SCAPH_EINVAL, "null engine");
+    return e->enqueue(src, host_depths);
+}
 
 int scaph_engine_create(const scaph_graph *g, const scaph_graph *gt, const scaph_config *cfg, scaph_engine **e)
 {
@@ -888,6 +940,7 @@ int scaph_engine_sync(scaph_engine *e)
 {
     if (!e) return set_error(SCAPH_EINVAL, "null engine");
     SCAPH_CUDA(cudaStreamSynchronize(e->st));
+    if (e->copy_st) SCAPH_CUDA(cudaStreamSynchronize(e->copy_st));
     return SCAPH_OK;
 }
 

@@ -157,6 +157,13 @@ struct scaph_engine {
     std::vector<std::pair<double, double>> dual_ms; // (push, pull) per level
     uint32_t *d_snap = nullptr, *d_pcnt = nullptr, *d_pdatas = nullptr;
     uint32_t *h_fstage = nullptr;  // pinned: the feature pass's page counts
+    // pipelined host output (scaph_bfs_enqueue): two device depth buffers,
+    // a copy stream, and per buffer "traversal done" / "copy done" events
+    uint32_t *d_pipe[2] = {nullptr, nullptr};
+    cudaStream_t copy_st = nullptr;
+    cudaEvent_t ev_run[2] = {nullptr, nullptr}, ev_copied[2] = {nullptr, nullptr};
+    uint64_t pipe_runs = 0;
+    int enqueue(uint32_t src, uint32_t *host_depths);
     // incremental page counts of the learned host loop (out of core)
     uint32_t *d_hist_in = nullptr;  // [kHistLevels][2][in-pages]: discoveries by in-page
     uint32_t *h_inc = nullptr;      // pinned read-back of a level's histograms

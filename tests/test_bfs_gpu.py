@@ -78,6 +78,35 @@ def test_async_runs_back_to_back():
     eng.close()
 
 
+def test_enqueue_pipelines_host_output():
+    """Pipelined runs into page-locked host buffers (two device buffers reused
+    in turn, copies on a second stream) give the oracle's depths, interleaved
+    with plain synchronous runs; the host loop refuses the pipelined call."""
+    csr = S.Csr.rmat(14, 16, seed=G.SEED + 10)
+    g = S.PagedGraph.from_csr(csr, pagesize_words=1 << 14)
+    eng = S.Engine(g)
+    srcs = G.sources(csr, 5, 10)
+    bufs = [S.PinnedArray(csr.V) for _ in srcs]
+    for b in bufs:
+        b.array.fill(0xDEADBEEF)
+    for s, b in zip(srcs[:3], bufs[:3]):
+        eng.bfs_enqueue(s, b.array)
+    mid, _, _ = eng.bfs(srcs[0])  # a synchronous run between pipelined ones
+    for s, b in zip(srcs[3:], bufs[3:]):
+        eng.bfs_enqueue(s, b.array)
+    eng.sync()
+    assert np.array_equal(mid, O.bfs(csr.idx, csr.ngh, srcs[0]))
+    for s, b in zip(srcs, bufs):
+        assert np.array_equal(b.array, O.bfs(csr.idx, csr.ngh, s)), f"src {s}"
+    eng.close()
+    hl = S.Engine(g, use_graph=2)
+    with pytest.raises(S.ScaphError):
+        hl.bfs_enqueue(srcs[0], bufs[0].array)
+    hl.close()
+    for b in bufs:
+        b.close()
+
+
 def test_rmat16_reference_sentinel(rmat16):
     """Reference convention: unreached = 63 (app/bfs.cu:18), bit-exact with bfs::check's rule."""
     csr, g = rmat16
