@@ -24,14 +24,14 @@
 #include "engine.h"
 #include "kernels.h"
 
-using // Pull phase A's first probes: 0 = the first in-edges, read from the pages;
+using namespace scaph;
+
+// Pull phase A's first probes: 0 = the first in-edges, read from the pages;
 // 1 = the same edges from dense per-vertex rows (16 B per vertex of device
 // memory); 2 = dense rows of the in-neighbours with the largest out-degree.
 #ifndef SCAPH_PULL_HEAD
 #define SCAPH_PULL_HEAD 2
 #endif
-
-namespace scaph;
 
 namespace scaph {
 
@@ -418,6 +418,9 @@ int scaph_engine::run_host_loop(uint32_t src, uint32_t *dd, uint32_t *dp)
     }
     // page counts of the last feature pass, reused by the pager
     std::vector<uint32_t> feat_pc, feat_hist;
+    // The pool holds the in-edge pages with half the out-edge pages beside
+    // them: what a level brings in stays for later levels and traversals.
+    const bool keep_pool = pager && !symmetric && 2 * npi + np <= 2 * (size_t)pager_nslots(pager);
     while (nf > 0 && level < kMaxLevels && (uint64_t)level + 1 < unreached) {
         const uint64_t used = vis_e + dead_edges;
         const uint64_t mu = E > used ? E - used : 0;
@@ -441,28 +444,46 @@ int scaph_engine::run_host_loop(uint32_t src, uint32_t *dd, uint32_t *dp)
                 y.resize(out);
                 mlp_forward_host(sched_host, f.data(), y.data());
                 if (level > 0) {
-                    // the network models kernel time (trained resident);
-                    // out of core the page traffic each direction would
-                    // cause is known exactly and overrides it when it
-                    // clearly dominates
+                    // the network models kernel time (trained resident)
                     dir = y[0] > 0.f ? 1 : 0;
                     // far from the alpha/beta threshold the rule decides
                     const int sure = alpha_beta_confident(prev_dir, nf, mf, mu, V, cfg.alpha, cfg.beta);
                     if (sure >= 0) dir = sure;
                     if (pager) {
-                        const int npi = (int)pc.size() / 2;
+                        // out of core the page traffic each direction would
+                        // cause is known exactly.  In a pool that keeps what
+                        // levels bring in (keep_pool), its contents follow
+                        // the directions taken: there, where either direction
+                        // would move pages, the rule decides (a level-local
+                        // choice by traffic leaves the pool worse for the
+                        // traversals after it).  In a smaller pool pages do
+                        // not stay, and a direction whose traffic is more
+                        // than twice the other's (and 1 ms more) is turned
+                        // around.
+                        const int npc = (int)pc.size() / 2;
                         const double t_push = pager_transfer_ms(pager, 0, hist.data(), hist.data() + np, (int)np,
                                                                 cfg.compact_threshold);
-                        const double t_pull = pager_transfer_ms(pager, symmetric ? 0 : 1, pc.data(), pc.data() + npi,
-                                                                npi, cfg.compact_threshold);
-                        if (t_push > 2 * t_pull + 1.0) dir = 1;
-                        else if (t_pull > 2 * t_push + 1.0) dir = 0;
+                        const double t_pull = pager_transfer_ms(pager, symmetric ? 0 : 1, pc.data(), pc.data() + npc,
+                                                                npc, cfg.compact_threshold);
+                        if (keep_pool) {
+                            if (t_push > 0 || t_pull > 0) dir = ab;
+                        } else if (t_push > 2 * t_pull + 1.0) {
+                            dir = 1;
+                        } else if (t_pull > 2 * t_push + 1.0) {
+                            dir = 0;
+                        }
                     }
                 }
                 // prefetch only pages the network is confident about (into
-                // free slots; never at the expense of resident pages)
-                for (int p = 0; p + 1 < out && p < (int)np; p++)
-                    if (y[1 + p] > 2.f) prefetch_pages.push_back(p);
+                // free slots; never at the expense of resident pages).  A
+                // pool that keeps what levels bring in is prefetched into
+                // only once it is three-quarters full (steady state, where
+                // the copies stay for later traversals); filling from cold,
+                // demand paging reads sparse pages zero-copy, and a prefetch
+                // would copy them whole.
+                if (!keep_pool || 4 * pager_free_slots(pager) < pager_nslots(pager))
+                    for (int p = 0; p + 1 < out && p < (int)np; p++)
+                        if (y[1 + p] > 2.f) prefetch_pages.push_back(p);
             }
             feat_pc = pc;
             feat_hist = std::move(hist);
@@ -741,7 +762,7 @@ int scaph_engine::collect(bool from_graph)
         if (from_graph) {
             t.ms = (double)(lc.t_end - tprev) * 1e-6;
             tprev = lc.t_end;
-            launches += (lc.dir == 0 ? 2 : 1) + 1;
+            launches += 4;  // push, giant, pull and decide run every level (two leave at once)
         } else {
             float ms = 0;
             cudaEventElapsedTime(&ms, ev_level[2 * l], ev_level[2 * l + 1]);

@@ -71,6 +71,8 @@ void pager_counters(const Pager *pg, uint64_t *h2d, uint64_t *zc, uint64_t *faul
 void pager_reset_counters(Pager *pg);
 void pager_evict_all(Pager *pg);
 int pager_nslots(const Pager *pg);
+// Slots holding no page.
+int pager_free_slots(const Pager *pg);
 float pager_resident_fraction(const Pager *pg, int gid, const std::vector<int> *pages);
 // Page traffic (ms at the measured PCIe bandwidth) a level would cause on
 // graph gid: per page with cnt > 0, nothing if resident, its active words

@@ -628,6 +628,13 @@ void pager_evict_all(Pager *pg) { pg->evict_all(); }
 
 int pager_nslots(const Pager *pg) { return pg->nslots; }
 
+int pager_free_slots(const Pager *pg)
+{
+    int n = 0;
+    for (const auto &s : pg->slots) n += s.g < 0;
+    return n;
+}
+
 float pager_resident_fraction(const Pager *pg, int gid, const std::vector<int> *pages)
 {
     const Pager::GState &G = pg->gs[gid];
