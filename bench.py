@@ -39,7 +39,7 @@ FALLBACK_HBM_GBS = 6650.0
 
 # Measured DRAM bytes (read + write) per k_pull launch on RMAT-24, mean over 200 launches;
 # see profiles/k_pull_rmat24_traffic.md for the ncu command.
-K_PULL_TRAFFIC_BYTES = 295_719_334
+K_PULL_TRAFFIC_BYTES = 295_834_080
 
 
 def parse_args():
@@ -577,8 +577,10 @@ def run_ours(args, world):
         e_ms = replicas.max_over_ranks(ev2.elapsed_time(ev3), world, "cuda")
         return replicas.aggregate_gteps(world, n_e2e, E, e_ms)
 
-    e2e_value = timed_e2e(lambda i: eng.bfs_enqueue(src_of(i), host_bufs[i & 1].array))
     e2e_sync_value = timed_e2e(lambda i: eng.bfs(src_of(i), depth_out=host_bufs[0].array))
+    # the pipelined call needs graph mode; the host-driven loop has the synchronous one only
+    e2e_value = e2e_sync_value if args.host_loop else \
+        timed_e2e(lambda i: eng.bfs_enqueue(src_of(i), host_bufs[i & 1].array))
 
     # roofline of the dominant kernel from per-level device times over every
     # source (separate, untimed pass)
@@ -610,7 +612,8 @@ def run_ours(args, world):
             "config": config_dict(csr, args.scale, len(srcs), {"parallelism": f"replicas x{world}",
                                                                 "graph_gen_s": round(gen_s, 1)}),
             "e2e": {"value": e2e_value, "unit": "GTEPS", "h2d_bytes_per_step": 4, "d2h_bytes_per_step": V * 4,
-                    "api": "scaph_bfs_enqueue (pipelined, page-locked host output)",
+                    "api": "scaph_bfs (one step at a time)" if args.host_loop else
+                           "scaph_bfs_enqueue (pipelined, page-locked host output)",
                     "sync_value": e2e_sync_value, "sync_api": "scaph_bfs (one step at a time)"},
             "gpu_launches": launches, "roofline": roof, "clocks": clk,
             "graph500_gteps_median": statistics.median(g500)}
