@@ -176,7 +176,10 @@ typedef struct scaph_config {
     int32_t  device;           /* CUDA device ordinal                       */
     void    *stream;           /* cudaStream_t to run on; NULL = own stream */
     int32_t  record_features;  /* host loop: keep the scheduler's feature
-                                  vector of every level (scaph_bfs_features) */
+                                  vector of every level (scaph_bfs_features);
+                                  graph mode: record the per-level page
+                                  histograms (scaph_bfs_page_hist), which
+                                  the learned direction records anyway     */
     int32_t  dual_timing;      /* host loop, graph resident: run every level
                                   both ways from the same state and record
                                   both times (training labels)             */
@@ -258,7 +261,9 @@ typedef struct scaph_level_trace {
 } scaph_level_trace;
 int scaph_bfs_trace(scaph_engine *e, scaph_level_trace *out, int cap);
 /* Active-vertex histogram of the frontier at `level` of the last run:
- * nodes[p] / datas[p] as get_page_info computes them (src/gpu_engine.cuh:397-441). */
+ * nodes[p] / datas[p] as get_page_info computes them (src/gpu_engine.cuh:397-441).
+ * Recorded by every host-loop run; by a graph-mode run only with
+ * record_features or the learned direction (SCAPH_EUNSUPPORTED otherwise). */
 int scaph_bfs_page_hist(scaph_engine *e, int level, uint32_t *nodes,
                         uint32_t *datas, int npages);
 

@@ -610,7 +610,10 @@ int scaph_engine::build_graph()
     gargs.base = base_state(d_depth, nullptr);
     gargs.bm3 = d_bm3;
     gargs.ctr0 = d_ctr;
-    gargs.hist0 = d_hist;
+    // the per-page histogram of each level's discoveries (get_page_info's
+    // counts) costs ~3% of a resident traversal: recorded in graph mode only
+    // for the learned direction (its features) or on request
+    gargs.hist0 = graph_records_hist() ? d_hist : nullptr;
     gargs.hist_levels = kHistLevels;
     gargs.npages_h = (uint32_t)np;
     gargs.ctl = d_ctl;
@@ -814,6 +817,7 @@ int scaph_engine::bfs(uint32_t src, uint32_t *depths, uint32_t *parents, int out
     pending_src = src;
     pending_parent = dp != nullptr;
     const bool use_graph = graph_mode();
+    last_hist = !use_graph || graph_records_hist();
     SCAPH_CUDA(cudaEventRecord(ev_start, st));
     int rc = use_graph ? launch_graph(src, dd, dp) : run_host_loop(src, dd, dp);
     if (rc) return rc;
@@ -859,6 +863,7 @@ int scaph_engine::enqueue(uint32_t src, uint32_t *host_depths)
     SCAPH_CUDA(cudaStreamWaitEvent(st, ev_copied[b], 0));  // the buffer's previous copy is done
     pending_src = src;
     pending_parent = false;
+    last_hist = graph_records_hist();
     int rc = launch_graph(src, d_pipe[b], nullptr);
     if (rc) return rc;
     pending = true;
@@ -986,6 +991,9 @@ int scaph_bfs_page_hist(scaph_engine *e, int level, uint32_t *nodes, uint32_t *d
     }
     const int np = (int)e->g->pages.size();
     if (npages < np) return set_error(SCAPH_EINVAL, "need %d pages", np);
+    if (!e->last_hist)
+        return set_error(SCAPH_EUNSUPPORTED, "graph-mode runs record page histograms only with record_features "
+                                             "or the learned direction");
     // histogram slot L holds the frontier discovered BY level L, i.e. the
     // frontier AT level L+1 (level 0's frontier is the source alone)
     if (level < 0 || level > e->last_levels || level > scaph_engine::kHistLevels)

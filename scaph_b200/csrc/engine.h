@@ -166,6 +166,11 @@ struct scaph_engine {
     cudaEvent_t ev_run[2] = {nullptr, nullptr}, ev_copied[2] = {nullptr, nullptr};
     uint64_t pipe_runs = 0;
     int enqueue(uint32_t src, uint32_t *host_depths);
+    bool last_hist = true;  // the last run recorded per-level page histograms
+    bool graph_records_hist() const
+    {
+        return (cfg.direction == SCAPH_DIR_LEARNED && sched) || cfg.record_features;
+    }
     // incremental page counts of the learned host loop (out of core)
     uint32_t *d_hist_in = nullptr;  // [kHistLevels][2][in-pages]: discoveries by in-page
     uint32_t *h_inc = nullptr;      // pinned read-back of a level's histograms

@@ -186,7 +186,14 @@ def test_trace_and_page_histogram(use_graph):
     csr = S.Csr.rmat(14, 16, seed=G.SEED + 6)
     g = S.PagedGraph.from_csr(csr, pagesize_words=1 << 14)
     src = G.sources(csr, 1, 6)[0]
-    eng = S.Engine(g, use_graph=use_graph)
+    if use_graph != 2:
+        # graph mode records the histograms only on request
+        plain = S.Engine(g, use_graph=use_graph)
+        plain.bfs(src)
+        with pytest.raises(S.ScaphError):
+            plain.page_hist(1)
+        plain.close()
+    eng = S.Engine(g, use_graph=use_graph, record_features=1)
     depth, _, st = eng.bfs(src)
     tr = eng.trace()
     assert len(tr) == st.levels
