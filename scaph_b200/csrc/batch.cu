@@ -249,9 +249,10 @@ __global__ void k_bt_start(MsDev *ps, MsDev base, BatchCtl *ctl, BatchCtl c0)
 }
 
 // depth rows: for each query slot of u's graph, the depth of u (bit planes),
-// or `unreached`
-template <int NW>
-__global__ void k_bt_unpack(const MsDev *ps, BatchArgs a, uint32_t *out, int nplanes, uint32_t unreached)
+// or `unreached`; NP (the depth bit planes) is a template argument so that
+// the planes stay in registers
+template <int NW, int NP>
+__global__ void k_bt_unpack(const MsDev *ps, BatchArgs a, uint32_t *out, uint32_t unreached)
 {
     __shared__ uint32_t slo[kBatchMaxGraphs + 1], sqs[kBatchMaxGraphs + 1];
     for (int i = threadIdx.x; i <= a.ngraphs; i += blockDim.x) {
@@ -267,8 +268,9 @@ __global__ void k_bt_unpack(const MsDev *ps, BatchArgs a, uint32_t *out, int npl
         const uint32_t q0 = sqs[g], q1 = sqs[g + 1];
         if (q0 == q1) continue;
         const Mask<NW> sn = ld_seen<NW>(s.sa, u);
-        Mask<NW> pl[kBatchPlanes + 8];
-        for (int k = 0; k < nplanes; k++) pl[k] = ld_mask<NW>(s.planes[k], u);
+        Mask<NW> pl[NP];
+#pragma unroll
+        for (int k = 0; k < NP; k++) pl[k] = ld_mask<NW>(s.planes[k], u);
         const uint32_t local = u - slo[g];
         for (uint32_t j = q0; j < q1; j++) {
             const uint32_t b = j - q0;
@@ -276,12 +278,27 @@ __global__ void k_bt_unpack(const MsDev *ps, BatchArgs a, uint32_t *out, int npl
             uint32_t d = unreached;
             if ((sn.w[word] >> bit) & 1ull) {
                 d = 0;
-                for (int k = 0; k < nplanes; k++) d |= (uint32_t)((pl[k].w[word] >> bit) & 1ull) << k;
+#pragma unroll
+                for (int k = 0; k < NP; k++) d |= (uint32_t)((pl[k].w[word] >> bit) & 1ull) << k;
             }
             out[a.qoff[j] + local] = d;
         }
     }
 }
+
+// The k_bt_unpack instantiation for the batch's plane counts (kBatchPlanes,
+// then three more per relaunch, up to kMsPlanes).
+template <int NW>
+const void *bt_unpack_kernel(int nplanes)
+{
+    switch (nplanes) {
+    case kBatchPlanes: return (const void *)k_bt_unpack<NW, kBatchPlanes>;
+    case kBatchPlanes + 3: return (const void *)k_bt_unpack<NW, kBatchPlanes + 3>;
+    case kBatchPlanes + 6: return (const void *)k_bt_unpack<NW, kBatchPlanes + 6>;
+    default: return (const void *)k_bt_unpack<NW, kMsPlanes>;
+    }
+}
+static_assert(kBatchPlanes + 6 < kMsPlanes, "plane counts of a batch: 5, 8, 11, then 12");
 
 }  // namespace
 }  // namespace scaph
@@ -564,9 +581,8 @@ int scaph_batch::build_graph(uint32_t *out)
 
     cudaGraphNode_t n_unpack;
     uint32_t unr = e->unreached;
-    int npl = nplanes;
-    void *unp_args[] = {&psc, &args, &out, &npl, &unr};
-    const void *f_unp = nw == 2 ? (const void *)k_bt_unpack<2> : (const void *)k_bt_unpack<1>;
+    void *unp_args[] = {&psc, &args, &out, &unr};
+    const void *f_unp = nw == 2 ? bt_unpack_kernel<2>(nplanes) : bt_unpack_kernel<1>(nplanes);
     rc = kernel_node(graph, f_unp, dim3(e->num_sms * 8), dim3(256), unp_args, {n_while}, &n_unpack);
     if (rc) return rc;
     SCAPH_CUDA(cudaGraphInstantiate(&gexec, graph, 0));

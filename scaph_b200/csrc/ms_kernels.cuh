@@ -145,7 +145,30 @@ struct MsDev {
     const uint32_t *head;
     const uint32_t *indeg;
     uint32_t head_ranked;
+    // pull levels: the frontier masks compacted (fmask[r] = visit_cur[v]
+    // for the r-th frontier vertex v) and, per bitmap word w, {act_cur[w],
+    // frontier vertices before word w}; one 8-byte load then gives a
+    // neighbour's frontier bit and its rank, and the compacted masks stay in
+    // L2 where the vertex-indexed array does not.  Null: read visit_cur.
+    const uint2 *actrank;
+    const unsigned long long *fmask;
 };
+
+// Frontier bit of v and, when set, its frontier mask (compacted or
+// vertex-indexed): the act word (with rank) load, then the mask load.
+template <int NW>
+__device__ __forceinline__ uint2 ld_actrank(const MsDev &s, uint32_t v)
+{
+    if (s.actrank) return __ldg(&s.actrank[v >> 5]);
+    return make_uint2(__ldg(&s.act_cur[v >> 5]), 0u);
+}
+
+template <int NW>
+__device__ __forceinline__ Mask<NW> ld_frontier_mask(const MsDev &s, uint32_t v, uint2 ar)
+{
+    if (s.actrank) return ld_mask<NW>(s.fmask, ar.y + __popc(ar.x & ((1u << (v & 31)) - 1u)));
+    return ld_mask<NW>(s.visit_cur, v);
+}
 
 
 namespace {
@@ -466,12 +489,16 @@ __device__ __forceinline__ void ms_pull_body(const GraphDev &g, const MsDev &s, 
                     for (int j = 0; j < 4; j++) v[j] = (uint32_t)j < len ? __ldg(&g.pool[st + j]) : 0xFFFFFFFFu;
                 }
                 bool on[4];
+                uint2 ar[4];
 #pragma unroll
-                for (int j = 0; j < 4; j++) on[j] = v[j] < s.V && test_bit(s.act_cur, v[j]);
+                for (int j = 0; j < 4; j++) {
+                    ar[j] = v[j] < s.V ? ld_actrank<NW>(s, v[j]) : make_uint2(0u, 0u);
+                    on[j] = (ar[j].x >> (v[j] & 31)) & 1u;
+                }
 #pragma unroll
                 for (int j = 0; j < 4; j++) {
                     if (on[j]) {
-                        const Mask<NW> m = ld_mask<NW>(s.visit_cur, v[j]);
+                        const Mask<NW> m = ld_frontier_mask<NW>(s, v[j], ar[j]);
 #pragma unroll
                         for (int i = 0; i < NW; i++) acc.w[i] |= m.w[i];
                     }
@@ -523,10 +550,12 @@ __device__ __forceinline__ void ms_pull_body(const GraphDev &g, const MsDev &s, 
                 const uint4 val = ld_nc_v4(g.pool + quad * 4);
                 const uint32_t vals[4] = {val.x, val.y, val.z, val.w};
                 bool in[4], on[4];
+                uint2 ar[4];
 #pragma unroll
                 for (int j = 0; j < 4; j++) {
                     in[j] = quad * 4 + j >= aa && quad * 4 + j < bb;
-                    on[j] = in[j] && vals[j] < s.V && test_bit(s.act_cur, vals[j]);
+                    ar[j] = in[j] && vals[j] < s.V ? ld_actrank<NW>(s, vals[j]) : make_uint2(0u, 0u);
+                    on[j] = (ar[j].x >> (vals[j] & 31)) & 1u;
                     a.inspected += in[j] ? 1 : 0;
                 }
                 Mask<NW> part;
@@ -535,7 +564,7 @@ __device__ __forceinline__ void ms_pull_body(const GraphDev &g, const MsDev &s, 
 #pragma unroll
                 for (int j = 0; j < 4; j++) {
                     if (on[j]) {
-                        const Mask<NW> m = ld_mask<NW>(s.visit_cur, vals[j]);
+                        const Mask<NW> m = ld_frontier_mask<NW>(s, vals[j], ar[j]);
 #pragma unroll
                         for (int w2 = 0; w2 < NW; w2++) part.w[w2] |= m.w[w2];
                     }
@@ -658,24 +687,119 @@ __global__ void k_ms_sources(MsDev s, const uint32_t *srcs, int nsrc)
 }
 
 // depth[i][u] from the bit planes; unreached where seen lacks bit i
+// ---------------------------------------------------------------------------
+// frontier compaction for pull levels (MsDev::actrank / fmask)
+// ---------------------------------------------------------------------------
+constexpr int kRankWordsPerCta = 4 * kMsBlock;  // bitmap words a CTA ranks
+
+// Frontier vertices in each CTA's run of kRankWordsPerCta words.
+static __global__ void __launch_bounds__(kMsBlock) k_ms_rank_sums(const uint32_t *act, uint32_t nwords, uint32_t *bsum)
+{
+    __shared__ uint32_t wsum[kMsBlock / 32];
+    const size_t w0 = (size_t)blockIdx.x * kRankWordsPerCta;
+    uint32_t c = 0;
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+        const size_t w = w0 + (size_t)j * kMsBlock + threadIdx.x;
+        if (w < nwords) c += __popc(act[w]);
+    }
+    uint32_t total;
+    kc::block_exclusive_scan<kMsBlock>(c, wsum, total);
+    if (threadIdx.x == 0) bsum[blockIdx.x] = total;
+}
+
+// Exclusive scan of the nb run totals, in place (one CTA).
+static __global__ void __launch_bounds__(kMsBlock) k_ms_rank_scan(uint32_t *bsum, uint32_t nb)
+{
+    __shared__ uint32_t wsum[kMsBlock / 32];
+    uint32_t carry = 0;
+    for (uint32_t i0 = 0; i0 < nb; i0 += kMsBlock) {
+        const uint32_t i = i0 + threadIdx.x;
+        const uint32_t x = i < nb ? bsum[i] : 0u;
+        uint32_t total;
+        const uint32_t ex = kc::block_exclusive_scan<kMsBlock>(x, wsum, total);
+        if (i < nb) bsum[i] = carry + ex;
+        carry += total;
+    }
+}
+
+// actrank[w] = {act[w], frontier vertices before word w}, and the frontier
+// masks gathered in vertex order into fmask.
 template <int NW>
-__global__ void k_ms_unpack(MsDev s, uint32_t *out, int nsrc, int nplanes, uint32_t unreached)
+__global__ void __launch_bounds__(kMsBlock) k_ms_rank_gather(const uint32_t *act, uint32_t nwords, const uint32_t *bsum,
+                                                             const unsigned long long *visit, uint2 *actrank,
+                                                             unsigned long long *fmask)
+{
+    __shared__ uint32_t wsum[kMsBlock / 32];
+    // this thread takes 4 consecutive words of the CTA's run
+    const size_t w0 = (size_t)blockIdx.x * kRankWordsPerCta + 4ull * threadIdx.x;
+    uint32_t a[4], c = 0;
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+        a[j] = w0 + j < nwords ? act[w0 + j] : 0u;
+        c += __popc(a[j]);
+    }
+    uint32_t total;
+    uint32_t r = bsum[blockIdx.x] + kc::block_exclusive_scan<kMsBlock>(c, wsum, total);
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+        if (w0 + j >= nwords) break;
+        actrank[w0 + j] = make_uint2(a[j], r);
+        uint32_t m = a[j];
+        while (m) {
+            const uint32_t v = (uint32_t)((w0 + j) << 5) + (__ffs(m) - 1);
+            st_mask<NW>(fmask, r++, ld_mask<NW>(visit, v));
+            m &= m - 1;
+        }
+    }
+}
+
+// Depth rows out[i][u] from the seen masks and the NP depth bit planes.  NP
+// is a template argument so that the planes stay in registers (a run-time
+// plane loop put them in local memory and made this pass 4x slower than its
+// writes).
+template <int NW, int NP>
+__global__ void __launch_bounds__(kMsBlock) k_ms_unpack(MsDev s, uint32_t *out, int nsrc, uint32_t unreached)
 {
     const size_t stride = (size_t)gridDim.x * blockDim.x;
     for (size_t u = (size_t)blockIdx.x * blockDim.x + threadIdx.x; u < s.V; u += stride) {
         const Mask<NW> sn = ld_seen<NW>(s.sa, (uint32_t)u);
-        Mask<NW> pl[kMsPlanes];
-        for (int k = 0; k < nplanes; k++) pl[k] = ld_mask<NW>(s.planes[k], (uint32_t)u);
+        Mask<NW> pl[NP > 0 ? NP : 1];
+#pragma unroll
+        for (int k = 0; k < NP; k++) pl[k] = ld_mask<NW>(s.planes[k], (uint32_t)u);
         for (int i = 0; i < nsrc; i++) {
             const int word = i >> 6, b = i & 63;
             uint32_t d = unreached;
             if ((sn.w[word] >> b) & 1ull) {
                 d = 0;
-                for (int k = 0; k < nplanes; k++) d |= (uint32_t)((pl[k].w[word] >> b) & 1ull) << k;
+#pragma unroll
+                for (int k = 0; k < NP; k++) d |= (uint32_t)((pl[k].w[word] >> b) & 1ull) << k;
             }
             out[(size_t)i * s.V + u] = d;
         }
     }
 }
+
+// The k_ms_unpack instantiation for nplanes (0..kMsPlanes).
+template <int NW>
+const void *ms_unpack_kernel(int nplanes)
+{
+    switch (nplanes) {
+    case 0: return (const void *)k_ms_unpack<NW, 0>;
+    case 1: return (const void *)k_ms_unpack<NW, 1>;
+    case 2: return (const void *)k_ms_unpack<NW, 2>;
+    case 3: return (const void *)k_ms_unpack<NW, 3>;
+    case 4: return (const void *)k_ms_unpack<NW, 4>;
+    case 5: return (const void *)k_ms_unpack<NW, 5>;
+    case 6: return (const void *)k_ms_unpack<NW, 6>;
+    case 7: return (const void *)k_ms_unpack<NW, 7>;
+    case 8: return (const void *)k_ms_unpack<NW, 8>;
+    case 9: return (const void *)k_ms_unpack<NW, 9>;
+    case 10: return (const void *)k_ms_unpack<NW, 10>;
+    case 11: return (const void *)k_ms_unpack<NW, 11>;
+    default: return (const void *)k_ms_unpack<NW, 12>;
+    }
+}
+static_assert(kMsPlanes == 12, "ms_unpack_kernel covers 0..12 planes");
 
 }  // namespace scaph
