@@ -37,8 +37,9 @@ PEAKS_FILE = os.path.join(ROOT, "MEASURED_PEAKS.json")
 FALLBACK_HBM_GBS = 6650.0
 
 
-# Measured DRAM bytes (read + write) per k_pull launch on RMAT-24, mean over 200 launches;
-# see profiles/k_pull_rmat24_traffic.md for the ncu command.
+# Measured DRAM bytes (read + write) per k_pull launch on RMAT-24: ncu's dram__bytes_read.sum
+# + dram__bytes_write.sum over all 200 k_pull launches of
+# `bench.py --host-loop --steps 2 --warmup 1 --no-cpu --no-extras`, mean per launch.
 K_PULL_TRAFFIC_BYTES = 295_834_080
 
 
@@ -601,7 +602,7 @@ def run_ours(args, world):
             "achieved": achieved, "peak": peak, "unit": "GB/s",
             "frac": achieved / peak if achieved else None, "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)",
             # DRAM read+write per k_pull launch, ncu over every k_pull launch of the same
-            # command with --host-loop (profiles/k_pull_rmat24_traffic.md)
+            # command with --host-loop (K_PULL_TRAFFIC_BYTES)
             "traffic": K_PULL_TRAFFIC_BYTES if dom == 1 and args.scale == 24 else None,
             "launches_sampled": nl, "alg_bytes_per_launch": alg / nl if nl else None,
             "share_of_level_time": dms / (per_dir[0][1] + per_dir[1][1])}

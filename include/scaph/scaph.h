@@ -207,7 +207,11 @@ typedef struct scaph_bfs_stats {
     uint64_t reached;           /* vertices with a finite depth             */
     uint64_t reached_edges;     /* sum of out-degrees of reached vertices   */
     uint64_t edges_inspected;   /* adjacency words read by the kernels      */
-    uint64_t alg_bytes;         /* algorithmic HBM bytes    */
+    uint64_t alg_bytes;         /* algorithmic HBM bytes: push levels 12 per
+                                   frontier vertex + 4 per edge; pull levels
+                                   12 per unvisited vertex + 4 per in-edge
+                                   inspected; each level V/8 of bitmap and
+                                   4 (+4 with parents) per discovered vertex */
     uint64_t h2d_bytes;         /* page bytes copied host->HBM              */
     uint64_t zc_bytes;          /* page bytes read zero-copy over PCIe      */
     uint64_t page_faults;       /* page loads on demand                     */
