@@ -274,12 +274,13 @@ __global__ void k_bt_unpack(const MsDev *ps, BatchArgs a, uint32_t *out, uint32_
         const uint32_t local = u - slo[g];
         for (uint32_t j = q0; j < q1; j++) {
             const uint32_t b = j - q0;
-            const int word = (int)(b >> 6), bit = (int)(b & 63);
+            const bool hi = b >= 64;
+            const int bit = (int)(b & 63);
             uint32_t d = unreached;
-            if ((sn.w[word] >> bit) & 1ull) {
+            if ((mask_word<NW>(sn, hi) >> bit) & 1ull) {
                 d = 0;
 #pragma unroll
-                for (int k = 0; k < NP; k++) d |= (uint32_t)((pl[k].w[word] >> bit) & 1ull) << k;
+                for (int k = 0; k < NP; k++) d |= (uint32_t)((mask_word<NW>(pl[k], hi) >> bit) & 1ull) << k;
             }
             out[a.qoff[j] + local] = d;
         }

@@ -757,26 +757,64 @@ __global__ void __launch_bounds__(kMsBlock) k_ms_rank_gather(const uint32_t *act
 // Depth rows out[i][u] from the seen masks and the NP depth bit planes.  NP
 // is a template argument so that the planes stay in registers (a run-time
 // plane loop put them in local memory and made this pass 4x slower than its
-// writes).
+// writes).  When the rows are 16-byte aligned and the planes of four
+// vertices fit in registers, a thread takes four consecutive vertices and
+// writes each row's four depths with one 16-byte store.
+// Word `hi` (0 or 1) of a mask, selected without indexing the array by a
+// run-time value (which would put the masks in local memory).
+template <int NW>
+__device__ __forceinline__ unsigned long long mask_word(const Mask<NW> &m, bool hi)
+{
+    if constexpr (NW == 1) return m.w[0];
+    else return hi ? m.w[NW - 1] : m.w[0];
+}
+
+template <int NW, int NP>
+__device__ __forceinline__ uint32_t unpack_depth(const Mask<NW> &sn, const Mask<NW> (&pl)[NP > 0 ? NP : 1], int i,
+                                                 uint32_t unreached)
+{
+    const bool hi = i >= 64;
+    const int b = i & 63;
+    if (!((mask_word<NW>(sn, hi) >> b) & 1ull)) return unreached;
+    uint32_t d = 0;
+#pragma unroll
+    for (int k = 0; k < NP; k++) d |= (uint32_t)((mask_word<NW>(pl[k], hi) >> b) & 1ull) << k;
+    return d;
+}
+
 template <int NW, int NP>
 __global__ void __launch_bounds__(kMsBlock) k_ms_unpack(MsDev s, uint32_t *out, int nsrc, uint32_t unreached)
 {
+    constexpr bool kVec = NW * NP <= 8;
     const size_t stride = (size_t)gridDim.x * blockDim.x;
-    for (size_t u = (size_t)blockIdx.x * blockDim.x + threadIdx.x; u < s.V; u += stride) {
+    const size_t t0 = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (kVec && (s.V & 3u) == 0 && (reinterpret_cast<uintptr_t>(out) & 15u) == 0) {
+        for (size_t q = t0; q < (s.V >> 2); q += stride) {
+            const uint32_t u0 = (uint32_t)q << 2;
+            Mask<NW> sn[4], pl[4][NP > 0 ? NP : 1];
+#pragma unroll
+            for (int r = 0; r < 4; r++) {
+                sn[r] = ld_seen<NW>(s.sa, u0 + r);
+#pragma unroll
+                for (int k = 0; k < NP; k++) pl[r][k] = ld_mask<NW>(s.planes[k], u0 + r);
+            }
+            for (int i = 0; i < nsrc; i++) {
+                uint4 d;
+                d.x = unpack_depth<NW, NP>(sn[0], pl[0], i, unreached);
+                d.y = unpack_depth<NW, NP>(sn[1], pl[1], i, unreached);
+                d.z = unpack_depth<NW, NP>(sn[2], pl[2], i, unreached);
+                d.w = unpack_depth<NW, NP>(sn[3], pl[3], i, unreached);
+                *reinterpret_cast<uint4 *>(out + (size_t)i * s.V + u0) = d;
+            }
+        }
+        return;
+    }
+    for (size_t u = t0; u < s.V; u += stride) {
         const Mask<NW> sn = ld_seen<NW>(s.sa, (uint32_t)u);
         Mask<NW> pl[NP > 0 ? NP : 1];
 #pragma unroll
         for (int k = 0; k < NP; k++) pl[k] = ld_mask<NW>(s.planes[k], (uint32_t)u);
-        for (int i = 0; i < nsrc; i++) {
-            const int word = i >> 6, b = i & 63;
-            uint32_t d = unreached;
-            if ((sn.w[word] >> b) & 1ull) {
-                d = 0;
-#pragma unroll
-                for (int k = 0; k < NP; k++) d |= (uint32_t)((pl[k].w[word] >> b) & 1ull) << k;
-            }
-            out[(size_t)i * s.V + u] = d;
-        }
+        for (int i = 0; i < nsrc; i++) out[(size_t)i * s.V + u] = unpack_depth<NW, NP>(sn, pl, i, unreached);
     }
 }
 
