@@ -454,7 +454,7 @@ __device__ __forceinline__ void pull_body(const GraphDev &g, const BfsDev &s, ui
             // ---- phase A: kPPT unvisited vertices per thread, all
             // their row (or header and first in-edge) loads issued before
             // any of their frontier probes
-            uint32_t vv[kPPT], len[kPPT], need[kPPT];
+            uint32_t vv[kPPT], len[kPPT], need[kPPT], dg[kPPT];
             unsigned long long st[kPPT];
             int p[kPPT];
             uint32_t u[kPPT][kPullSerial];
@@ -463,6 +463,7 @@ __device__ __forceinline__ void pull_body(const GraphDev &g, const BfsDev &s, ui
             for (int i = 0; i < kPPT; i++) {
                 const uint32_t k = c0 + i * BLOCK + threadIdx.x;
                 vv[i] = 0;
+                dg[i] = 0;
                 len[i] = 0;
                 need[i] = 0;
                 st[i] = 0;
@@ -473,6 +474,7 @@ __device__ __forceinline__ void pull_body(const GraphDev &g, const BfsDev &s, ui
                 if (!ok[i]) continue;
                 const uint32_t v = q[k];
                 vv[i] = v;
+                dg[i] = __ldg(&s.degree[v]);  // travels with the row loads (needed if v is found)
                 if (s.head) {
                     // dense rows: the in-degree and the first in-edges of
                     // consecutive vertices, independent coalesced loads; the
@@ -529,7 +531,7 @@ __device__ __forceinline__ void pull_body(const GraphDev &g, const BfsDev &s, ui
                     s.depth[v] = s.level + 1;
                     if (s.parent) s.parent[v] = par;
                     mark_found(v);
-                    const uint32_t dv = __ldg(&s.degree[v]);
+                    const uint32_t dv = dg[i];
                     t.next++;
                     t.next_edges += dv;
                     if (s.page_nodes) {
