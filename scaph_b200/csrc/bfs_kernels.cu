@@ -1051,27 +1051,6 @@ cudaError_t run_level(int dir, int block, int grid, const GraphDev &g, const Bfs
     }
 }
 
-template <int BLOCK>
-static cudaError_t launch_level_g(int dir, int grid, const GraphDev &g, const BfsGraphArgs &a, cudaStream_t st)
-{
-    if (dir == 0) {
-        k_push_g<BLOCK><<<grid, BLOCK, 0, st>>>(g, a);
-        k_push_giant_g<BLOCK><<<grid, BLOCK, 0, st>>>(g, a);
-    } else {
-        k_pull_g<BLOCK><<<grid, BLOCK, 0, st>>>(g, a);
-    }
-    return cudaGetLastError();
-}
-
-cudaError_t run_level_graph(int dir, int block, int grid, const GraphDev &g, const BfsGraphArgs &a, cudaStream_t st)
-{
-    switch (block) {
-    case 128: return launch_level_g<128>(dir, grid, g, a, st);
-    case 512: return launch_level_g<512>(dir, grid, g, a, st);
-    default: return launch_level_g<256>(dir, grid, g, a, st);
-    }
-}
-
 void level_graph_kernels(int block, const void **push, const void **giant, const void **pull)
 {
     switch (block) {

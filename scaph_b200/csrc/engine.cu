@@ -7,9 +7,10 @@
 // Two ways to run the level loop:
 //  * graph mode (default when the whole graph is resident): one CUDA-graph
 //    launch per BFS.  Its level loop is a conditional WHILE node whose body
-//    is IF(push){push, giant} -> IF(pull){pull} -> decide; the decide kernel
-//    applies the direction rule on the device and sets the conditionals, so
-//    a BFS never returns to the host between levels;
+//    is push -> giant -> pull -> decide (the level kernels the level's
+//    direction does not select leave at once); the decide kernel applies the
+//    direction rule on the device and sets the loop's condition, so a BFS
+//    never returns to the host between levels;
 //  * host loop: one launch per level and a 64-byte counter read-back,
 //    with CUDA events around every level (per-level kernel timing) - used
 //    for out-of-core page batches and for the roofline pass.

@@ -15,8 +15,6 @@ cudaError_t run_level(int dir, int block, int grid, const GraphDev &g, const Bfs
 cudaError_t run_ranges(int dir, int block, int grid, const GraphDev &g, const BfsDev &s, const RangeList &rl,
                        cudaStream_t st);
 cudaError_t run_giant(int block, int grid, const GraphDev &g, const BfsDev &s, cudaStream_t st);
-// Graph mode: the same level kernels reading the level from a BfsCtl.
-cudaError_t run_level_graph(int dir, int block, int grid, const GraphDev &g, const BfsGraphArgs &a, cudaStream_t st);
 // k_graph_init(BfsGraphArgs, u32* depth, u32* parent, u32 src, u32 unreached, const u32* dead, u32 nlevels_clear)
 // Graph mode: the push, giant-chunk and pull kernels of a level (each leaves
 // at once unless the level's direction selects it).
@@ -24,9 +22,9 @@ void level_graph_kernels(int block, const void **push, const void **giant, const
 const void *graph_init_kernel();
 // k_graph_start(BfsGraphArgs)
 const void *graph_start_kernel();
-// k_decide(BfsGraphArgs, DecideArgs, handle loop, handle push, handle pull)
+// k_decide(BfsGraphArgs, DecideArgs, handle loop)
 const void *decide_kernel();
-// k_decide_learned(BfsGraphArgs, DecideArgs, MlpDev, handle loop, handle push, handle pull): 64 threads
+// k_decide_learned(BfsGraphArgs, DecideArgs, MlpDev, handle loop): 64 threads
 const void *decide_learned_kernel();
 // Resident CTAs per SM of the level kernel for `dir` at `block` threads.
 int level_occupancy(int dir, int block);
