@@ -91,6 +91,19 @@ int scaph_gen_powerlaw(uint32_t V, uint64_t E, double zipf_s, uint32_t max_degre
 int scaph_gen_web(uint32_t V, uint64_t E, double s, uint32_t max_degree,
                   uint32_t block, double local_frac, uint64_t seed, scaph_csr *out);
 
+/* Text exports of the flat CSR files <p>_csr.* for cross-framework checks,
+ * byte-identical to the reference's converters (inputs read as they read
+ * them: V from the size of _csr.deg, E from the size of _csr.ngh):
+ *   SCAPH_EXPORT_LIGRA         <p>.ligra         (tools/bin2ligra.cpp:66-108)
+ *   SCAPH_EXPORT_LIGRA_WEIGHT  <p>.ligra.weight  (tools/bin2ligraweight.cpp:66-120)
+ *   SCAPH_EXPORT_TOTEM         <p>.totem         (tools/bin2totem.cpp:66-110)
+ *   SCAPH_EXPORT_TOTEM_WEIGHT  <p>weight.totem   (tools/bin2totemweight.cpp:66-117) */
+#define SCAPH_EXPORT_LIGRA         1
+#define SCAPH_EXPORT_LIGRA_WEIGHT  2
+#define SCAPH_EXPORT_TOTEM         3
+#define SCAPH_EXPORT_TOTEM_WEIGHT  4
+int scaph_csr_export(const char *prefix, int kind);
+
 /* Reverse every edge (in-edge CSR for pull on directed graphs). */
 int scaph_csr_transpose(const scaph_csr *in, scaph_csr *out);
 /* Copies caller arrays into a library-owned CSR. */

@@ -5,9 +5,10 @@ legs, as the checker.  The engine (scaph_b200) never imports this module.
 
 * liboracle.so      - bfs_oracle.c, the C restatement of the reference's
                       CPU BFS (app/bfs.cu:70-101) and helpers.
-* _ref/libscaphref.so, _ref/pagegencsr - the reference's own code compiled
-                      from its sources by oracle/Makefile (only present where
-                      the reference tree was available at build time).
+* _ref/libscaphref.so, _ref/pagegencsr, _ref/bin2ligra, _ref/bin2ligraweight,
+  _ref/bin2totem    - the reference's own code compiled from its sources by
+                      oracle/Makefile (only present where the reference tree
+                      was available at build time).
 """
 from __future__ import annotations
 
@@ -20,6 +21,10 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "liboracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libscaphref.so")
 REF_PAGEGEN = os.path.join(HERE, "_ref", "pagegencsr")
+# the reference's CSR -> text converters (tools/bin2ligra.cpp, bin2ligraweight.cpp,
+# bin2totem.cpp); bin2totemweight.cpp is not built: it reads E weights into a
+# buffer of V+1 words (tools/bin2totemweight.cpp:94-96)
+REF_EXPORTERS = {k: os.path.join(HERE, "_ref", k) for k in ("bin2ligra", "bin2ligraweight", "bin2totem")}
 
 _o = None
 _r = None
@@ -195,3 +200,33 @@ def min_reaching_id(idx, ngh) -> np.ndarray:
     if olib().oracle_min_reaching_id(len(idx) - 1, _p(idx), _p(ngh), _p(out)) != 0:
         raise ValueError("oracle_min_reaching_id failed")
     return out
+
+
+def export_text(idx32, ngh, wgh, kind: str) -> bytes:
+    """The reference converters' text formats, restated (small graphs only):
+    "ligra" / "ligra.weight" (tools/bin2ligra.cpp:92-104,
+    tools/bin2ligraweight.cpp:99-115): a header line, V, E, then the V
+    offsets idx[0..V-1], the E neighbours (and the E weights), one per line;
+    "totem" / "weight.totem" (tools/bin2totem.cpp:92-104,
+    tools/bin2totemweight.cpp:99-111): "#Nodes: V", "#Edges: E",
+    "#Undirected", then one "src<TAB>dst[<TAB>weight]" line per edge."""
+    V, E = len(idx32) - 1, len(ngh)
+    if wgh is None:  # the weight file of an unweighted graph holds zeros
+        wgh = np.zeros(E, np.uint32)
+    lines = []
+    if kind in ("ligra", "ligra.weight"):
+        lines.append("WeightedAdjacencyGraph" if kind == "ligra.weight" else "AdjacencyGraph")
+        lines += [str(V), str(E)]
+        lines += [str(int(x)) for x in idx32[:V]]
+        lines += [str(int(x)) for x in ngh]
+        if kind == "ligra.weight":
+            lines += [str(int(x)) for x in wgh]
+    else:
+        lines += [f"#Nodes: {V}", f"#Edges: {E}", "#Undirected"]
+        for v in range(V):
+            for e in range(int(idx32[v]), int(idx32[v + 1])):
+                if kind == "weight.totem":
+                    lines.append(f"{v}\t{int(ngh[e])}\t{int(wgh[e])}")
+                else:
+                    lines.append(f"{v}\t{int(ngh[e])}")
+    return ("\n".join(lines) + "\n").encode()

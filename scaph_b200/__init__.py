@@ -23,6 +23,10 @@ OK, EINVAL, EIO, ENOMEM, ECUDA, EFORMAT, ETIMEOUT, EUNSUPPORTED, EDEVICE = 0, -1
 DIR_ALPHABETA, DIR_PUSH, DIR_PULL, DIR_LEARNED = 0, 1, 2, 3
 UNREACHED = 0xFFFFFFFF
 REF_UNREACHED = 63  # MAXDEPTH of the reference BFS app (app/bfs.cu:18)
+# text exports of <prefix>_csr.* (scaph_csr_export): kind -> file written
+EXPORT_LIGRA, EXPORT_LIGRA_WEIGHT, EXPORT_TOTEM, EXPORT_TOTEM_WEIGHT = 1, 2, 3, 4
+EXPORT_SUFFIX = {EXPORT_LIGRA: ".ligra", EXPORT_LIGRA_WEIGHT: ".ligra.weight", EXPORT_TOTEM: ".totem",
+                 EXPORT_TOTEM_WEIGHT: "weight.totem"}
 
 
 class ScaphError(RuntimeError):
@@ -98,6 +102,7 @@ def lib() -> C.CDLL:
         "scaph_csr_write": ([C.c_char_p, P(_Csr)], i32),
         "scaph_csr_read": ([C.c_char_p, i32, P(_Csr)], i32),
         "scaph_pages_write": ([C.c_char_p, P(_Csr), u32, i32], i32),
+        "scaph_csr_export": ([C.c_char_p, i32], i32),
         "scaph_graph_open": ([C.c_char_p, i32, P(vp)], i32),
         "scaph_graph_from_csr": ([P(_Csr), u32, i32, P(vp)], i32),
         "scaph_graph_get_info": ([vp, P(_GraphInfo)], i32),
@@ -280,6 +285,14 @@ class Csr:
 
     def write_pages(self, prefix: str, pagesize_words: int, weighted: bool = False) -> None:
         _check(lib().scaph_pages_write(prefix.encode(), C.byref(self._c), pagesize_words, int(weighted)))
+
+
+def csr_export(prefix: str, kind: int) -> str:
+    """Writes the text export `kind` (EXPORT_*) of the flat CSR files
+    <prefix>_csr.* - what tools/bin2ligra, bin2ligraweight, bin2totem and
+    bin2totemweight write - and returns the path written."""
+    _check(lib().scaph_csr_export(prefix.encode(), kind))
+    return prefix + EXPORT_SUFFIX[kind]
 
 
 # ---------------------------------------------------------------------------
