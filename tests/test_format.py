@@ -46,6 +46,34 @@ def test_writer_byte_identical_to_pagegencsr_live(tmp_path, scale, ef, seed):
     assert da == db and len(da) >= 3
 
 
+def test_weighted_writer_byte_identical_to_pagegencsr_golden(tmp_path):
+    """{ngr, wgh} pages: scaph_pages_write(weighted) == the digests of the
+    files tools/pagegencsr.cpp writes with its `w` flag."""
+    import tests.golden.make_weighted_pages_golden as mk
+
+    meta = json.load(open(os.path.join(GOLD, "pagegencsr_weighted_digests.json")))
+    csr = mk.graph()
+    assert (csr.V, csr.E) == (meta["V"], meta["E"])
+    csr.write_pages(str(tmp_path / "g"), meta["pagesize_mb"] << 20, weighted=True)
+    assert _digests(tmp_path) == meta["files"]
+
+
+@pytest.mark.skipif(not os.path.exists(O.REF_PAGEGEN), reason="oracle/_ref/pagegencsr not built")
+@pytest.mark.parametrize("scale,ef,seed", [(14, 8, 1), (12, 32, 2), (16, 16, 3)])
+def test_weighted_writer_byte_identical_to_pagegencsr_live(tmp_path, scale, ef, seed):
+    c = S.Csr.rmat(scale, ef, seed=seed)
+    w = np.random.default_rng(seed).integers(1, 1 << 20, c.E).astype(np.uint32)
+    csr = S.Csr.from_arrays(c.idx, c.ngh, w)
+    a, b = tmp_path / "a", tmp_path / "b"
+    a.mkdir()
+    b.mkdir()
+    csr.write(str(b / "g"))
+    subprocess.run([O.REF_PAGEGEN, str(b / "g"), "1", "w"], check=True, capture_output=True)
+    csr.write_pages(str(a / "g"), 1 << 20, weighted=True)
+    da, db = _digests(a), _digests(b)
+    assert da == db and len(da) >= 3
+
+
 def test_open_roundtrip_and_degrees(tmp_path):
     csr = S.Csr.rmat(13, 16, seed=G.SEED + 60)
     p = str(tmp_path / "g")
