@@ -74,6 +74,27 @@ def test_weighted_writer_byte_identical_to_pagegencsr_live(tmp_path, scale, ef, 
     assert da == db and len(da) >= 3
 
 
+@pytest.mark.skipif(not os.path.exists(O.REF_PAGEGEN), reason="oracle/_ref/pagegencsr not built")
+@pytest.mark.parametrize("weighted", [False, True])
+def test_reader_opens_reference_written_pages(tmp_path, weighted):
+    """scaph_graph_open on the files tools/pagegencsr.cpp itself wrote reads
+    back the CSR they came from (degrees, adjacency, weights)."""
+    c = S.Csr.rmat(17, 16, seed=G.SEED + 152)  # ~2M edges: several 1 Mi-word pages
+    if weighted:
+        w = np.random.default_rng(153).integers(1, 1000, c.E).astype(np.uint32)
+        c = S.Csr.from_arrays(c.idx, c.ngh, w)
+    p = str(tmp_path / "g")
+    c.write(p)
+    subprocess.run([O.REF_PAGEGEN, p, "1", "w" if weighted else "u"], check=True, capture_output=True)
+    g = S.PagedGraph.open(p, weighted=weighted)
+    assert (g.V, g.E) == (c.V, c.E) and g.npages >= 2
+    assert np.array_equal(g.degree(), c.degree())
+    back = g.to_csr()
+    assert np.array_equal(back.idx, c.idx) and np.array_equal(back.ngh, c.ngh)
+    if weighted:
+        assert np.array_equal(back.wgh, c.wgh)
+
+
 def test_open_roundtrip_and_degrees(tmp_path):
     csr = S.Csr.rmat(13, 16, seed=G.SEED + 60)
     p = str(tmp_path / "g")
