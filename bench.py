@@ -35,6 +35,7 @@ sys.path.insert(0, ROOT)
 METRIC = "BFS GTEPS (edge_count / traversal time), plain direction-optimizing engine, RMAT-24 in HBM"
 PEAKS_FILE = os.path.join(ROOT, "MEASURED_PEAKS.json")
 FALLBACK_HBM_GBS = 6650.0
+NOMINAL_HBM_GBS = 8000.0
 
 
 # Measured DRAM bytes (read + write) per k_pull launch on RMAT-24: ncu's dram__bytes_read.sum
@@ -601,6 +602,7 @@ def run_ours(args, world):
     roof = {"bound": "hbm", "kernel": "k_pull" if dom == 1 else "k_push(+k_push_giant)",
             "achieved": achieved, "peak": peak, "unit": "GB/s",
             "frac": achieved / peak if achieved else None, "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)",
+            "frac_of_nominal": achieved / NOMINAL_HBM_GBS if achieved else None,  # B200 HBM3e, 8 TB/s
             # DRAM read+write per k_pull launch, ncu over every k_pull launch of the same
             # command with --host-loop (K_PULL_TRAFFIC_BYTES)
             "traffic": K_PULL_TRAFFIC_BYTES if dom == 1 and args.scale == 24 else None,
