@@ -23,6 +23,8 @@ and prefetches pages, the depths never change.
 """
 from __future__ import annotations
 
+import time
+
 from dataclasses import dataclass
 
 import numpy as np
@@ -236,11 +238,19 @@ def train(traces, g: PagedGraph, gt: PagedGraph | None, nslots: int, page_ms: fl
                       page_words=g.pagesize)
     net = Mlp(G + n_out, 1 + n_out, seed=seed, device=device)
     loss0, _ = net.loss_grad(X, T, W)
-    loss = net.train(X, T, W, epochs=epochs, batch=min(256, len(X)), lr=lr, seed=seed)
+    batch = min(256, len(X))
+    t0 = time.perf_counter()
+    loss = net.train(X, T, W, epochs=epochs, batch=batch, lr=lr, seed=seed)
+    t1 = time.perf_counter()
     Y = net.forward(X)
+    t2 = time.perf_counter()
     m = W[:, 0] > 0
     acc = float(((Y[m, 0] > 0) == (T[m, 0] > 0.5)).mean()) if m.any() else 1.0
-    return net, {"rows": int(len(X)), "loss0": loss0, "loss": loss, "direction_accuracy": acc}
+    steps = epochs * -(-len(X) // batch)
+    # host wall clock around calls that return results to the host
+    return net, {"rows": int(len(X)), "loss0": loss0, "loss": loss, "direction_accuracy": acc,
+                 "train_us_per_step": (t1 - t0) * 1e6 / max(1, steps), "train_steps": steps, "batch": batch,
+                 "forward_us_per_call": (t2 - t1) * 1e6}
 
 
 def evaluate(g: PagedGraph, gt: PagedGraph | None, sources, net: Mlp | None, pool_bytes: int, cold=True,
