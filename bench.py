@@ -618,6 +618,10 @@ def run_ours(args, world):
             "achieved": achieved, "peak": peak, "unit": "GB/s",
             "frac": achieved / peak if achieved else None, "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)",
             "frac_of_nominal": achieved / NOMINAL_HBM_GBS if achieved else None,  # B200 HBM3e, 8 TB/s
+            "alg_bytes_rule": "push: 12 B per frontier vertex + 4 B per edge; pull: 12 B per unvisited vertex + "
+                              "4 B per in-edge inspected; each level V/8 B of bitmap + 4 B per discovered vertex; "
+                              "frontier/visited probes not counted (bitmaps of %.1f MB, L2-resident)"
+                              % (csr.V / 8 / 1e6),
             # DRAM read+write per k_pull launch, ncu over every k_pull launch of the same
             # command with --host-loop (K_PULL_TRAFFIC_BYTES)
             "traffic": K_PULL_TRAFFIC_BYTES if dom == 1 and args.scale == 24 else None,
