@@ -463,19 +463,28 @@ int scaph_store_counters(const scaph_store *s, uint64_t *h2d_bytes, uint64_t *zc
  *   d_page   16-byte aligned, at least round_up(3*nodenum + edgenum, 4) words
  *   limits   nodenum <= SCAPH_NOALLOC_MAX_V, edgenum <= SCAPH_NOALLOC_MAX_E,
  *            larger inputs return SCAPH_EINVAL before any GPU work
- * Its scratch state is a fixed ~1.3 MB __device__ array inside the library,
- * held on every GPU that loads it until the process exits.  All calls share
- * it and leave their contents in it; each call clears what it needs, but
- * calls whose GPU work overlaps race on it.  The first call on a device
- * looks up the array's address (cudaGetSymbolAddress, with that device
- * current); make that first call before any stream capture.  The call
- * synchronises `stream` (a cudaStream_t; NULL = default stream) once per
- * level. */
+ *   flags    SCAPH_NOALLOC_SYMMETRIC: every edge of the page has its reverse,
+ *            so pull levels may read the page as in-edges and the alpha/beta
+ *            switch is used; without it every level pushes (right for
+ *            directed pages)
+ *   unreached  depth of unreached vertices; 0 = 0xFFFFFFFF, 1 is rejected
+ *   stats    NULL, or the run's levels, push/pull level counts, reached
+ *            vertices and edges, edges inspected and kernel launches
+ * A page whose Node records do not fit nodenum/edgenum returns SCAPH_EFORMAT
+ * before any traversal.  There is no level cap: paths up to nodenum deep
+ * get their exact depths.  Its scratch state is a fixed ~1.3 MB __device__
+ * array inside the library, held on every GPU that loads it until the
+ * process exits.  All calls share it and leave their contents in it; each
+ * call clears what it needs, but calls whose GPU work overlaps race on it.
+ * Each call looks up the array's address (cudaGetSymbolAddress, current
+ * device) and synchronises `stream` (a cudaStream_t; NULL = default stream)
+ * once per level. */
 #define SCAPH_NOALLOC_MAX_V (1u << 18)
 #define SCAPH_NOALLOC_MAX_E (1u << 22)
+#define SCAPH_NOALLOC_SYMMETRIC 1
 int scaph_bfs_page_noalloc(const uint32_t *d_page, uint32_t nodenum, uint32_t edgenum,
-                           uint32_t src, uint32_t unreached, uint32_t *d_depth,
-                           uint32_t *d_parent, void *stream);
+                           uint32_t src, uint32_t unreached, int flags, uint32_t *d_depth,
+                           uint32_t *d_parent, scaph_bfs_stats *stats, void *stream);
 
 /* ---- host helpers ------------------------------------------------------ */
 

@@ -23,6 +23,7 @@ OK, EINVAL, EIO, ENOMEM, ECUDA, EFORMAT, ETIMEOUT, EUNSUPPORTED, EDEVICE = 0, -1
 DIR_ALPHABETA, DIR_PUSH, DIR_PULL, DIR_LEARNED = 0, 1, 2, 3
 UNREACHED = 0xFFFFFFFF
 REF_UNREACHED = 63  # MAXDEPTH of the reference BFS app (app/bfs.cu:18)
+NOALLOC_SYMMETRIC = 1  # scaph_bfs_page_noalloc: the page is symmetric, pull levels allowed
 # text exports of <prefix>_csr.* (scaph_csr_export): kind -> file written
 EXPORT_LIGRA, EXPORT_LIGRA_WEIGHT, EXPORT_TOTEM, EXPORT_TOTEM_WEIGHT = 1, 2, 3, 4
 EXPORT_SUFFIX = {EXPORT_LIGRA: ".ligra", EXPORT_LIGRA_WEIGHT: ".ligra.weight", EXPORT_TOTEM: ".totem",

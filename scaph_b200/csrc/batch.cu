@@ -788,9 +788,14 @@ int scaph_batch_run(scaph_batch *b, const scaph_query *q, int nq, uint32_t *dept
     c0.mode = e->cfg.direction == SCAPH_DIR_PUSH ? 1 : e->cfg.direction == SCAPH_DIR_PULL ? 2 : 0;
     c0.alpha = b->params.alpha;
     c0.beta = b->params.beta;
+    // the level cap comes from the depth planes, or from the sentinel (the
+    // loop assigns depths below `unreached` only); stopping at the
+    // sentinel's cap is the traversal's end, not an overflow
+    bool unr_bound = false;
     for (int attempt = 0; attempt < 3; attempt++) {
         c0.max_level = std::min<uint32_t>((1u << b->nplanes) - 1, kMaxLevels);
-        if ((uint64_t)c0.max_level + 1 > e->unreached) c0.max_level = e->unreached - 1;
+        unr_bound = (uint64_t)c0.max_level + 1 > e->unreached;
+        if (unr_bound) c0.max_level = e->unreached - 1;
         // the graph bakes in pointers, sizes and the start state: rebuild
         // when any of them changed
         if (!b->gexec || b->g_nw != b->nw || b->g_block != b->params.block_size || b->g_ctas != b->params.ctas_per_sm ||
@@ -813,13 +818,13 @@ int scaph_batch_run(scaph_batch *b, const scaph_query *q, int nq, uint32_t *dept
         SCAPH_CUDA(cudaEventRecord(e->ev_stop, st));
         SCAPH_CUDA(cudaMemcpyAsync(b->h_ctl, b->d_ctl, sizeof(BatchCtl), cudaMemcpyDeviceToHost, st));
         SCAPH_CUDA(cudaStreamSynchronize(st));
-        if (!b->h_ctl->overflow) break;
+        if (!b->h_ctl->overflow || unr_bound) break;
         // deeper than the planes can hold: more planes, run again
         b->nplanes = std::min(kMsPlanes, b->nplanes + 3);
         b->drop_graph();
     }
     const BatchCtl &c = *b->h_ctl;
-    if (c.overflow) return set_error(SCAPH_EUNSUPPORTED, "traversal deeper than %d levels", (1 << kMsPlanes) - 1);
+    if (c.overflow && !unr_bound) return set_error(SCAPH_EUNSUPPORTED, "traversal deeper than %d levels", (1 << kMsPlanes) - 1);
     if (c.err) return set_error(SCAPH_EDEVICE, "batch kernels reported error flags 0x%x", c.err);
     const int levels = (int)c.level;
     b->trace.clear();

@@ -598,6 +598,8 @@ int scaph_engine::run_host_loop(uint32_t src, uint32_t *dd, uint32_t *dp)
         level++;
     }
     last_levels = level;
+    if (nf > 0 && level == kMaxLevels && (uint64_t)level + 1 < unreached)
+        return set_error(SCAPH_EUNSUPPORTED, "traversal deeper than %d levels", kMaxLevels);
     return SCAPH_OK;
 }
 
@@ -806,6 +808,10 @@ int scaph_engine::collect(bool from_graph)
     }
     pending = false;
     if (err) return set_error(SCAPH_EDEVICE, "level kernel reported error flags 0x%x", err);
+    // the level loop stops at kMaxLevels (the per-level counter records);
+    // a frontier still left there means deeper vertices were not reached
+    if (last_levels == kMaxLevels && nf > 0 && (uint64_t)last_levels + 1 < unreached)
+        return set_error(SCAPH_EUNSUPPORTED, "traversal deeper than %d levels", kMaxLevels);
     return SCAPH_OK;
 }
 

@@ -362,6 +362,8 @@ static int ms_run(scaph_engine *e, const uint32_t *srcs, int nsrc, uint32_t *out
         stats->launches = launches;
     }
     if (err) return set_error(SCAPH_EDEVICE, "multi-source kernels reported error flags 0x%x", err);
+    if (nf > 0 && level == kMaxLevels && (uint64_t)level + 1 < e->unreached)
+        return set_error(SCAPH_EUNSUPPORTED, "traversal deeper than %d levels", kMaxLevels);
     return SCAPH_OK;
 }
 

@@ -20,13 +20,16 @@
 //    call clears what must start at zero, but calls whose GPU work overlaps
 //    (on different streams, or from different host threads) race on it and
 //    give wrong results: serialise them;
-//  * the device address of the array is looked up with cudaGetSymbolAddress
-//    the first time the entry point runs on a device (with that device
-//    current); make that first call before any stream capture.
+//  * pull levels read the same page as in-edges, which is right only when
+//    every edge has its reverse: the caller says so with
+//    SCAPH_NOALLOC_SYMMETRIC, otherwise every level pushes;
+//  * every call looks up the device address of the array with
+//    cudaGetSymbolAddress (current device), so nothing is cached across a
+//    device reset; the call synchronises its stream once per level.
 #include <cuda_runtime.h>
 
 #include <algorithm>
-#include <mutex>
+#include <cstring>
 
 #include "engine.h"
 #include "kernels.h"
@@ -39,7 +42,6 @@ constexpr uint32_t kMaxV = SCAPH_NOALLOC_MAX_V;
 constexpr uint32_t kMaxE = SCAPH_NOALLOC_MAX_E;
 constexpr uint32_t kWords = kMaxV / 32;
 constexpr uint32_t kGiantCap = 2 * (kMaxE / kGiantEdges) + 1024;
-constexpr int kMaxDevices = 64;
 constexpr uint32_t kCshift = 18;  // kMaxV = 1 << 18: every vertex maps to coarse[0]
 static_assert((1u << kCshift) >= kMaxV, "coarse shift must cover kMaxV");
 
@@ -85,31 +87,24 @@ __global__ void k_noalloc_setup(unsigned char *scratch, const uint32_t *page, ui
     }
 }
 
-std::mutex g_mu;
-void *g_scratch_addr[kMaxDevices] = {};
-
-// Device address of g_noalloc_scratch on the current device (looked up once).
+// Device address of g_noalloc_scratch on the current device.  Looked up on
+// every call: the lookup is cheap next to the per-level synchronisation, and
+// an address cached across a cudaDeviceReset would be stale.
 int scratch_address(unsigned char **out)
 {
-    int dev = 0;
-    SCAPH_CUDA(cudaGetDevice(&dev));
-    if (dev < 0 || dev >= kMaxDevices) return set_error(SCAPH_EUNSUPPORTED, "device %d beyond %d", dev, kMaxDevices);
-    std::lock_guard<std::mutex> lock(g_mu);
-    if (!g_scratch_addr[dev]) {
-        void *p = nullptr;
-        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-        if (e != cudaSuccess || !p)
-            return set_error(SCAPH_ECUDA, "cudaGetSymbolAddress(g_noalloc_scratch): %s", cudaGetErrorString(e));
-        g_scratch_addr[dev] = p;
-    }
-    *out = static_cast<unsigned char *>(g_scratch_addr[dev]);
+    void *p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || !p)
+        return set_error(SCAPH_ECUDA, "cudaGetSymbolAddress(g_noalloc_scratch): %s", cudaGetErrorString(e));
+    *out = static_cast<unsigned char *>(p);
     return SCAPH_OK;
 }
 
 }  // namespace
 
 extern "C" int scaph_bfs_page_noalloc(const uint32_t *d_page, uint32_t nodenum, uint32_t edgenum, uint32_t src,
-                                      uint32_t unreached, uint32_t *d_depth, uint32_t *d_parent, void *stream)
+                                      uint32_t unreached, int flags, uint32_t *d_depth, uint32_t *d_parent,
+                                      scaph_bfs_stats *stats, void *stream)
 {
     clear_error();
     if (!d_page || !d_depth) return set_error(SCAPH_EINVAL, "null page or depth pointer");
@@ -118,7 +113,10 @@ extern "C" int scaph_bfs_page_noalloc(const uint32_t *d_page, uint32_t nodenum, 
         return set_error(SCAPH_EINVAL, "nodenum %u outside 1..%u (SCAPH_NOALLOC_MAX_V)", nodenum, kMaxV);
     if (edgenum > kMaxE) return set_error(SCAPH_EINVAL, "edgenum %u above %u (SCAPH_NOALLOC_MAX_E)", edgenum, kMaxE);
     if (src >= nodenum) return set_error(SCAPH_EINVAL, "source %u out of range (V=%u)", src, nodenum);
+    if (flags & ~SCAPH_NOALLOC_SYMMETRIC) return set_error(SCAPH_EINVAL, "unknown flags 0x%x", flags);
     if (unreached == 0) unreached = 0xFFFFFFFFu;
+    if (unreached < 2) return set_error(SCAPH_EINVAL, "unreached sentinel must be >= 2");
+    const bool symmetric = (flags & SCAPH_NOALLOC_SYMMETRIC) != 0;
     unsigned char *scr = nullptr;
     int rc = scratch_address(&scr);
     if (rc) return rc;
@@ -177,10 +175,13 @@ extern "C" int scaph_bfs_page_noalloc(const uint32_t *d_page, uint32_t nodenum, 
     uint32_t deg_src = 0;
     SCAPH_CUDA(cudaMemcpyAsync(&deg_src, s.degree + src, 4, cudaMemcpyDeviceToHost, st));
     SCAPH_CUDA(cudaStreamSynchronize(st));
-    uint64_t nf = 1, prev_nf = 0, mf = deg_src, vis_e = deg_src;
-    int dir = 0, cur = 0;
-    for (int level = 0; nf > 0 && level < kMaxLevels && (uint64_t)level + 1 < unreached; level++) {
-        if (level > 0) dir = alpha_beta_next(dir, nf, prev_nf, mf, E - vis_e, V, 14.0f, 24.0f);
+    uint64_t nf = 1, prev_nf = 0, mf = deg_src, vis_n = 1, vis_e = deg_src, inspected = 0;
+    int dir = 0, cur = 0, level = 0, npush = 0, npull = 0;
+    // no level cap beyond the sentinel's: the level counters are one record
+    // reused every level, and the loop ends once a level discovers nothing
+    // (at most V levels)
+    for (; nf > 0 && (uint64_t)level + 1 < unreached; level++) {
+        if (level > 0 && symmetric) dir = alpha_beta_next(dir, nf, prev_nf, mf, E - vis_e, V, 14.0f, 24.0f);
         SCAPH_CUDA(cudaMemsetAsync(ctr, 0, sizeof(LevelCounters), st));
         SCAPH_CUDA(cudaMemsetAsync(bm[cur ^ 1], 0, (size_t)nwords * 4, st));
         s.front = bm[cur];
@@ -191,11 +192,24 @@ extern "C" int scaph_bfs_page_noalloc(const uint32_t *d_page, uint32_t nodenum, 
         SCAPH_CUDA(cudaMemcpyAsync(&lc, ctr, sizeof(lc), cudaMemcpyDeviceToHost, st));
         SCAPH_CUDA(cudaStreamSynchronize(st));
         if (lc.error) return set_error(SCAPH_EDEVICE, "level kernel reported error flags 0x%x", lc.error);
+        if (dir == 0) npush++; else npull++;
+        inspected += lc.inspected;
         prev_nf = nf;
         nf = lc.next;
         mf = lc.next_edges;
+        vis_n += nf;
         vis_e += mf;
         cur ^= 1;
+    }
+    if (stats) {
+        memset(stats, 0, sizeof(*stats));
+        stats->levels = level;
+        stats->push_levels = npush;
+        stats->pull_levels = npull;
+        stats->reached = vis_n;
+        stats->reached_edges = vis_e;
+        stats->edges_inspected = inspected;
+        stats->launches = 3 + (d_parent ? 1 : 0) + (uint64_t)npush * 2 + npull;
     }
     return SCAPH_OK;
 }

@@ -143,6 +143,26 @@ def test_deep_path_and_cap(use_graph):
     assert d.max() == 63 and (d == 62).sum() == 1
 
 
+@pytest.mark.parametrize("use_graph", [0, 2], ids=["graph", "hostloop"])
+def test_deeper_than_level_cap_is_an_error(use_graph):
+    """The engine's level loop keeps one counter record per level (4096): a
+    path longer than that returns SCAPH_EUNSUPPORTED instead of depths with
+    the far end left unreached; the multi-source loop does the same."""
+    csr = G.path(4200)
+    g = S.PagedGraph.from_csr(csr, pagesize_words=1 << 15)
+    eng = S.Engine(g, direction=S.DIR_PUSH, use_graph=use_graph)
+    with pytest.raises(S.ScaphError) as ex:
+        eng.bfs(0)
+    assert ex.value.code == S.EUNSUPPORTED and "deeper than 4096" in str(ex.value)
+    # from the middle the traversal is 2100 levels deep: exact
+    d, _, st = eng.bfs(2100)
+    assert np.array_equal(d, O.bfs(csr.idx, csr.ngh, 2100)) and st.levels == 2100
+    with pytest.raises(S.ScaphError) as ex:
+        eng.msbfs([0, 5])
+    assert ex.value.code == S.EUNSUPPORTED
+    eng.close()
+
+
 def test_isolated_source_and_ragged_V():
     csr = G.random_graph(1001, 900, seed=3)  # V not a multiple of 32, isolated vertices
     g = S.PagedGraph.from_csr(csr, pagesize_words=512)
