@@ -130,14 +130,33 @@ def gpu_index(local_rank: int) -> int:
     return local_rank
 
 
-def config_dict(csr, scale, nsrc, extra=None):
-    d = {"workload": f"rmat{scale}-ef16 single-source BFS, {nsrc} seeded sources, alpha/beta 14/24, in HBM",
-         "graph": f"RMAT scale {scale}, ef 16, a/b/c/d .57/.19/.19/.05, symmetrised, dedup",
-         "V": csr.V, "E": csr.E, "sources": nsrc, "pagesize_words": 10 * 1024 * 1024,
-         "l2": "inputs larger than L2 (paged graph %.2f GB > 126 MB)" % (4 * (3 * csr.V + csr.E) / 1e9)}
-    if extra:
-        d.update(extra)
-    return d
+def config_dict(V, E, scale, nsrc):
+    """The workload's description; identical in both arms."""
+    return {"workload": f"rmat{scale}-ef16 single-source BFS, {nsrc} seeded sources, alpha/beta 14/24, in HBM",
+            "graph": f"RMAT scale {scale}, ef 16, a/b/c/d .57/.19/.19/.05, symmetrised, dedup",
+            "V": V, "E": E, "sources": nsrc, "pagesize_words": 10 * 1024 * 1024,
+            "l2": "inputs larger than L2 (paged graph %.2f GB > 126 MB)" % (4 * (3 * V + E) / 1e9)}
+
+
+# ---------------------------------------------------------------------------
+# the checker: depths against the CPU oracle (outside every timed region)
+# ---------------------------------------------------------------------------
+def oracle_check(idx, ngh, runs, unreached=0xFFFFFFFF, threads=0):
+    """runs: (source, uint32 depth array) pairs.  Each is compared bit for bit
+    with the level-synchronous restatement of bfs::check (app/bfs.cu:70-101)
+    run with OpenMP on the host cores."""
+    import numpy as np
+
+    from oracle import oracle as O
+
+    n, bad, t0 = 0, [], time.perf_counter()
+    for src, depth in runs:
+        ref = O.bfs_omp(idx, ngh, int(src), unreached, threads)
+        n += 1
+        if not np.array_equal(np.asarray(depth).view(np.uint32), ref):
+            bad.append(int(src))
+    return {"bit_exact_vs_oracle": n > 0 and not bad, "checked": n, "mismatched_sources": bad[:8],
+            "oracle": "level-synchronous bfs::check restatement, OpenMP", "check_s": round(time.perf_counter() - t0, 1)}
 
 
 # ---------------------------------------------------------------------------
@@ -167,24 +186,41 @@ def _ref_worker_bfs(src):
     return time.perf_counter() - t
 
 
+def rmat24_for_reference(scale, nsrc):
+    """The headline graph and sources, built without the product library:
+    the oracle's RMAT generator (identical CSR to scaph_gen_rmat, checked by
+    a CPU test) and the same seeded choice of sources as
+    scaph_b200.workloads.config2."""
+    import numpy as np
+
+    from oracle import oracle as O
+
+    seed = 0x5CA90000 + 1
+    idx, ngh = O.gen_rmat(scale, 16, 0.57, 0.19, 0.19, seed, True)
+    cand = np.flatnonzero(np.diff(idx) > 0)
+    rng = np.random.default_rng(seed)
+    srcs = [int(x) for x in rng.choice(cand, size=min(nsrc, len(cand)), replace=False)]
+    return idx, ngh, srcs
+
+
 def run_reference(args, world):
     import multiprocessing as mp
 
     import numpy as np
 
     from oracle import oracle as O
-    from scaph_b200 import workloads
 
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    csr, srcs = workloads.config2(args.scale, args.sources)
+    idx, ngh, srcs = rmat24_for_reference(args.scale, args.sources)
+    V, E = len(idx) - 1, len(ngh)
     kind = "reference" if O.ref_available() else "port"
     tmp = tempfile.mkdtemp(dir="/dev/shm" if os.path.isdir("/dev/shm") else None)
     idx_path, ngh_path = os.path.join(tmp, "idx.npy"), os.path.join(tmp, "ngh.npy")
-    np.save(idx_path, csr.idx.astype(np.uint32))
-    np.save(ngh_path, csr.ngh)
-    E = csr.E
+    np.save(idx_path, idx.astype(np.uint32))
+    np.save(ngh_path, ngh)
+    del idx, ngh
     cores = os.cpu_count() or 1
     ctx = mp.get_context("spawn")
     with ctx.Pool(cores, initializer=_ref_worker_init, initargs=(idx_path, ngh_path)) as pool:
@@ -202,7 +238,7 @@ def run_reference(args, world):
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "GTEPS", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * wall / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
-            "data": "synthetic (seeded RMAT)", "config": config_dict(csr, args.scale, len(srcs)),
+            "data": "synthetic (seeded RMAT)", "config": config_dict(V, E, args.scale, len(srcs)),
             "cpu_baseline": {"value": value, "unit": "GTEPS", "cores": cores, "kind": kind, "sample": sample},
             "e2e": {"value": value, "unit": "GTEPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -302,7 +338,9 @@ def extra_config4a(stream):
     ms_plain = e0.elapsed_time(e1)
     eng.close()
     n = len(srcs)
-    return {"graph": "RMAT-25 ef16", "V": csr.V, "E": csr.E, "sources_per_launch": n,
+    # every row of the batched launch against the CPU oracle (untimed)
+    parity = oracle_check(csr.idx, csr.ngh, ((s, out[i].cpu().numpy()) for i, s in enumerate(srcs)))
+    return {"graph": "RMAT-25 ef16", "V": csr.V, "E": csr.E, "sources_per_launch": n, "parity": parity,
             "batched_ms": ms_batch, "batched_gteps_per_source": n * csr.E / (ms_batch / 1e3) / 1e9,
             "plain_ms_for_same_sources": ms_plain, "plain_gteps": n * csr.E / (ms_plain / 1e3) / 1e9,
             "speedup_vs_plain": ms_plain / ms_batch, "levels": len(tr),
@@ -349,6 +387,16 @@ def extra_config4b(stream):
     torch.cuda.synchronize()
     ms_plain = e0.elapsed_time(e1)
     exact = bool(torch.equal(out, ref))
+    # every query's row against the CPU oracle on its own graph (untimed)
+    host = out.cpu().numpy()
+    parity = {"checked": 0, "mismatched_sources": [], "check_s": 0.0}
+    for (gi, src), off in zip(queries, offs):
+        r = oracle_check(graphs[gi].idx, graphs[gi].ngh, [(src, host[off:off + graphs[gi].V])])
+        parity["checked"] += r["checked"]
+        parity["check_s"] += r["check_s"]
+        if r["mismatched_sources"]:
+            parity["mismatched_sources"].append([gi, src])
+    parity["bit_exact_vs_oracle"] = parity["checked"] == len(queries) and not parity["mismatched_sources"]
     for e in engines:
         e.close()
     b.close()
@@ -360,14 +408,24 @@ def extra_config4b(stream):
             "graph_gen_s": round(gen_s, 1), "launches_per_batch": runs[-1].launches,
             "batched_ms": ms_batch, "batched_gteps": teps / (ms_batch / 1e3) / 1e9,
             "plain_ms": ms_plain, "plain_gteps": teps / (ms_plain / 1e3) / 1e9,
-            "speedup_vs_plain": ms_plain / ms_batch, "bit_exact_vs_plain": exact, "levels": len(tr),
+            "speedup_vs_plain": ms_plain / ms_batch, "bit_exact_vs_plain": exact, "parity": parity,
+            "levels": len(tr),
             "directions": "".join("p" if t["direction"] else "P" for t in tr),
             "autotune": {"params": tune["params"], "default_ms": tune["default_ms"], "tuned_ms": tune["ms"],
                          "candidates": tune["tried"], "seconds": round(tune["seconds"], 1)}}
 
 
-def _run_set(S, g, gt, srcs, pool, net=None, cold=False, warm_pass=True, **kw):
-    """Times `srcs`; returns total ms, PCIe bytes, levels."""
+def _digest(a):
+    import hashlib
+
+    import numpy as np
+
+    return hashlib.blake2b(memoryview(np.ascontiguousarray(a)), digest_size=16).hexdigest()
+
+
+def _run_set(S, g, gt, srcs, pool, net=None, cold=False, warm_pass=True, digests=None, **kw):
+    """Times `srcs`; returns total ms, PCIe bytes, levels.  With `digests`
+    (source -> list), a digest of every checked source's depths is added."""
     eng = S.Engine(g, gt, pool_bytes=pool, direction=S.DIR_LEARNED if net else 0, **kw)
     if net:
         eng.set_scheduler(net)
@@ -378,20 +436,24 @@ def _run_set(S, g, gt, srcs, pool, net=None, cold=False, warm_pass=True, **kw):
     for s in srcs:
         if cold:
             eng.evict_all()
-        _, _, st = eng.bfs(s)
+        d, _, st = eng.bfs(s)
         ms += st.ms
         h2d += st.h2d_bytes
         zc += st.zc_bytes
         levels += st.levels
+        if digests is not None and s in digests:
+            digests[s].append(_digest(d))
     eng.close()
     return {"ms": ms, "h2d_bytes": h2d, "zc_bytes": zc, "levels": levels}
 
 
-def extra_config3(nsrc_train=16, nsrc_eval=16):
+def extra_config3(nsrc_train=32, nsrc_eval=32, nsrc_oracle=16):
     """Directed power law 41.6M / 1.47B: the learned scheduler (trained on
-    dual-timed plain runs) against alpha/beta + demand paging, in HBM and out
-    of core with the 12 GB page pool (warm: steady-state serving; cold: every
-    source starts from an empty pool)."""
+    dual-timed plain runs of 32 sources) against alpha/beta + demand paging
+    on 32 held-out sources, in HBM and out of core with the 12 GB page pool
+    (warm: steady-state serving; cold: every source starts from an empty
+    pool).  The depths of the first 16 held-out sources, in every regime and
+    both arms, are checked against the CPU oracle (digests)."""
     import time as _t
 
     import scaph_b200 as S
@@ -400,6 +462,7 @@ def extra_config3(nsrc_train=16, nsrc_eval=16):
     t0 = _t.time()
     csr, tcsr = workloads.config3()
     g, gt = workloads.paged(csr), workloads.paged(tcsr)
+    del tcsr
     gen_s = _t.time() - t0
     srcs = workloads.random_sources(csr, nsrc_train + nsrc_eval, workloads.SEED_BASE + 2)
     train, held = srcs[:nsrc_train], srcs[nsrc_train:]
@@ -408,22 +471,36 @@ def extra_config3(nsrc_train=16, nsrc_eval=16):
     page_ms = g.pagesize * 4 / 50e9 * 1e3  # page copy at ~50 GB/s (PCIe Gen5 x16, pinned)
     traces = scheduler.collect(g, gt, train)
     net, info = scheduler.train(traces, g, gt, nslots, page_ms, epochs=200)
+    info["held_out"] = scheduler.held_out_accuracy(net, scheduler.collect(g, gt, held), g, gt, nslots, page_ms)
     E, n = csr.E, len(held)
     res = {"graph": "directed power law, Zipf 1.9 out-degree, preferential-attachment destinations",
            "V": csr.V, "E": E, "out_pages": g.npages, "in_pages": gt.npages, "pool_bytes": pool,
            "graph_gen_s": round(gen_s, 1), "train_sources": nsrc_train, "eval_sources": n, "training": info}
+    digests = {s: [] for s in held[:nsrc_oracle]}
     for name, kw in (("hbm", dict(pool=0, use_graph=0)), ("ooc_warm", dict(pool=pool)),
                      ("ooc_cold", dict(pool=pool, cold=True))):
         plain = _run_set(S, g, gt, held, kw["pool"], None, cold=kw.get("cold", False),
-                         use_graph=kw.get("use_graph", 0))
+                         use_graph=kw.get("use_graph", 0), digests=digests)
         learned = _run_set(S, g, gt, held, kw["pool"], net, cold=kw.get("cold", False),
-                           use_graph=kw.get("use_graph", 0) if kw["pool"] else 0)
+                           use_graph=kw.get("use_graph", 0) if kw["pool"] else 0, digests=digests)
         res[name] = {
             "plain_gteps": n * E / (plain["ms"] / 1e3) / 1e9, "learned_gteps": n * E / (learned["ms"] / 1e3) / 1e9,
             "speedup": plain["ms"] / learned["ms"],
             "plain_pcie_bytes_per_level": plain["h2d_bytes"] / max(1, plain["levels"]),
             "learned_pcie_bytes_per_level": learned["h2d_bytes"] / max(1, learned["levels"]),
             "plain_zero_copy_bytes": plain["zc_bytes"], "learned_zero_copy_bytes": learned["zc_bytes"]}
+    # the checker: oracle depths of the checked held-out sources against the
+    # six runs of each (plain and learned, three regimes)
+    from oracle import oracle as O
+
+    t1, bad = _t.perf_counter(), []
+    for s, ds in digests.items():
+        ref = _digest(O.bfs_omp(csr.idx, csr.ngh, s))
+        if len(ds) != 6 or any(d != ref for d in ds):
+            bad.append(s)
+    res["parity"] = {"bit_exact_vs_oracle": not bad, "checked": len(digests), "runs_per_source": 6,
+                     "mismatched_sources": bad[:8], "check_s": round(_t.perf_counter() - t1, 1),
+                     "oracle": "level-synchronous bfs::check restatement, OpenMP (depth digests)"}
     return res
 
 
@@ -443,7 +520,7 @@ def extra_config5(stream, nsrc=128, nplain=8):
     srcs = workloads.random_sources(csr, nsrc, workloads.SEED_BASE + 4)
     gen_s = time.time() - t0
     V, E = csr.V, csr.E
-    del csr, csr_t  # the paged copies are what the engines use
+    del csr_t  # the paged copies are what the engines use (csr stays for the checker)
     pool = 24_000_000_000
     out = {"graph": "web-like: power-law out-degree s=2.1, 90% of edges inside 4096-id blocks", "V": V, "E": E,
            "out_pages": g.npages, "in_pages": gt.npages, "pool_bytes": pool,
@@ -483,6 +560,9 @@ def extra_config5(stream, nsrc=128, nplain=8):
     eng.close()
     out["plain"] = plain
     out["plain_sources_timed"] = nplain
+    # the checker: rows of the last batched launch against the CPU oracle (untimed)
+    nchk = max(nplain, 8)
+    out["parity"] = oracle_check(csr.idx, csr.ngh, ((s, depth[i].cpu().numpy()) for i, s in enumerate(srcs[:nchk])))
     for regime in ("cold", "warm"):
         best = max(out["batched_alpha_beta"][regime]["gteps_per_source"],
                    out["batched_transfer_rule"][regime]["gteps_per_source"])
@@ -562,11 +642,32 @@ def run_ours(args, world):
     clk = clocks.stop()
     # kernels those runs launched (the direction decisions are deterministic,
     # so a counted replay of the same sources launches the same kernels)
-    launches, g500 = 0, []
+    # Every distinct timed source (up to 16 per rank on several GPUs, where
+    # the ranks share the host cores) is also checked bit for bit against the
+    # CPU oracle, from the same replay.
+    launches, g500, parity_runs = 0, [], []
+    check_cap = len(srcs) if world == 1 else max(1, 16 // world)
+    threads = max(1, (os.cpu_count() or 1) // world)
+    seen = set()
+    parity = {"checked": 0, "mismatched_sources": [], "check_s": 0.0}
     for i in range(args.steps):
         st = eng.bfs_device(src_of(i), depth.data_ptr())
         launches += st.launches
         g500.append(st.reached_edges / 2 / (st.ms / 1e3) / 1e9)  # Graph500: undirected edges reached
+        if src_of(i) not in seen and len(seen) < check_cap:
+            seen.add(src_of(i))
+            r = oracle_check(csr.idx, csr.ngh, [(src_of(i), depth.cpu().numpy())], threads=threads)
+            parity["checked"] += r["checked"]
+            parity["mismatched_sources"] += r["mismatched_sources"]
+            parity["check_s"] += r["check_s"]
+    nbad = len(parity["mismatched_sources"])
+    if world > 1:
+        t = torch.tensor([parity["checked"], nbad], dtype=torch.int64, device="cuda")
+        dist.all_reduce(t)
+        parity["checked"], nbad = int(t[0]), int(t[1])
+    parity["bit_exact_vs_oracle"] = parity["checked"] > 0 and nbad == 0
+    parity["oracle"] = "level-synchronous bfs::check restatement, OpenMP on %d host threads per rank" % threads
+    parity["sources"] = "every distinct timed source" if world == 1 else f"up to {check_cap} timed sources per rank"
     ms = replicas.max_over_ranks(ev0.elapsed_time(ev1), world, "cuda")
     if world > 1:
         dist.barrier()
@@ -630,9 +731,9 @@ def run_ours(args, world):
 
     line = {"metric": METRIC, "value": value, "unit": "GTEPS", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "u32", "data": "synthetic (seeded RMAT, generated on the host)",
-            "config": config_dict(csr, args.scale, len(srcs), {"parallelism": f"replicas x{world}",
-                                                                "graph_gen_s": round(gen_s, 1)}),
+            "vs_baseline": None, "dtype": "u32", "data": "synthetic (seeded RMAT)",
+            "config": config_dict(V, E, args.scale, len(srcs)),
+            "parallelism": f"replicas x{world}", "graph_gen_s": round(gen_s, 1), "parity": parity,
             "e2e": {"value": e2e_value, "unit": "GTEPS", "h2d_bytes_per_step": 4, "d2h_bytes_per_step": V * 4,
                     "api": "scaph_bfs (one step at a time)" if args.host_loop else
                            "scaph_bfs_enqueue (pipelined, page-locked host output)",
@@ -641,6 +742,7 @@ def run_ours(args, world):
             "graph500_gteps_median": statistics.median(g500)}
     if rank == 0 and world == 1 and not args.no_cpu:
         line["cpu_baseline"] = cpu_baseline(csr, srcs, args.cpu_seconds)
+        line["cpu_baseline_openmp"] = line["cpu_baseline"].pop("openmp")
     for b in host_bufs:
         b.close()
     eng_h.close()

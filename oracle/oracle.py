@@ -19,6 +19,10 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "liboracle.so")
+# Root of the reference source tree where it is present (the recipes in
+# oracle/Makefile and __graft_entry__.build() compile it from there); only
+# build-and-compare tests read it, and they skip when it is absent.
+REFERENCE_DIR = os.environ.get("SCAPH_REFERENCE", "/root/reference")
 REF_SO = os.path.join(HERE, "_ref", "libscaphref.so")
 REF_PAGEGEN = os.path.join(HERE, "_ref", "pagegencsr")
 # the reference's CSR -> text converters (tools/bin2ligra.cpp, bin2ligraweight.cpp,
@@ -65,6 +69,11 @@ def olib() -> C.CDLL:
         L.oracle_sssp_dijkstra.restype = i32
         L.oracle_min_reaching_id.argtypes = [u32, vp, vp, vp]
         L.oracle_min_reaching_id.restype = i32
+        L.oracle_gen_rmat.argtypes = [i32, C.c_double, C.c_double, C.c_double, C.c_double, C.c_uint64, i32, vp,
+                                      C.POINTER(C.c_void_p), C.POINTER(C.c_uint64)]
+        L.oracle_gen_rmat.restype = i32
+        L.oracle_free.argtypes = [vp]
+        L.oracle_free.restype = None
         _o = L
     return _o
 
@@ -94,6 +103,22 @@ def rlib() -> C.CDLL:
 
 def _csr(idx, ngh):
     return np.ascontiguousarray(idx, np.uint64), np.ascontiguousarray(ngh, np.uint32)
+
+
+def gen_rmat(scale: int, edgefactor: float, a: float, b: float, c: float, seed: int, scramble: bool = True):
+    """The seeded RMAT graph of scaph_gen_rmat, generated without the
+    product library (gen_oracle.c): (idx uint64[V+1], ngh uint32[E])."""
+    V = 1 << scale
+    idx = np.empty(V + 1, np.uint64)
+    ptr, E = C.c_void_p(), C.c_uint64()
+    if olib().oracle_gen_rmat(scale, edgefactor, a, b, c, seed, 1 if scramble else 0, _p(idx), C.byref(ptr),
+                              C.byref(E)) != 0:
+        raise MemoryError("oracle_gen_rmat failed")
+    try:
+        ngh = np.ctypeslib.as_array(C.cast(ptr, C.POINTER(C.c_uint32)), shape=(max(1, E.value),))[:E.value].copy()
+    finally:
+        olib().oracle_free(ptr)
+    return idx, ngh
 
 
 def bfs(idx, ngh, src: int, unreached: int = 0xFFFFFFFF) -> np.ndarray:

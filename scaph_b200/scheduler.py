@@ -253,6 +253,26 @@ def train(traces, g: PagedGraph, gt: PagedGraph | None, nslots: int, page_ms: fl
                  "forward_us_per_call": (t2 - t1) * 1e6}
 
 
+def held_out_accuracy(net: Mlp, traces, g: PagedGraph, gt: PagedGraph | None, nslots: int, page_ms: float,
+                      compact_threshold=3, prefetch_logit=2.0) -> dict:
+    """The trained network on traces it was not trained on: direction
+    accuracy against the same labels (levels 1..), and the page prediction
+    as the engine uses it (prefetch where the logit exceeds prefetch_logit):
+    precision and recall against the pages that really hold the next
+    level's frontier."""
+    n_out, n_in = g.npages, (gt or g).npages
+    X, T, W = dataset(traces, nslots, page_ms, g.V, n_out, n_in, gt is None,
+                      zc_words=compact_threshold * (g.pagesize // 32), page_words=g.pagesize)
+    Y = net.forward(X)
+    m = W[:, 0] > 0
+    dir_acc = float(((Y[m, 0] > 0) == (T[m, 0] > 0.5)).mean()) if m.any() else 1.0
+    pred, true = Y[:, 1:] > prefetch_logit, T[:, 1:] > 0.5
+    tp = int((pred & true).sum())
+    return {"rows": int(len(X)), "direction_rows": int(m.sum()), "direction_accuracy": dir_acc,
+            "prefetch_precision": tp / max(1, int(pred.sum())), "prefetch_recall": tp / max(1, int(true.sum())),
+            "prefetch_logit": prefetch_logit}
+
+
 def evaluate(g: PagedGraph, gt: PagedGraph | None, sources, net: Mlp | None, pool_bytes: int, cold=True,
              **engine_kw) -> dict:
     """Out-of-core runs of `sources`: alpha/beta + demand paging, or the learned

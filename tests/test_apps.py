@@ -15,7 +15,7 @@ from oracle import oracle as O
 from tests import graphs as G
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-REF_APP = "/root/reference/app"
+REF_APP = os.path.join(O.REFERENCE_DIR, "app")
 FAR_BFS = 63           # MAXDEPTH of app/bfs.cu:18
 FAR_SSSP = 0x7FFFFFFF  # MAXPATH of app/sssp.cu:11
 

@@ -163,3 +163,26 @@ def test_set_run_matches_reference():
         for val in (0, 1):
             ref = O.rlib().ref_set_run(m, off, n, val) & 0xFFFFFFFF
             assert L.oracle_set_run(m, off, n, val) == ref
+
+
+@pytest.mark.parametrize("scale,ef,seed,scramble", [(8, 16, 1, True), (12, 16, 0x5CA90001, True),
+                                                    (14, 8, 7, False), (17, 32, 0x5CA90003, True)])
+def test_oracle_rmat_generator_equals_the_library_generator(scale, ef, seed, scramble):
+    """bench.py's reference arm builds its graph with the oracle's generator
+    (no product library in that process): it must give the same CSR."""
+    idx, ngh = O.gen_rmat(scale, ef, 0.57, 0.19, 0.19, seed, scramble)
+    csr = S.Csr.rmat(scale, ef, 0.57, 0.19, 0.19, seed=seed, scramble=scramble)
+    assert np.array_equal(idx, csr.idx)
+    assert np.array_equal(ngh, csr.ngh)
+
+
+def test_reference_arm_workload_equals_ours():
+    """Same graph and same sources in both bench arms (small scale)."""
+    import bench
+    from scaph_b200 import workloads
+
+    idx, ngh, srcs = bench.rmat24_for_reference(14, 16)
+    csr, srcs2 = workloads.config2(14, 16)
+    assert srcs == srcs2
+    assert np.array_equal(idx, csr.idx) and np.array_equal(ngh, csr.ngh)
+    assert bench.config_dict(len(idx) - 1, len(ngh), 14, 16) == bench.config_dict(csr.V, csr.E, 14, len(srcs2))

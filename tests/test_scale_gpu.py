@@ -1,0 +1,116 @@
+"""Parity at larger sizes: an RMAT-21 graph cut into ~600 pages (more than
+the 512 page-table entries and 1024 coarse-index buckets the level kernels
+stage in shared memory, so they read the tables from global memory), RMAT-22
+at the reference's 10 Mi-word pages, and a directed power-law graph of 2.2M
+vertices with its transposed pages, in HBM and streamed through a small
+page pool.  Single-source runs, multi-source batches and the out-of-core
+pager are compared bit for bit with the CPU oracle (OpenMP restatement of
+bfs::check, app/bfs.cu:70-101)."""
+import numpy as np
+import pytest
+
+import scaph_b200 as S
+from oracle import oracle as O
+from tests import graphs as G
+
+pytestmark = pytest.mark.gpu
+
+
+def _same(csr, src, depth, unreached=S.UNREACHED):
+    ref = O.bfs_omp(csr.idx, csr.ngh, int(src), unreached)
+    bad = np.flatnonzero(depth != ref)
+    assert bad.size == 0, f"src {src}: {bad.size} mismatches, v={bad[0]} gpu={depth[bad[0]]} cpu={ref[bad[0]]}"
+
+
+@pytest.fixture(scope="module")
+def rmat21():
+    csr = S.Csr.rmat(21, 16, seed=G.SEED + 60, scramble=True)
+    g = S.PagedGraph.from_csr(csr, pagesize_words=1 << 16)
+    assert g.npages > 512
+    return csr, g
+
+
+@pytest.fixture(scope="module")
+def powerlaw2m():
+    csr = S.Csr.powerlaw(2_200_000, 33_000_000, 1.9, 1 << 15, seed=G.SEED + 61)
+    tcsr = csr.transpose()
+    g = S.PagedGraph.from_csr(csr, pagesize_words=1 << 18)
+    gt = S.PagedGraph.from_csr(tcsr, pagesize_words=1 << 18)
+    return csr, g, gt
+
+
+@pytest.mark.parametrize("use_graph", [0, 2], ids=["graph", "hostloop"])
+def test_rmat21_many_pages(rmat21, use_graph):
+    csr, g = rmat21
+    eng = S.Engine(g, use_graph=use_graph)
+    srcs = G.sources(csr, 3, 60) + [int(np.argmax(csr.degree()))]
+    pulls = 0
+    for src in srcs:
+        depth, parent, st = eng.bfs(src, parents=True)
+        _same(csr, src, depth)
+        rc, bad = O.validate_tree(csr.idx, csr.ngh, src, depth, parent)
+        assert rc == 0, f"invalid BFS tree (code {rc} at {bad})"
+        pulls += st.pull_levels
+    assert pulls > 0
+    eng.close()
+
+
+def test_rmat21_msbfs_64(rmat21):
+    csr, g = rmat21
+    eng = S.Engine(g)
+    srcs = G.sources(csr, 64, 62)
+    depth, st = eng.msbfs(srcs)
+    for i, s in enumerate(srcs):
+        _same(csr, s, depth[i])
+    eng.close()
+
+
+def test_rmat21_out_of_core(rmat21):
+    csr, g = rmat21
+    eng = S.Engine(g, pool_bytes=100 * g.pagesize * 4)  # 100 slots for ~600 pages
+    for i, src in enumerate(G.sources(csr, 3, 63)):
+        if i == 1:
+            eng.evict_all()
+        depth, _, st = eng.bfs(src)
+        _same(csr, src, depth)
+        assert st.page_faults > 0 or st.zc_bytes > 0
+    eng.close()
+
+
+def test_rmat22_reference_pages():
+    csr = S.Csr.rmat(22, 16, seed=G.SEED + 64, scramble=True)
+    g = S.PagedGraph.from_csr(csr)
+    eng = S.Engine(g)
+    for src in G.sources(csr, 3, 64):
+        depth, _, _ = eng.bfs(src)
+        _same(csr, src, depth)
+    eng.close()
+
+
+@pytest.mark.parametrize("direction", [S.DIR_ALPHABETA, S.DIR_PULL])
+def test_powerlaw2m_directed_in_hbm(powerlaw2m, direction):
+    csr, g, gt = powerlaw2m
+    eng = S.Engine(g, gt, direction=direction)
+    for src in G.sources(csr, 3, 65):
+        depth, parent, st = eng.bfs(src, parents=True)
+        _same(csr, src, depth)
+        rc, bad = O.validate_tree(csr.idx, csr.ngh, src, depth, parent)
+        assert rc == 0, f"invalid BFS tree (code {rc} at {bad})"
+    eng.close()
+
+
+def test_powerlaw2m_directed_out_of_core(powerlaw2m):
+    csr, g, gt = powerlaw2m
+    total = g.npages + gt.npages
+    eng = S.Engine(g, gt, pool_bytes=(total // 4) * g.pagesize * 4)
+    srcs = G.sources(csr, 3, 66)
+    for i, src in enumerate(srcs):
+        if i == 1:
+            eng.evict_all()
+        depth, _, st = eng.bfs(src)
+        _same(csr, src, depth)
+    # the multi-source traversal through the same pager
+    depth, st = eng.msbfs(srcs + G.sources(csr, 61, 67))
+    for i, s in enumerate(srcs):
+        _same(csr, s, depth[i])
+    eng.close()
