@@ -59,6 +59,7 @@ def parse_args():
     ap.add_argument("--no-config5", action="store_true",
                     help="skip the 105M-vertex / 3.7B-edge web graph (about a minute to generate)")
     ap.add_argument("--only-extra", default=None, help=argparse.SUPPRESS)
+    ap.add_argument("--no-tune", action="store_true", help="keep the engine's default tunables")
     ap.add_argument("--host-loop", action="store_true",
                     help="time the host-driven level loop (one launch per level kernel) instead of one "
                          "CUDA-graph launch per BFS; for profilers that time kernels one launch at a time")
@@ -321,10 +322,15 @@ def extra_config4a(stream):
     g = workloads.paged(csr)
     eng = S.Engine(g, stream=stream.cuda_stream)
     out = torch.empty((len(srcs), csr.V), dtype=torch.int32, device="cuda")
+    from scaph_b200 import autotune
+
+    tune = autotune.tune_engine(eng, workloads.random_sources(csr, 64, workloads.SEED_BASE + 203), out.data_ptr(),
+                                multi=True, repeats=2)
     eng.msbfs_device(srcs, out.data_ptr())
     runs = [eng.msbfs_device(srcs, out.data_ptr()) for _ in range(3)]
     ms_batch = min(r.ms for r in runs)
     tr = eng.msbfs_trace()
+    eng.tune(alpha=14.0, beta=24.0)  # the plain engine keeps the default alpha/beta
     d = torch.empty(csr.V, dtype=torch.int32, device="cuda")
     for s in srcs[:3]:
         eng.bfs_device(s, d.data_ptr())
@@ -341,6 +347,7 @@ def extra_config4a(stream):
     # every row of the batched launch against the CPU oracle (untimed)
     parity = oracle_check(csr.idx, csr.ngh, ((s, out[i].cpu().numpy()) for i, s in enumerate(srcs)))
     return {"graph": "RMAT-25 ef16", "V": csr.V, "E": csr.E, "sources_per_launch": n, "parity": parity,
+            "autotune": tune,
             "batched_ms": ms_batch, "batched_gteps_per_source": n * csr.E / (ms_batch / 1e3) / 1e9,
             "plain_ms_for_same_sources": ms_plain, "plain_gteps": n * csr.E / (ms_plain / 1e3) / 1e9,
             "speedup_vs_plain": ms_plain / ms_batch, "levels": len(tr),
@@ -504,30 +511,53 @@ def extra_config3(nsrc_train=32, nsrc_eval=32, nsrc_oracle=16):
     return res
 
 
-def extra_config5(stream, nsrc=128, nplain=8):
+def extra_config5(stream, nsrc=128, nplain=8, ntrain=8):
     """Web-crawl-like graph 105M / 3.7B streamed out of core with a 24 GB page
-    pool: 128 sources per multi-source launch (alpha/beta, and with the
-    scheduler's out-of-core transfer rule) against the plain engine (one
-    source per launch, alpha/beta + demand paging), warm and cold pools."""
+    pool: 128 sources per multi-source launch - with alpha/beta, with the
+    scheduler's page-traffic rule alone, and with the learned scheduler
+    (network trained on this graph's plain-engine traces and on two
+    multi-source batches of other sources; it picks directions near the
+    switch point and prefetches the pages it predicts for the next level) -
+    against the plain engine (one source per launch, alpha/beta + demand
+    paging), warm and cold pools."""
     import torch
 
+    import numpy as np
+
     import scaph_b200 as S
-    from scaph_b200 import workloads
+    from scaph_b200 import scheduler, workloads
 
     t0 = time.time()
     csr, csr_t = workloads.config5()
     g, gt = workloads.paged(csr), workloads.paged(csr_t)
     srcs = workloads.random_sources(csr, nsrc, workloads.SEED_BASE + 4)
+    pool_train = [s for s in workloads.random_sources(csr, 2 * nsrc + ntrain + nsrc, workloads.SEED_BASE + 104)
+                  if s not in set(srcs)]
     gen_s = time.time() - t0
     V, E = csr.V, csr.E
     del csr_t  # the paged copies are what the engines use (csr stays for the checker)
     pool = 24_000_000_000
+    nslots = pool // (g.pagesize * 4)
     out = {"graph": "web-like: power-law out-degree s=2.1, 90% of edges inside 4096-id blocks", "V": V, "E": E,
            "out_pages": g.npages, "in_pages": gt.npages, "pool_bytes": pool,
-           "pool_pages": pool // (g.pagesize * 4), "graph_gen_s": round(gen_s, 1), "sources": nsrc}
+           "pool_pages": nslots, "graph_gen_s": round(gen_s, 1), "sources": nsrc}
     depth = torch.empty((nsrc, V), dtype=torch.int32, device="cuda")
-    for name, direction in (("batched_alpha_beta", S.DIR_ALPHABETA), ("batched_transfer_rule", S.DIR_LEARNED)):
+    # the scheduler network, trained on this graph (sources disjoint from the
+    # evaluated ones)
+    t1 = time.time()
+    page_ms = g.pagesize * 4 / 50e9 * 1e3
+    traces = scheduler.collect(g, gt, pool_train[:ntrain])
+    ms_rows = scheduler.collect_ms(g, gt, [pool_train[ntrain:ntrain + nsrc], pool_train[ntrain + nsrc:ntrain + 2 * nsrc]],
+                                   depth_ptr=depth.data_ptr())
+    net, info = scheduler.train(traces, g, gt, nslots, page_ms, epochs=200, ms_rows=ms_rows)
+    info["collect_and_train_s"] = round(time.time() - t1, 1)
+    out["training"] = info
+    arms = (("batched_alpha_beta", S.DIR_ALPHABETA, None), ("batched_transfer_rule", S.DIR_LEARNED, None),
+            ("batched_learned", S.DIR_LEARNED, net))
+    for name, direction, sched in arms:
         eng = S.Engine(g, gt, pool_bytes=pool, direction=direction, stream=stream.cuda_stream)
+        if sched is not None:
+            eng.set_scheduler(sched)
         res = {}
         for regime in ("cold", "warm"):
             if regime == "cold":
@@ -536,8 +566,9 @@ def extra_config5(stream, nsrc=128, nplain=8):
             tr = eng.msbfs_trace()
             res[regime] = {"ms": st.ms, "gteps_per_source": nsrc * E / (st.ms / 1e3) / 1e9,
                            "h2d_bytes": st.h2d_bytes, "zero_copy_bytes": st.zc_bytes,
-                           "page_faults": st.page_faults, "levels": st.levels,
+                           "page_faults": st.page_faults, "prefetched": st.prefetched, "levels": st.levels,
                            "pcie_bytes_per_level": (st.h2d_bytes + st.zc_bytes) / max(1, st.levels),
+                           "pcie_alg_bytes_per_level": st.pcie_alg_bytes / max(1, st.levels),
                            "directions": "".join("p" if t["direction"] else "P" for t in tr)}
         out[name] = res
         eng.close()
@@ -546,7 +577,7 @@ def extra_config5(stream, nsrc=128, nplain=8):
     d1 = torch.empty(V, dtype=torch.int32, device="cuda")
     plain = {}
     for regime in ("cold", "warm"):
-        ms, h2d, zc, exact = 0.0, 0, 0, True
+        ms, h2d, zc, alg, lv, exact = 0.0, 0, 0, 0, 0, True
         for i, s in enumerate(srcs[:nplain]):
             if regime == "cold":
                 eng.evict_all()
@@ -554,20 +585,57 @@ def extra_config5(stream, nsrc=128, nplain=8):
             ms += st.ms
             h2d += st.h2d_bytes
             zc += st.zc_bytes
+            alg += st.pcie_alg_bytes
+            lv += st.levels
             exact &= bool(torch.equal(d1, depth[i]))
         plain[regime] = {"ms_per_source": ms / nplain, "gteps": E / (ms / nplain / 1e3) / 1e9,
-                         "pcie_bytes_per_source": (h2d + zc) / nplain, "batched_rows_equal": exact}
+                         "pcie_bytes_per_source": (h2d + zc) / nplain, "pcie_bytes_per_level": (h2d + zc) / max(1, lv),
+                         "pcie_alg_bytes_per_level": alg / max(1, lv), "batched_rows_equal": exact}
     eng.close()
     out["plain"] = plain
     out["plain_sources_timed"] = nplain
-    # the checker: rows of the last batched launch against the CPU oracle (untimed)
+    for regime in ("cold", "warm"):
+        out[f"speedup_vs_plain_{regime}"] = out["batched_learned"][regime]["gteps_per_source"] / plain[regime]["gteps"]
+        out[f"learned_vs_batched_alpha_beta_{regime}"] = (out["batched_alpha_beta"][regime]["ms"] /
+                                                        out["batched_learned"][regime]["ms"])
+    # the checker: rows of the last (learned, warm) batched launch against the
+    # CPU oracle, untimed; the oracle's own time on those sources is the CPU
+    # baseline (level-synchronous bfs::check restatement, OpenMP, every core)
     nchk = max(nplain, 8)
     out["parity"] = oracle_check(csr.idx, csr.ngh, ((s, depth[i].cpu().numpy()) for i, s in enumerate(srcs[:nchk])))
-    for regime in ("cold", "warm"):
-        best = max(out["batched_alpha_beta"][regime]["gteps_per_source"],
-                   out["batched_transfer_rule"][regime]["gteps_per_source"])
-        out[f"speedup_vs_plain_{regime}"] = best / plain[regime]["gteps"]
+    cpu_s = out["parity"]["check_s"]
+    out["cpu_baseline"] = {"value": nchk * E / max(cpu_s, 1e-9) / 1e9, "unit": "GTEPS per source",
+                           "cores": os.cpu_count() or 1, "kind": "port",
+                           "sample": f"{nchk} sources of the same graph, level-synchronous restatement of bfs::check "
+                                     f"with OpenMP, {cpu_s:.1f} s (includes comparing the rows)"}
     return out
+
+
+def learned_batched_vs_plain(extras):
+    """The metric's own comparison, from the config-5 and PCIe extras:
+    learned+batched against the plain engine on the largest out-of-core
+    configuration, GTEPS per source and PCIe bytes per level (actual and
+    algorithmic), with the PCIe roofline of the cold batched launch."""
+    c5, pc = extras.get("config5_ooc_batched") or {}, extras.get("pcie") or {}
+    if "batched_learned" not in c5:
+        return {"unavailable": c5.get("error", "config 5 not run")}
+    link = pc.get("h2d_gbs_measured")
+    cold = c5["batched_learned"]["cold"]
+    moved = cold["h2d_bytes"] + cold["zero_copy_bytes"]
+    achieved = moved / (cold["ms"] / 1e3) / 1e9
+    return {
+        "config": "config 5: web-like graph V=%d E=%d, 24 GB page pool, %d sources per launch" % (
+            c5["V"], c5["E"], c5["sources"]),
+        "learned_batched": c5["batched_learned"], "plain": c5["plain"],
+        "batched_alpha_beta": c5["batched_alpha_beta"],
+        "gteps_ratio_cold": c5["speedup_vs_plain_cold"], "gteps_ratio_warm": c5["speedup_vs_plain_warm"],
+        "learned_vs_batched_alpha_beta_cold": c5["learned_vs_batched_alpha_beta_cold"],
+        "learned_vs_batched_alpha_beta_warm": c5["learned_vs_batched_alpha_beta_warm"],
+        "roofline": {"bound": "pcie", "achieved": achieved, "peak": link, "unit": "GB/s",
+                     "frac": achieved / link if link else None,
+                     "peak_source": "pinned host-to-device copy measured in the same run",
+                     "traffic": moved, "alg_bytes": cold["pcie_alg_bytes_per_level"] * cold["levels"]},
+        "cpu_baseline": c5["cpu_baseline"], "parity": c5["parity"], "training": c5.get("training")}
 
 
 def extra_pcie(stream):
@@ -619,6 +687,14 @@ def run_ours(args, world):
     torch.cuda.set_stream(stream)
     eng = S.Engine(g, device=local_rank, stream=stream.cuda_stream, use_graph=2 if args.host_loop else 0)
     depth = torch.empty(V, dtype=torch.int32, device="cuda")
+    # the engine's tunables, picked by the autotuner on 8 other sources of
+    # the same graph (untimed)
+    tune = None
+    if not args.no_tune:
+        from scaph_b200 import autotune
+
+        tune = autotune.tune_engine(eng, workloads.random_sources(csr, 8, workloads.SEED_BASE + 201),
+                                    depth.data_ptr())
 
     order = replicas.rank_sources(srcs, rank, max(args.steps, args.warmup))
 
@@ -704,6 +780,8 @@ def run_ours(args, world):
     # source (separate, untimed pass)
     per_dir = {0: [0, 0.0, 0], 1: [0, 0.0, 0]}  # alg bytes, ms, launches
     eng_h = S.Engine(g, device=local_rank, stream=stream.cuda_stream, use_graph=2)  # per-level CUDA events
+    if tune:
+        eng_h.tune(**tune["params"])
     for s in srcs:
         eng_h.bfs(s)
         for t in eng_h.trace():
@@ -734,6 +812,7 @@ def run_ours(args, world):
             "vs_baseline": None, "dtype": "u32", "data": "synthetic (seeded RMAT)",
             "config": config_dict(V, E, args.scale, len(srcs)),
             "parallelism": f"replicas x{world}", "graph_gen_s": round(gen_s, 1), "parity": parity,
+            "autotune": tune,
             "e2e": {"value": e2e_value, "unit": "GTEPS", "h2d_bytes_per_step": 4, "d2h_bytes_per_step": V * 4,
                     "api": "scaph_bfs (one step at a time)" if args.host_loop else
                            "scaph_bfs_enqueue (pipelined, page-locked host output)",
@@ -765,6 +844,7 @@ def run_ours(args, world):
                 extras[name] = {"error": f"{type(exc).__name__}: {exc}"}
             print(f"[bench] {name}: {json.dumps(extras[name])[:300]}", file=sys.stderr, flush=True)
         line["extras"] = extras
+        line["learned_batched_vs_plain"] = learned_batched_vs_plain(extras)
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()

@@ -33,6 +33,18 @@ extern "C" {
 
 /* Message of the last failing call on this thread ("" if none). */
 const char *scaph_last_error(void);
+/* Test hook with no counterpart in the reference, where a failing CUDA call
+ * ends the process (H_ERR -> exit, src/gpu_engine.cuh:28-39).  Arms a host
+ * side fault: after `skip` further calls at `site` succeed, the next `count`
+ * calls there fail as the CUDA runtime would report it, without calling it,
+ * so that tests can check that every entry point returns a status (and
+ * leaves nothing half-built) instead of aborting.  Sites:
+ *   "pinned_alloc"   cudaMallocHost (scaph_host_alloc, engine staging)
+ *   "host_register"  cudaHostRegister of a graph's pages (out-of-core pool)
+ *   "page_copy"      a host-to-HBM page copy of the out-of-core pool
+ *   "device_alloc"   cudaMalloc of scaph_engine_create's per-vertex state
+ * site NULL disarms every site.  SCAPH_EINVAL for an unknown site. */
+int scaph_fault_inject(const char *site, int skip, int count);
 /* Library version string. */
 const char *scaph_version(void);
 
@@ -199,6 +211,19 @@ typedef struct scaph_config {
     float    link_gbs;         /* out-of-core learned scheduler: host->HBM
                                   page bandwidth (GB/s) its transfer-cost
                                   estimate assumes; 0 = measured at create  */
+    /* Launch-shape tunables (the reference's are FLAGS_num_blks /
+     * FLAGS_num_thds / FLAGS_num_stream, src/app.cuh:38-52, used per page at
+     * src/app.cuh:438); 0 = default.  Searched by scaph_b200/autotune.py.  */
+    int32_t  giant_edges;      /* push: adjacency longer than this is cut into
+                                  chunks of this many edges, one CTA each;
+                                  128..65536, 0 = 1024                      */
+    int32_t  pull_gather_ratio;/* a pull level gathers several tiles' vertices
+                                  into one queue when fewer than one vertex
+                                  in this many is unvisited; 0 = 64         */
+    int32_t  ms_compact_l2_div;/* multi-source pull: frontier masks are
+                                  compacted when they fit L2 / this; 0 = 3  */
+    int32_t  ms_compact_min_deg;/* ... and the frontier has at least this
+                                  many out-edges per vertex; 0 = 16        */
 } scaph_config;
 
 typedef struct scaph_engine scaph_engine;
@@ -231,6 +256,11 @@ typedef struct scaph_bfs_stats {
     uint64_t prefetched;        /* page loads issued ahead by the scheduler */
     uint64_t launches;          /* kernels this library launched            */
     double   ms;                /* device time of the traversal (events)    */
+    uint64_t pcie_alg_bytes;    /* out of core: the least the levels had to
+                                   bring over the link, 4 * sum(deg+3) of the
+                                   active vertices of needed pages that were
+                                   not resident (get_page_info's datas,
+                                   src/gpu_engine.cuh:413-419)             */
 } scaph_bfs_stats;
 
 /* Single-source level-synchronous BFS (replaces App::run, src/app.cuh:220-265,
@@ -241,6 +271,13 @@ typedef struct scaph_bfs_stats {
  * stats may be NULL. */
 int scaph_bfs(scaph_engine *e, uint32_t src, uint32_t *depths, uint32_t *parents,
               int out_on_device, scaph_bfs_stats *stats);
+/* Sets an engine's run-time tunables from cfg: alpha, beta, block_size,
+ * ctas_per_sm, giant_edges, pull_gather_ratio, ms_compact_l2_div and
+ * ms_compact_min_deg (0 = default; the other fields are ignored).  They
+ * change the schedule only, never the depths.  Waits for the engine's work
+ * and drops its CUDA graph (the next run rebuilds it).  Replaces setting
+ * FLAGS_num_blks / FLAGS_num_thds between runs (src/app.cuh:38-52). */
+int scaph_engine_tune(scaph_engine *e, const scaph_config *cfg);
 /* Out-of-core engines (pool_bytes smaller than the graph's pages): drops
  * every page from the HBM pool, so the next traversal starts cold. */
 int scaph_engine_evict_all(scaph_engine *e);
@@ -279,7 +316,7 @@ typedef struct scaph_level_trace {
 int scaph_bfs_trace(scaph_engine *e, scaph_level_trace *out, int cap);
 /* Active-vertex histogram of the frontier at `level` of the last run:
  * nodes[p] / datas[p] as get_page_info computes them (src/gpu_engine.cuh:397-441).
- * Recorded by every host-loop run; by a graph-mode run only with
+ * Recorded by out-of-core runs, and by resident runs only with
  * record_features or the learned direction (SCAPH_EUNSUPPORTED otherwise). */
 int scaph_bfs_page_hist(scaph_engine *e, int level, uint32_t *nodes,
                         uint32_t *datas, int npages);
@@ -319,8 +356,10 @@ int scaph_mlp_load(scaph_mlp *m, const char *path);
  * logit exceeds 0 are prefetched while the level runs.  The engine keeps
  * the pointer; it never changes depths. */
 int scaph_engine_set_scheduler(scaph_engine *e, scaph_mlp *m);
-/* Feature rows of the last host-loop run (record_features or learned mode):
- * returns the row count, writes min(rows, cap) rows of *dim floats. */
+/* Feature rows of the last host-loop scaph_bfs or of the last scaph_msbfs
+ * (record_features or learned mode; a multi-source row counts the union of
+ * the batch's frontiers): returns the row count, writes min(rows, cap) rows
+ * of *dim floats. */
 int scaph_bfs_features(scaph_engine *e, float *out, int cap, int *dim);
 /* Unvisited vertices per in-edge page at `level` of the last run
  * (record_features): the pages a pull at that level would read, and their

@@ -255,3 +255,22 @@ def export_text(idx32, ngh, wgh, kind: str) -> bytes:
                 else:
                     lines.append(f"{v}\t{int(ngh[e])}")
     return ("\n".join(lines) + "\n").encode()
+
+
+def pagerank(idx, ngh, iters: int = 20, damping: float = 0.85) -> np.ndarray:
+    """PageRank by power iteration in float64 (the rule scaph_b200/apps/pr
+    applies in float32): rank'(v) = (1-d)/V + d * (sum over edges u->v of
+    rank(u)/outdeg(u) + (rank of vertices without out-edges)/V), from the
+    uniform vector.  The reference has no working PageRank to restate
+    (app/pr.cu does not build)."""
+    idx, ngh = _csr(idx, ngh)
+    V = len(idx) - 1
+    deg = np.diff(idx).astype(np.float64)
+    src = np.repeat(np.arange(V), np.diff(idx).astype(np.int64))
+    rank = np.full(V, 1.0 / V)
+    for _ in range(iters):
+        contrib = np.where(deg > 0, rank / np.maximum(deg, 1.0), 0.0)
+        dangling = rank[deg == 0].sum()
+        acc = np.bincount(ngh, weights=contrib[src], minlength=V)
+        rank = (1.0 - damping) / V + damping * (acc + dangling / V)
+    return rank

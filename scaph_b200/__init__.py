@@ -52,7 +52,8 @@ class _Config(C.Structure):
                 ("ctas_per_sm", C.c_int32), ("copy_streams", C.c_int32), ("prefetch", C.c_int32),
                 ("compact_threshold", C.c_int32), ("use_graph", C.c_int32), ("device", C.c_int32),
                 ("stream", C.c_void_p), ("record_features", C.c_int32), ("dual_timing", C.c_int32),
-                ("link_gbs", C.c_float)]
+                ("link_gbs", C.c_float), ("giant_edges", C.c_int32), ("pull_gather_ratio", C.c_int32),
+                ("ms_compact_l2_div", C.c_int32), ("ms_compact_min_deg", C.c_int32)]
 
 
 class _Stats(C.Structure):
@@ -60,7 +61,7 @@ class _Stats(C.Structure):
                 ("_pad", C.c_int32), ("reached", C.c_uint64), ("reached_edges", C.c_uint64),
                 ("edges_inspected", C.c_uint64), ("alg_bytes", C.c_uint64), ("h2d_bytes", C.c_uint64),
                 ("zc_bytes", C.c_uint64), ("page_faults", C.c_uint64), ("prefetched", C.c_uint64),
-                ("launches", C.c_uint64), ("ms", C.c_double)]
+                ("launches", C.c_uint64), ("ms", C.c_double), ("pcie_alg_bytes", C.c_uint64)]
 
 
 class _Query(C.Structure):
@@ -120,6 +121,7 @@ def lib() -> C.CDLL:
         "scaph_engine_sync": ([vp], i32),
         "scaph_bfs_enqueue": ([vp, u32, vp], i32),
         "scaph_engine_evict_all": ([vp], i32),
+        "scaph_engine_tune": ([vp, P(_Config)], i32),
         "scaph_mlp_create": ([i32, i32, u64, i32, P(vp)], i32),
         "scaph_mlp_destroy": ([vp], None),
         "scaph_mlp_num_params": ([vp], C.c_size_t),
@@ -147,6 +149,7 @@ def lib() -> C.CDLL:
         "scaph_host_alloc": ([C.c_size_t], vp),
         "scaph_host_free": ([vp], None),
         "scaph_device_count": ([], i32),
+        "scaph_fault_inject": ([C.c_char_p, i32, i32], i32),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)
@@ -164,6 +167,13 @@ def _check(rc: int) -> int:
 
 def _ptr(a: np.ndarray | None) -> C.c_void_p | None:
     return None if a is None else C.c_void_p(a.ctypes.data)
+
+
+def fault_inject(site: str | None, skip: int = 0, count: int = 1) -> None:
+    """Test hook (scaph_fault_inject): after `skip` further calls at `site`
+    succeed, the next `count` fail as the CUDA runtime would report it;
+    site None disarms every site."""
+    _check(lib().scaph_fault_inject(site.encode() if site else None, skip, count))
 
 
 def device_count() -> int:
@@ -425,11 +435,13 @@ class BfsStats:
     prefetched: int
     launches: int
     ms: float
+    pcie_alg_bytes: int = 0
 
 
 def _stats(s: _Stats) -> BfsStats:
     return BfsStats(s.levels, s.push_levels, s.pull_levels, s.reached, s.reached_edges, s.edges_inspected,
-                    s.alg_bytes, s.h2d_bytes, s.zc_bytes, s.page_faults, s.prefetched, s.launches, s.ms)
+                    s.alg_bytes, s.h2d_bytes, s.zc_bytes, s.page_faults, s.prefetched, s.launches, s.ms,
+                    s.pcie_alg_bytes)
 
 
 class Engine:
@@ -440,11 +452,12 @@ class Engine:
                  beta: float = 24.0, block_size: int = 256, ctas_per_sm: int = 0, copy_streams: int = 2,
                  prefetch: int = 0, compact_threshold: int = 3, use_graph: int = 0, device: int = 0,
                  stream: int | None = None, record_features: int = 0, dual_timing: int = 0,
-                 link_gbs: float = 0.0):
+                 link_gbs: float = 0.0, giant_edges: int = 0, pull_gather_ratio: int = 0,
+                 ms_compact_l2_div: int = 0, ms_compact_min_deg: int = 0):
         self.graph, self.transposed = graph, transposed
         cfg = _Config(pool_bytes, unreached, direction, alpha, beta, block_size, ctas_per_sm, copy_streams,
                       prefetch, compact_threshold, use_graph, device, stream, record_features, dual_timing,
-                      link_gbs)
+                      link_gbs, giant_edges, pull_gather_ratio, ms_compact_l2_div, ms_compact_min_deg)
         self._cfg = cfg
         h = C.c_void_p()
         _check(lib().scaph_engine_create(graph._h, transposed._h if transposed else None, C.byref(cfg), C.byref(h)))
@@ -516,7 +529,8 @@ class Engine:
         self._sched = mlp  # keep the network alive while the engine uses it
 
     def features(self) -> np.ndarray:
-        """Scheduler feature rows of the last host-loop run (levels x dim)."""
+        """Scheduler feature rows of the last host-loop single-source run or
+        of the last multi-source run (levels x dim)."""
         dim = C.c_int()
         rows = _check(lib().scaph_bfs_features(self._h, None, 0, C.byref(dim)))
         out = np.zeros((rows, dim.value), np.float32)
@@ -530,6 +544,27 @@ class Engine:
         datas = np.zeros(npages_in, np.uint32)
         _check(lib().scaph_bfs_pull_pages(self._h, level, _ptr(cnt), _ptr(datas), npages_in))
         return cnt, datas
+
+    TUNABLES = ("alpha", "beta", "block_size", "ctas_per_sm", "giant_edges", "pull_gather_ratio",
+                "ms_compact_l2_div", "ms_compact_min_deg")
+
+    def tune(self, **kw) -> None:
+        """Sets run-time tunables (scaph_engine_tune); others keep their value."""
+        for k, v in kw.items():
+            if k not in self.TUNABLES:
+                raise ScaphError(EINVAL, f"not a tunable: {k}")
+            setattr(self._cfg, k, v)
+        _check(lib().scaph_engine_tune(self._h, C.byref(self._cfg)))
+
+    _TUNABLE_DEFAULTS = {"giant_edges": 1024, "pull_gather_ratio": 64, "ms_compact_l2_div": 3,
+                         "ms_compact_min_deg": 16}
+
+    def tunables(self) -> dict:
+        """The tunables in force (0 fields shown as the defaults they mean)."""
+        out = {k: getattr(self._cfg, k) for k in self.TUNABLES}
+        for k, v in self._TUNABLE_DEFAULTS.items():
+            out[k] = out[k] or v
+        return out
 
     def evict_all(self) -> None:
         """Out-of-core engines: start the next traversal with a cold page pool."""

@@ -1,4 +1,5 @@
-"""Autotuner for the query-batch kernels (scaph_batch_*).
+"""Autotuners for the query-batch kernels (scaph_batch_*) and for the
+single- and multi-source engine (scaph_engine_tune).
 
 The batch's level kernels take their CTA size (256 or 512 threads), the
 number of CTAs per SM, and the two direction-switch thresholds alpha / beta
@@ -22,7 +23,7 @@ import time
 
 import numpy as np
 
-from . import Batch
+from . import Batch, Engine
 
 SHAPES = [(256, c) for c in (2, 3, 4, 6, 8)] + [(512, c) for c in (1, 2, 3, 4)]
 ALPHAS = (7.0, 10.0, 14.0, 20.0, 28.0)
@@ -125,3 +126,78 @@ def tune_batch(batch: Batch, queries, ptr: int, repeats: int = 3, cache: str | N
     db[key] = out
     _store(path, db)
     return dict(out, cached=False)
+
+
+# ---------------------------------------------------------------------------
+# the engine: single-source traversals and multi-source batches
+# ---------------------------------------------------------------------------
+GIANT = (256, 512, 1024, 2048, 4096)
+GATHER = (16, 32, 64, 128, 256)
+CTAS = (0, 2, 3, 4, 6, 8)  # 0: the occupancy limit
+MS_L2_DIV = (2, 3, 4, 6, 8)
+MS_MIN_DEG = (4, 8, 16, 32, 64)
+
+
+def _engine_run(eng: Engine, sources, ptr: int, multi: bool) -> float:
+    if multi:
+        return eng.msbfs_device(sources, ptr).ms
+    return sum(eng.bfs_device(int(s), ptr).ms for s in sources)
+
+
+def _engine_checksum(eng: Engine, sources, multi: bool) -> int:
+    if multi:
+        rows = eng.msbfs(sources)[0]
+    else:
+        rows = [eng.bfs(int(s))[0] for s in sources]
+    h = 0
+    for i, r in enumerate(rows):
+        r = np.asarray(r)
+        h = (h * 1000003 + int(np.bitwise_xor.reduce(r.astype(np.uint64) * np.uint64(2654435761) +
+                                                     np.arange(len(r), dtype=np.uint64))) + i) & (2**64 - 1)
+    return h
+
+
+def tune_engine(eng: Engine, sources, ptr: int, multi: bool = False, repeats: int = 3) -> dict:
+    """Coordinate search over the engine's tunables on the caller's own
+    workload: `sources` run one by one (single-source; `ptr` a device
+    buffer of V words) or as one multi-source batch (`ptr`: len(sources) * V
+    words).  Single-source: CTAs per SM, the giant-chunk cut, the pull
+    gather ratio, alpha, beta; multi-source: the mask-compaction thresholds,
+    alpha, beta.  Each candidate is timed best of `repeats` (device time);
+    the default's spread over `repeats` more runs is reported beside the
+    result, so a gain can be told from noise.  The chosen tunables must
+    reproduce the default's depths (checksum).  Sets and returns them."""
+    t0 = time.time()
+    start = eng.tunables()
+    ref_sum = _engine_checksum(eng, sources, multi)
+    _engine_run(eng, sources, ptr, multi)  # warm
+    runs = [_engine_run(eng, sources, ptr, multi) for _ in range(2 * repeats)]
+    default_ms = min(runs)
+    best, best_ms, tried = dict(start), default_ms, 1
+
+    def trial(p):
+        nonlocal best, best_ms, tried
+        eng.tune(**p)
+        _engine_run(eng, sources, ptr, multi)  # builds the CUDA graph
+        ms = min(_engine_run(eng, sources, ptr, multi) for _ in range(repeats))
+        tried += 1
+        if ms < best_ms:
+            best, best_ms = dict(p), ms
+
+    if multi:
+        axes = (("ms_compact_l2_div", MS_L2_DIV), ("ms_compact_min_deg", MS_MIN_DEG), ("alpha", ALPHAS),
+                ("beta", BETAS))
+    else:
+        axes = (("ctas_per_sm", CTAS), ("giant_edges", GIANT), ("pull_gather_ratio", GATHER), ("alpha", ALPHAS),
+                ("beta", BETAS))
+    for name, values in axes:
+        for v in values:
+            if v != best[name]:
+                trial(dict(best, **{name: v}))
+    eng.tune(**best)
+    if _engine_checksum(eng, sources, multi) != ref_sum:
+        eng.tune(**start)
+        raise RuntimeError("tuned engine parameters changed the depths")
+    return {"params": best, "ms": best_ms, "default_ms": default_ms,
+            "default_spread_ms": [min(runs), max(runs)], "tried": tried, "seconds": time.time() - t0,
+            "gain_beyond_noise": best_ms < min(runs) - (max(runs) - min(runs))}

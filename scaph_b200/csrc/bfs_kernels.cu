@@ -322,14 +322,15 @@ __device__ __forceinline__ void push_body(const GraphDev &g, const BfsDev &s, ui
                     st = pd.base + 3ull * pd.nodenum + pos;
                     t.headers++;
                     t.inspected += len;
-                    if (len > kGiantEdges) {
-                        const uint32_t nch = (len + kGiantEdges - 1) / kGiantEdges;
+                    const uint32_t ge = s.giant_edges ? s.giant_edges : kGiantEdges;
+                    if (len > ge) {
+                        const uint32_t nch = (len + ge - 1) / ge;
                         const uint32_t at = atomicAdd(&s.ctr->giant, nch);
                         if (at + nch <= s.giant_cap) {
                             for (uint32_t c = 0; c < nch; c++) {
                                 GiantChunk gc;
-                                gc.start = st + (unsigned long long)c * kGiantEdges;
-                                gc.len = min(kGiantEdges, len - c * kGiantEdges);
+                                gc.start = st + (unsigned long long)c * ge;
+                                gc.len = min(ge, len - c * ge);
                                 gc.src = v;
                                 s.giant[at + c] = gc;
                             }
@@ -384,7 +385,8 @@ __device__ __forceinline__ void giant_body(const GraphDev &g, const BfsDev &s)
     ThreadAcc t;
     for (uint32_t c = blockIdx.x; c < n; c += gridDim.x) {
         const GiantChunk gc = s.giant[c];
-        if (gc.len > kGiantEdges || gc.start + gc.len > g.pool_words || gc.src >= s.V) {
+        if (gc.len > (s.giant_edges ? s.giant_edges : kGiantEdges) || gc.start + gc.len > g.pool_words ||
+            gc.src >= s.V) {
             if (threadIdx.x == 0) atomicOr(&s.ctr->error, 8u);  // corrupt chunk record
             continue;
         }
@@ -450,10 +452,33 @@ __device__ __forceinline__ void pull_body(const GraphDev &g, const BfsDev &s, ui
                 atomicOr(&fnd[(v >> 5) - tbase], bit);
             }
         };
+        // a vertex found by phase A: depth, parent, the found bitmaps, the
+        // counters and the page histograms (p < 0: page looked up here)
+        auto found = [&](uint32_t v, uint32_t par, uint32_t dv, int p) {
+            s.depth[v] = s.level + 1;
+            if (s.parent) s.parent[v] = par;
+            mark_found(v);
+            t.next++;
+            t.next_edges += dv;
+            if (s.page_nodes) {
+                if (p < 0 || !hist_same) p = hist_same ? lut.of(v) : page_of(s.hg, v);
+                hist_add(sm, s, p, dv + 3);
+            }
+            hist_in_add(sm, s, v);
+        };
+        // phase B needs where vertex v's in-list lives (false: page missing)
+        auto list_start = [&](uint32_t v, int &p, unsigned long long &st) -> bool {
+            p = lut.of(v);
+            const PageDev pd = lut.pages[p];
+            if (pd.base == kNotResident) {
+                atomicOr(&s.ctr->error, 4u);
+                return false;
+            }
+            st = pd.base + 3ull * pd.nodenum + g.pool[pd.base + 3ull * (v - pd.left) + 1];
+            t.headers++;
+            return true;
+        };
         for (uint32_t c0 = 0; c0 < total; c0 += kPPT * BLOCK) {
-            // ---- phase A: kPPT unvisited vertices per thread, all
-            // their row (or header and first in-edge) loads issued before
-            // any of their frontier probes
             uint32_t vv[kPPT], len[kPPT], need[kPPT], dg[kPPT];
             unsigned long long st[kPPT];
             int p[kPPT];
@@ -467,93 +492,130 @@ __device__ __forceinline__ void pull_body(const GraphDev &g, const BfsDev &s, ui
                 len[i] = 0;
                 need[i] = 0;
                 st[i] = 0;
-                p[i] = 0;
+                p[i] = -1;
                 ok[i] = k < total;
 #pragma unroll
                 for (uint32_t j = 0; j < kPullSerial; j++) u[i][j] = 0xFFFFFFFFu;
-                if (!ok[i]) continue;
-                const uint32_t v = q[k];
-                vv[i] = v;
-                dg[i] = __ldg(&s.degree[v]);  // travels with the row loads (needed if v is found)
-                if (s.head) {
-                    // dense rows: the in-degree and the first in-edges of
-                    // consecutive vertices, independent coalesced loads; the
-                    // page is read only if these do not decide
-                    len[i] = __ldg(&s.indeg[v]);
-                    const uint4 h = ld_nc_v4(s.head + (size_t)kPullHead * v);
-                    u[i][0] = h.x;
+                if (ok[i]) vv[i] = q[k];
+            }
+            if (s.prec) {
+                // ---- phase A from the 8-byte records: the top-ranked
+                // in-neighbour settles most vertices (frontier hubs), and the
+                // in-degree field ends those with no other in-edge; only the
+                // rest read the in-degree and the row of ranked in-neighbours
+                uint2 rec[kPPT];
+#pragma unroll
+                for (int i = 0; i < kPPT; i++) rec[i] = ok[i] ? ld_nc_v2(s.prec + vv[i]) : make_uint2(0xFFFFFFFFu, 0u);
+                bool slow[kPPT];
+#pragma unroll
+                for (int i = 0; i < kPPT; i++) {
+                    slow[i] = false;
+                    if (!ok[i]) continue;
+                    const uint32_t h0 = rec[i].x, nin = rec[i].y >> 28;
+                    dg[i] = rec[i].y & kPrecDegMax;
+                    if (h0 < s.V && test_bit(s.front, h0)) {
+                        t.inspected += 1;
+                        found(vv[i], h0, dg[i] == kPrecDegMax ? __ldg(&s.degree[vv[i]]) : dg[i], -1);
+                    } else if (nin <= 1) {
+                        t.inspected += nin;
+                    } else {
+                        slow[i] = true;
+                    }
+                }
+#pragma unroll
+                for (int i = 0; i < kPPT; i++) {
+                    if (!slow[i]) continue;
+                    len[i] = __ldg(&s.indeg[vv[i]]);
+                    const uint4 h = ld_nc_v4(s.head + (size_t)kPullHead * vv[i]);
                     u[i][1] = h.y;
                     u[i][2] = h.z;
                     u[i][3] = h.w;
-                } else {
-                    p[i] = lut.of(v);
-                    const PageDev pd = lut.pages[p[i]];
-                    if (pd.base != kNotResident) {
-                        const uint32_t *node = g.pool + pd.base + 3ull * (v - pd.left);
-                        len[i] = node[2];
-                        st[i] = pd.base + 3ull * pd.nodenum + node[1];
-                        t.headers++;
-#pragma unroll
-                        for (uint32_t j = 0; j < kPullSerial; j++)
-                            u[i][j] = j < len[i] ? __ldg(&g.pool[st[i] + j]) : 0xFFFFFFFFu;
-                    } else {
-                        atomicOr(&s.ctr->error, 4u);
-                        ok[i] = false;
-                    }
+                    if (dg[i] == kPrecDegMax) dg[i] = __ldg(&s.degree[vv[i]]);
                 }
-            }
 #pragma unroll
-            for (int i = 0; i < kPPT; i++) {
-                if (!ok[i]) continue;
-                const uint32_t v = vv[i];
-                uint32_t hit = 0;
-#if SCAPH_PULL_FIRST_PROBE
-                // ranked rows: the top in-neighbour alone first (it settles
-                // most vertices), the other three only on a miss
-                if (s.head_ranked) {
-                    if (u[i][0] < s.V && test_bit(s.front, u[i][0])) hit = 1u;
-                    else {
+                for (int i = 0; i < kPPT; i++) {
+                    if (!slow[i]) continue;
+                    uint32_t hit = 0;
 #pragma unroll
-                        for (uint32_t j = 1; j < kPullSerial; j++)
-                            if (u[i][j] < s.V && test_bit(s.front, u[i][j])) hit |= 1u << j;
-                    }
-                } else
-#endif
-                {
-#pragma unroll
-                    for (uint32_t j = 0; j < kPullSerial; j++)
+                    for (uint32_t j = 1; j < kPullSerial; j++)
                         if (u[i][j] < s.V && test_bit(s.front, u[i][j])) hit |= 1u << j;
-                }
-                if (hit) {
-                    const uint32_t j = __ffs(hit) - 1;
-                    t.inspected += j + 1;
-                    const uint32_t par = u[i][j];
-                    s.depth[v] = s.level + 1;
-                    if (s.parent) s.parent[v] = par;
-                    mark_found(v);
-                    const uint32_t dv = dg[i];
-                    t.next++;
-                    t.next_edges += dv;
-                    if (s.page_nodes) {
-                        if (s.head && hist_same) p[i] = lut.of(v);
-                        hist_add(sm, s, hist_same ? p[i] : page_of(s.hg, v), dv + 3);
+                    if (hit) {
+                        const uint32_t j = __ffs(hit) - 1;
+                        t.inspected += j + 1;
+                        found(vv[i], j == 1 ? u[i][1] : j == 2 ? u[i][2] : u[i][3], dg[i], -1);
+                    } else {
+                        t.inspected += min(len[i], kPullSerial);
+                        need[i] = len[i] > kPullSerial && list_start(vv[i], p[i], st[i]);
                     }
-                    hist_in_add(sm, s, v);
-                } else {
-                    t.inspected += min(len[i], kPullSerial);
-                    need[i] = len[i] > kPullSerial;
-                    if (need[i] && s.head) {
-                        // phase B needs where the list lives
+                }
+            } else {
+                // ---- phase A: kPPT unvisited vertices per thread, all
+                // their row (or header and first in-edge) loads issued before
+                // any of their frontier probes
+#pragma unroll
+                for (int i = 0; i < kPPT; i++) {
+                    if (!ok[i]) continue;
+                    const uint32_t v = vv[i];
+                    dg[i] = __ldg(&s.degree[v]);  // travels with the row loads (needed if v is found)
+                    if (s.head) {
+                        // dense rows: the in-degree and the first in-edges of
+                        // consecutive vertices, independent coalesced loads; the
+                        // page is read only if these do not decide
+                        len[i] = __ldg(&s.indeg[v]);
+                        const uint4 h = ld_nc_v4(s.head + (size_t)kPullHead * v);
+                        u[i][0] = h.x;
+                        u[i][1] = h.y;
+                        u[i][2] = h.z;
+                        u[i][3] = h.w;
+                    } else {
                         p[i] = lut.of(v);
                         const PageDev pd = lut.pages[p[i]];
                         if (pd.base != kNotResident) {
                             const uint32_t *node = g.pool + pd.base + 3ull * (v - pd.left);
+                            len[i] = node[2];
                             st[i] = pd.base + 3ull * pd.nodenum + node[1];
                             t.headers++;
+#pragma unroll
+                            for (uint32_t j = 0; j < kPullSerial; j++)
+                                u[i][j] = j < len[i] ? __ldg(&g.pool[st[i] + j]) : 0xFFFFFFFFu;
                         } else {
                             atomicOr(&s.ctr->error, 4u);
-                            need[i] = 0;
+                            ok[i] = false;
                         }
+                    }
+                }
+#pragma unroll
+                for (int i = 0; i < kPPT; i++) {
+                    if (!ok[i]) continue;
+                    const uint32_t v = vv[i];
+                    uint32_t hit = 0;
+#if SCAPH_PULL_FIRST_PROBE
+                    // ranked rows: the top in-neighbour alone first (it settles
+                    // most vertices), the other three only on a miss
+                    if (s.head_ranked) {
+                        if (u[i][0] < s.V && test_bit(s.front, u[i][0])) hit = 1u;
+                        else {
+#pragma unroll
+                            for (uint32_t j = 1; j < kPullSerial; j++)
+                                if (u[i][j] < s.V && test_bit(s.front, u[i][j])) hit |= 1u << j;
+                        }
+                    } else
+#endif
+                    {
+#pragma unroll
+                        for (uint32_t j = 0; j < kPullSerial; j++)
+                            if (u[i][j] < s.V && test_bit(s.front, u[i][j])) hit |= 1u << j;
+                    }
+                    if (hit) {
+                        const uint32_t j = __ffs(hit) - 1;
+                        t.inspected += j + 1;
+                        static_assert(kPullSerial == 4, "the parent select below names four probes");
+                        const uint32_t par = j == 0 ? u[i][0] : j == 1 ? u[i][1] : j == 2 ? u[i][2] : u[i][3];
+                        found(v, par, dg[i], s.head ? -1 : p[i]);
+                    } else {
+                        t.inspected += min(len[i], kPullSerial);
+                        need[i] = len[i] > kPullSerial;
+                        if (need[i] && s.head) need[i] = list_start(v, p[i], st[i]);
                     }
                 }
             }
@@ -873,7 +935,7 @@ __global__ void k_decide(BfsGraphArgs a, DecideArgs d, cudaGraphConditionalHandl
         const uint32_t src = c->src;
         const unsigned long long src_dead = (d.dead_bm[src >> 5] >> (src & 31)) & 1u;
         const unsigned long long unv = (unsigned long long)d.V - d.dead - c->vis_n + src_dead;
-        c->pull_gather = unv * kPullGatherRatio < d.V ? 1u : 0u;
+        c->pull_gather = unv * d.gather_ratio < d.V ? 1u : 0u;
     }
     c->level = L + 1;
     cudaGraphSetConditional(h_loop, 1);
@@ -959,7 +1021,7 @@ __global__ void __launch_bounds__(64) k_decide_learned(BfsGraphArgs a, DecideArg
         for (int j = 0; j < 64; j++) y += bf(h2[j]) * bf(W3[(size_t)j * net.out]);
         const int nd = d.mode == 1 ? 0 : d.mode == 2 ? 1 : s_guard >= 0 ? s_guard : (y > 0.f ? 1 : 0);
         c->dir = nd;
-        c->pull_gather = s_unv * kPullGatherRatio < d.V ? 1u : 0u;
+        c->pull_gather = s_unv * d.gather_ratio < d.V ? 1u : 0u;
         c->level = L + 1;
         cudaGraphSetConditional(h_loop, 1);
     }

@@ -14,6 +14,14 @@ namespace scaph {
 int set_error(int code, const char *fmt, ...);
 void clear_error();
 
+// Host-side fault injection (scaph_fault_inject): the call sites below ask
+// injected_fault() before their CUDA call; while an injection is armed for
+// the site, the call is not made and the site's CUDA error is returned
+// instead, as if the runtime had failed.
+enum FaultSite { kFaultPinnedAlloc = 0, kFaultHostRegister, kFaultPageCopy, kFaultDeviceAlloc, kFaultSites };
+// cudaSuccess (no injection) or the error to report for this call.
+int injected_fault(FaultSite site);
+
 // Splitmix64 finaliser: a counter-based hash, so that generated graphs do not
 // depend on the number of threads used.
 static inline uint64_t mix64(uint64_t x)

@@ -12,7 +12,7 @@ constexpr uint32_t kNoParent = 0xFFFFFFFFu;
 constexpr int kHistCap = 512;           // pages histogrammed in shared memory
 constexpr int kLutPages = 512;          // page-table entries staged in shared memory
 constexpr int kLutCoarse = 1024;        // coarse-index entries staged in shared memory
-constexpr uint32_t kGiantEdges = 1024;  // push: adjacency longer than this is split
+constexpr uint32_t kGiantEdges = 1024;  // push: adjacency longer than this is split (default)
 constexpr int kMaxLevels = 4096;        // hard cap on BFS levels per run
 
 // One page of the device page table.  `base` is the word offset of the page's
@@ -81,6 +81,10 @@ struct BfsDev {
     const uint32_t *indeg;
     uint32_t head_ranked;      // head rows are not the list's first edges:
                                // phase B scans the whole list
+    // pull: one 8-byte record per vertex read first by phase A (null: phase
+    // A reads the in-degree and head row directly): x = the top-ranked
+    // in-neighbour (head row entry 0), y = pull_meta(in-degree, out-degree)
+    const uint2 *prec;
     // histogram of the discovered vertices over the IN-edge graph's pages
     // (count, sum(indeg+3)): keeps the pull-side page counts current without
     // a pass over all vertices (directed graphs; null when not wanted)
@@ -88,10 +92,22 @@ struct BfsDev {
     uint32_t *page_datas_in;
     GraphDev hgi;
     uint32_t pull_gather;      // sparse pull level: gather several tiles per queue
+    uint32_t giant_edges;      // push: adjacency longer than this becomes chunks (0: kGiantEdges)
 };
 
+// Second word of a pull record: the in-degree capped at 15 in the top four
+// bits (phase A needs to know only whether it exceeds the probes already
+// made), the out-degree below them; an out-degree of kPrecDegMax or more is
+// stored as kPrecDegMax and read from the degree array instead.
+constexpr uint32_t kPrecDegMax = (1u << 28) - 1;
+__host__ __device__ inline uint32_t pull_meta(uint32_t indeg, uint32_t outdeg)
+{
+    return ((indeg < 15u ? indeg : 15u) << 28) | (outdeg < kPrecDegMax ? outdeg : kPrecDegMax);
+}
+
 // A pull level gathers the vertices of several tiles into one queue when the
-// unvisited vertices are this sparse (fewer than one per kPullGatherRatio).
+// unvisited vertices are this sparse (fewer than one per kPullGatherRatio;
+// scaph_config.pull_gather_ratio overrides it).
 constexpr unsigned long long kPullGatherRatio = 64;
 
 // Graph mode: state of one traversal kept on the device, so a whole BFS runs
@@ -138,6 +154,7 @@ struct DecideArgs {
     int32_t mode;                   // SCAPH_DIR_*
     float alpha, beta;
     int32_t max_levels;
+    uint32_t gather_ratio;          // pull levels gather tiles below 1 unvisited per this many
 };
 
 // Beamer's direction-optimizing rule (SC'12): leave top-down when the
@@ -197,6 +214,8 @@ __device__ __forceinline__ uint4 ld_nc_v4(const uint32_t *p)
 {
     return __ldg(reinterpret_cast<const uint4 *>(p));
 }
+
+__device__ __forceinline__ uint2 ld_nc_v2(const uint2 *p) { return __ldg(p); }
 
 __device__ __forceinline__ uint32_t test_bit(const uint32_t *bm, uint32_t v)
 {

@@ -126,6 +126,8 @@ BfsDev scaph_engine::base_state(uint32_t *dd, uint32_t *dp) const
     s.head = d_head;
     s.indeg = d_indeg;
     s.head_ranked = head_ranked ? 1u : 0u;
+    s.prec = d_prec;
+    s.giant_edges = (uint32_t)cfg.giant_edges;
     return s;
 }
 
@@ -143,6 +145,12 @@ int scaph_engine::create(const Graph *g_, const Graph *gt_, const scaph_config *
     if (cfg.alpha <= 0) cfg.alpha = 14.0f;
     if (cfg.beta <= 0) cfg.beta = 24.0f;
     block = cfg.block_size == 128 || cfg.block_size == 512 ? cfg.block_size : 256;
+    if (cfg.giant_edges == 0) cfg.giant_edges = (int32_t)kGiantEdges;
+    if (cfg.giant_edges < 128 || cfg.giant_edges > 65536)
+        return set_error(SCAPH_EINVAL, "giant_edges %d outside 128..65536", cfg.giant_edges);
+    if (cfg.pull_gather_ratio <= 0) cfg.pull_gather_ratio = (int32_t)kPullGatherRatio;
+    if (cfg.ms_compact_l2_div <= 0) cfg.ms_compact_l2_div = 3;
+    if (cfg.ms_compact_min_deg <= 0) cfg.ms_compact_min_deg = 16;
     device = cfg.device;
     if (g->weighted) return set_error(SCAPH_EUNSUPPORTED, "BFS engine needs unweighted pages");
     if (gt && (gt->V != V || gt->E != E || gt->weighted))
@@ -187,6 +195,15 @@ int scaph_engine::create(const Graph *g_, const Graph *gt_, const scaph_config *
         head_ranked = SCAPH_PULL_HEAD == 2;
         SCAPH_CUDA(cudaMalloc(&d_head, head.size() * 4));
         SCAPH_CUDA(cudaMemcpy(d_head, head.data(), head.size() * 4, cudaMemcpyHostToDevice));
+        // the 8-byte records phase A reads first: the top-ranked in-neighbour,
+        // and the in- and out-degree in one word (pull_meta)
+        const std::vector<uint32_t> &indeg = gt ? gt->degree : g->degree;
+        std::vector<uint2> prec(V);
+        #pragma omp parallel for schedule(static)
+        for (int64_t v = 0; v < (int64_t)V; v++)
+            prec[v] = make_uint2(head[(size_t)v * kPullHead], pull_meta(indeg[v], g->degree[v]));
+        SCAPH_CUDA(cudaMalloc(&d_prec, (size_t)V * sizeof(uint2)));
+        SCAPH_CUDA(cudaMemcpy(d_prec, prec.data(), (size_t)V * sizeof(uint2), cudaMemcpyHostToDevice));
     }
 
     // vertices no edge reaches (in-degree 0) are never discovered: they start
@@ -203,6 +220,7 @@ int scaph_engine::create(const Graph *g_, const Graph *gt_, const scaph_config *
     SCAPH_CUDA(cudaMalloc(&d_dead, (size_t)nwords * 4));
     SCAPH_CUDA(cudaMemcpyAsync(d_dead, dead.data(), (size_t)nwords * 4, cudaMemcpyHostToDevice, st));
 
+    SCAPH_CUDA((cudaError_t)injected_fault(kFaultDeviceAlloc));
     SCAPH_CUDA(cudaMalloc(&d_depth, (size_t)V * 4));
     SCAPH_CUDA(cudaMalloc(&d_parent, (size_t)V * 4));
     SCAPH_CUDA(cudaMalloc(&d_visited, (size_t)nwords * 4));
@@ -215,7 +233,10 @@ int scaph_engine::create(const Graph *g_, const Graph *gt_, const scaph_config *
     SCAPH_CUDA(cudaMallocHost(&h_ctl, sizeof(BfsCtl)));
     const size_t np = g->pages.size();
     SCAPH_CUDA(cudaMalloc(&d_hist, sizeof(uint32_t) * 2 * np * kHistLevels));
-    giant_cap = (uint32_t)std::min<uint64_t>(0xFFFFFFF0u, 2 * (E / kGiantEdges) + 1024);
+    // sum of ceil(len / cut) over one level's lists of more than cut edges is
+    // at most 2 E / cut; the multi-source kernels cut at kGiantEdges
+    const uint64_t cut = std::min<uint64_t>((uint64_t)cfg.giant_edges, kGiantEdges);
+    giant_cap = (uint32_t)std::min<uint64_t>(0xFFFFFFF0u, 2 * (E / cut) + 1024);
     SCAPH_CUDA(cudaMalloc(&d_giant, sizeof(GiantChunk) * (size_t)giant_cap));
     SCAPH_CUDA(cudaEventCreate(&ev_start));
     SCAPH_CUDA(cudaEventCreate(&ev_stop));
@@ -252,6 +273,7 @@ void scaph_engine::destroy()
     pager = nullptr;
     cudaFree(d_indeg);
     cudaFree(d_head);
+    cudaFree(d_prec);
     cudaFree(d_snap);
     cudaFree(d_pcnt);
     cudaFree(d_pdatas);
@@ -283,6 +305,24 @@ void scaph_engine::destroy()
     if (own_stream && st) cudaStreamDestroy(st);
 }
 
+// The first ten scheduler features of a level (layout in scaph.h), shared
+// by the single- and multi-source loops and by k_decide_learned.
+void scaph::sched_globals(float *f, uint64_t nf, uint64_t mf, uint64_t unvis, uint64_t mu, uint32_t V, uint64_t E,
+                          int level, int prev_dir)
+{
+    auto lg = [](double x, double d) { return (float)(std::log2(1.0 + x) / d); };
+    f[0] = lg((double)nf, 32);
+    f[1] = lg((double)mf, 40);
+    f[2] = lg((double)unvis, 32);
+    f[3] = lg((double)mu, 40);
+    f[4] = (float)((double)nf / V);
+    f[5] = (float)std::min(1.0, (double)mf / std::max<uint64_t>(1, E));
+    f[6] = (float)((double)unvis / V);
+    f[7] = (float)std::min(1.0, (double)mu / std::max<uint64_t>(1, E));
+    f[8] = (float)level / 32.f;
+    f[9] = (float)prev_dir;
+}
+
 // Scheduler features of the coming level (layout in scaph.h): 16 globals,
 // then the frontier's share of every out-edge page.  The frontier histogram
 // and the pull-side page counts come from the incremental copies the host
@@ -298,7 +338,10 @@ int scaph_engine::features(int level, uint32_t src, uint64_t nf, uint64_t mf, ui
     // frontier histogram over out-pages, counts then active words (level 0:
     // the source alone)
     // both read-backs land in pinned staging and wait on one synchronisation
-    if (!h_fstage) SCAPH_CUDA(cudaMallocHost(&h_fstage, sizeof(uint32_t) * 2 * (np + (size_t)npi)));
+    if (!h_fstage) {
+        SCAPH_CUDA((cudaError_t)injected_fault(kFaultPinnedAlloc));
+        SCAPH_CUDA(cudaMallocHost(&h_fstage, sizeof(uint32_t) * 2 * (np + (size_t)npi)));
+    }
     uint32_t *hh = h_fstage, *hp = h_fstage + 2 * np;
     const bool hist_inc = level > 0 && inc_hist_level == level;
     const bool hist_dev = level > 0 && level - 1 < kHistLevels && !hist_inc;
@@ -328,17 +371,7 @@ int scaph_engine::features(int level, uint32_t src, uint64_t nf, uint64_t mf, ui
     pull_cnt.assign(2 * (size_t)npi, 0);  // counts, then active words
     if (pull_inc) pull_cnt.assign(inc_pull.begin(), inc_pull.end());
     else if (pull_dev) pull_cnt.assign(hp, hp + 2 * (size_t)npi);
-    auto lg = [](double x, double d) { return (float)(std::log2(1.0 + x) / d); };
-    f[0] = lg((double)nf, 32);
-    f[1] = lg((double)mf, 40);
-    f[2] = lg((double)unvis, 32);
-    f[3] = lg((double)mu, 40);
-    f[4] = (float)((double)nf / V);
-    f[5] = (float)std::min(1.0, (double)mf / std::max<uint64_t>(1, E));
-    f[6] = (float)((double)unvis / V);
-    f[7] = (float)std::min(1.0, (double)mu / std::max<uint64_t>(1, E));
-    f[8] = (float)level / 32.f;
-    f[9] = (float)prev_dir;
+    sched_globals(f, nf, mf, unvis, mu, V, E, level, prev_dir);
     float res_out = 1.f, res_in = 1.f, res_push = 1.f, res_pull = 1.f;
     if (pager) {
         std::vector<int> push_pages, pull_pages;
@@ -370,6 +403,10 @@ int scaph_engine::run_host_loop(uint32_t src, uint32_t *dd, uint32_t *dp)
     const bool learned = cfg.direction == SCAPH_DIR_LEARNED && sched;
     const bool want_feat = learned || cfg.record_features;
     const bool dual = cfg.dual_timing && !pager;
+    // per-level page histograms (get_page_info's counts) cost a shared-memory
+    // atomic pair per discovered vertex: recorded only where something reads
+    // them (pager, learned features, record_features)
+    const bool hist_on = host_records_hist();
     SCAPH_CUDA(fill_u32(dd, unreached, V, fill_grid, st));
     if (dp) SCAPH_CUDA(fill_u32(dp, kNoParent, V, fill_grid, st));
     SCAPH_CUDA(cudaMemcpyAsync(d_visited, d_dead, (size_t)nwords * 4, cudaMemcpyDeviceToDevice, st));
@@ -380,6 +417,7 @@ int scaph_engine::run_host_loop(uint32_t src, uint32_t *dd, uint32_t *dp)
     uint32_t *bm[2] = {d_bm3, d_bm3 + nwords};
     SCAPH_CUDA(set_source(s, src, bm[0], st));
     level_h2d.clear();
+    pcie_alg = 0;
     dual_ms.clear();
     feat_log.clear();
     pull_log.clear();
@@ -495,7 +533,7 @@ int scaph_engine::run_host_loop(uint32_t src, uint32_t *dd, uint32_t *dp)
         s.next = next;
         s.ctr = d_ctr + level;
         s.level = (uint32_t)level;
-        if (level < kHistLevels) {
+        if (hist_on && level < kHistLevels) {
             s.page_nodes = d_hist + (size_t)level * 2 * np;
             s.page_datas = s.page_nodes + np;
         } else {
@@ -503,7 +541,7 @@ int scaph_engine::run_host_loop(uint32_t src, uint32_t *dd, uint32_t *dp)
         }
         {
             const uint64_t unv_now = (uint64_t)V - n_dead - vis_n + (src_dead ? 1 : 0);
-            s.pull_gather = unv_now * kPullGatherRatio < V ? 1u : 0u;
+            s.pull_gather = unv_now * (uint64_t)cfg.pull_gather_ratio < V ? 1u : 0u;
         }
         s.page_nodes_in = s.page_datas_in = nullptr;
         if (incr && d_hist_in && level < kHistLevels) {
@@ -548,6 +586,7 @@ int scaph_engine::run_host_loop(uint32_t src, uint32_t *dd, uint32_t *dp)
             } else {
                 rc = pager_needs(this, pager, run_dir, level, src, needed, datas);
             }
+            if (!rc) pcie_alg += 4 * pager_missing_words(pager, run_dir == 0 || symmetric ? 0 : 1, needed, datas);
             if (!rc) rc = pager_run_level(this, pager, run_dir, s, needed, datas);
             if (!rc && !prefetch_pages.empty() && run_dir == 0) rc = pager_prefetch(this, pager, 0, prefetch_pages);
             if (rc) return rc;
@@ -630,6 +669,7 @@ int scaph_engine::build_graph()
     dargs.alpha = cfg.alpha;
     dargs.beta = cfg.beta;
     dargs.max_levels = kMaxLevels;
+    dargs.gather_ratio = (uint32_t)cfg.pull_gather_ratio;
 
     // init (run inputs are this node's arguments, replaced per launch)
     uint32_t *depth0 = d_depth, *parent0 = nullptr, src0 = 0, unr = unreached, nclear = kMaxLevels;
@@ -805,6 +845,7 @@ int scaph_engine::collect(bool from_graph)
         last_stats.zc_bytes = zc;
         last_stats.page_faults = f;
         last_stats.prefetched = pf;
+        last_stats.pcie_alg_bytes = pcie_alg;
     }
     pending = false;
     if (err) return set_error(SCAPH_EDEVICE, "level kernel reported error flags 0x%x", err);
@@ -824,7 +865,7 @@ int scaph_engine::bfs(uint32_t src, uint32_t *depths, uint32_t *parents, int out
     pending_src = src;
     pending_parent = dp != nullptr;
     const bool use_graph = graph_mode();
-    last_hist = !use_graph || graph_records_hist();
+    last_hist = use_graph ? graph_records_hist() : host_records_hist();
     SCAPH_CUDA(cudaEventRecord(ev_start, st));
     int rc = use_graph ? launch_graph(src, dd, dp) : run_host_loop(src, dd, dp);
     if (rc) return rc;
@@ -959,6 +1000,41 @@ int scaph_bfs_pull_pages(scaph_engine *e, int level, uint32_t *cnt, uint32_t *da
     return n;
 }
 
+int scaph_engine_tune(scaph_engine *e, const scaph_config *c)
+{
+    clear_error();
+    if (!e || !c) return set_error(SCAPH_EINVAL, "null argument");
+    const int ge = c->giant_edges ? c->giant_edges : (int)kGiantEdges;
+    if (ge < 128 || ge > 65536) return set_error(SCAPH_EINVAL, "giant_edges %d outside 128..65536", ge);
+    if (c->block_size && c->block_size != 128 && c->block_size != 256 && c->block_size != 512)
+        return set_error(SCAPH_EINVAL, "block_size %d not 128, 256 or 512", c->block_size);
+    SCAPH_CUDA(cudaSetDevice(e->device));
+    SCAPH_CUDA(cudaStreamSynchronize(e->st));
+    e->drop_graph();  // the graph bakes in grid sizes and decision arguments
+    scaph_config &k = e->cfg;
+    k.alpha = c->alpha > 0 ? c->alpha : 14.0f;
+    k.beta = c->beta > 0 ? c->beta : 24.0f;
+    k.giant_edges = ge;
+    k.pull_gather_ratio = c->pull_gather_ratio > 0 ? c->pull_gather_ratio : (int32_t)kPullGatherRatio;
+    k.ms_compact_l2_div = c->ms_compact_l2_div > 0 ? c->ms_compact_l2_div : 3;
+    k.ms_compact_min_deg = c->ms_compact_min_deg > 0 ? c->ms_compact_min_deg : 16;
+    k.ctas_per_sm = c->ctas_per_sm;
+    e->block = c->block_size ? c->block_size : 256;
+    const int occ_push = std::max(1, level_occupancy(0, e->block)), occ_pull = std::max(1, level_occupancy(1, e->block));
+    e->grid_push = k.ctas_per_sm > 0 ? k.ctas_per_sm * e->num_sms : occ_push * e->num_sms;
+    e->grid_pull = k.ctas_per_sm > 0 ? k.ctas_per_sm * e->num_sms : occ_pull * e->num_sms;
+    const uint64_t cut = std::min<uint64_t>((uint64_t)ge, kGiantEdges);
+    const uint32_t cap = (uint32_t)std::min<uint64_t>(0xFFFFFFF0u, 2 * (e->E / cut) + 1024);
+    if (cap > e->giant_cap) {
+        cudaFree(e->d_giant);
+        e->d_giant = nullptr;
+        e->giant_cap = 0;
+        SCAPH_CUDA(cudaMalloc(&e->d_giant, sizeof(scaph::GiantChunk) * (size_t)cap));
+        e->giant_cap = cap;
+    }
+    return SCAPH_OK;
+}
+
 int scaph_engine_evict_all(scaph_engine *e)
 {
     if (!e) return set_error(SCAPH_EINVAL, "null engine");
@@ -999,7 +1075,7 @@ int scaph_bfs_page_hist(scaph_engine *e, int level, uint32_t *nodes, uint32_t *d
     const int np = (int)e->g->pages.size();
     if (npages < np) return set_error(SCAPH_EINVAL, "need %d pages", np);
     if (!e->last_hist)
-        return set_error(SCAPH_EUNSUPPORTED, "graph-mode runs record page histograms only with record_features "
+        return set_error(SCAPH_EUNSUPPORTED, "resident runs record page histograms only with record_features "
                                              "or the learned direction");
     // histogram slot L holds the frontier discovered BY level L, i.e. the
     // frontier AT level L+1 (level 0's frontier is the source alone)
@@ -1019,7 +1095,7 @@ int scaph_bfs_page_hist(scaph_engine *e, int level, uint32_t *nodes, uint32_t *d
 void *scaph_host_alloc(size_t bytes)
 {
     void *p = nullptr;
-    if (cudaMallocHost(&p, bytes) != cudaSuccess) {
+    if (injected_fault(kFaultPinnedAlloc) != cudaSuccess || cudaMallocHost(&p, bytes) != cudaSuccess) {
         set_error(SCAPH_ENOMEM, "cudaMallocHost(%zu)", bytes);
         return nullptr;
     }

@@ -65,7 +65,8 @@ int pager_prefetch(scaph_engine *e, Pager *pg, int gid, const std::vector<int> &
 // Pages of graph gid holding set bits of `bits` (invert: clear bits), with
 // their words sum(deg*ew+3); synchronises st.
 int pager_page_counts(Pager *pg, int gid, const uint32_t *bits, bool invert, const uint32_t *deg, uint32_t ew,
-                      int grid, cudaStream_t st, std::vector<int> &needed, std::vector<uint32_t> &datas);
+                      int grid, cudaStream_t st, std::vector<int> &needed, std::vector<uint32_t> &datas,
+                      std::vector<uint32_t> *counts = nullptr);
 void pager_counters(const Pager *pg, uint64_t *h2d, uint64_t *zc, uint64_t *faults, uint64_t *prefetched,
                     uint64_t *hits, uint64_t *level_h2d);
 void pager_reset_counters(Pager *pg);
@@ -74,6 +75,11 @@ int pager_nslots(const Pager *pg);
 // Slots holding no page.
 int pager_free_slots(const Pager *pg);
 float pager_resident_fraction(const Pager *pg, int gid, const std::vector<int> *pages);
+// Active words sum(deg*ew+3) of the needed pages that are not resident: the
+// least a level must bring over the link (get_page_info's `datas`,
+// src/gpu_engine.cuh:413-419, over the pages the pool lacks).
+uint64_t pager_missing_words(const Pager *pg, int gid, const std::vector<int> &needed,
+                             const std::vector<uint32_t> &datas);
 // Page traffic (ms at the measured PCIe bandwidth) a level would cause on
 // graph gid: per page with cnt > 0, nothing if resident, its active words
 // if sparse enough for zero-copy reads, else a full page copy.
@@ -83,6 +89,8 @@ cudaError_t page_unvisited(const GraphDev &g, const uint32_t *visited, const uin
                            uint32_t *datas, int grid, cudaStream_t st);
 cudaError_t page_counts(const GraphDev &g, const uint32_t *bits, bool invert, const uint32_t *deg, uint32_t ew,
                         uint32_t *cnt, uint32_t *datas, int grid, cudaStream_t st);
+void sched_globals(float *f, uint64_t nf, uint64_t mf, uint64_t unvis, uint64_t mu, uint32_t V, uint64_t E, int level,
+                   int prev_dir);
 int mlp_forward_device(scaph_mlp *m, const float *hX, int n, float *hY);
 int mlp_dims(const scaph_mlp *m, int *in, int *out);
 int mlp_device_view(const scaph_mlp *m, MlpDev *v);
@@ -147,8 +155,10 @@ struct scaph_engine {
     scaph::Pager *pager = nullptr;  // out-of-core mode: pool smaller than the graph
     uint32_t *d_indeg = nullptr;    // in-degree per vertex (pull page statistics)
     uint32_t *d_head = nullptr;     // kPullHead in-edges per vertex (pull phase A)
+    uint2 *d_prec = nullptr;        // 8-byte pull record per vertex (pull phase A)
     bool head_ranked = false;       // d_head holds the top in-neighbours by out-degree
     std::vector<uint64_t> level_h2d;  // page bytes copied per level of the last run
+    uint64_t pcie_alg = 0;            // algorithmic link bytes of the last run
     scaph_bfs_stats pager_stats{};
     // learned scheduler / training traces
     scaph_mlp *sched = nullptr;
@@ -171,6 +181,9 @@ struct scaph_engine {
     {
         return (cfg.direction == SCAPH_DIR_LEARNED && sched) || cfg.record_features;
     }
+    // the host loop also needs them out of core (the pager reads the pages
+    // holding the frontier from them)
+    bool host_records_hist() const { return pager != nullptr || graph_records_hist(); }
     // incremental page counts of the learned host loop (out of core)
     uint32_t *d_hist_in = nullptr;  // [kHistLevels][2][in-pages]: discoveries by in-page
     uint32_t *h_inc = nullptr;      // pinned read-back of a level's histograms

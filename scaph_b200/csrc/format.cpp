@@ -8,6 +8,7 @@
 #include <sys/stat.h>
 
 #include <algorithm>
+#include <atomic>
 #include <functional>
 #include <cstdlib>
 #include <cstring>
@@ -31,6 +32,25 @@ int set_error(int code, const char *fmt, ...)
 }
 
 void clear_error() { g_last_error.clear(); }
+
+namespace {
+struct FaultArm {
+    std::atomic<int> skip{0}, count{0};
+};
+FaultArm g_faults[kFaultSites];
+const char *const kFaultNames[kFaultSites] = {"pinned_alloc", "host_register", "page_copy", "device_alloc"};
+const int kFaultErrors[kFaultSites] = {(int)cudaErrorMemoryAllocation, (int)cudaErrorHostMemoryAlreadyRegistered,
+                                       (int)cudaErrorUnknown, (int)cudaErrorMemoryAllocation};
+}  // namespace
+
+int injected_fault(FaultSite site)
+{
+    FaultArm &f = g_faults[site];
+    if (f.count.load(std::memory_order_relaxed) <= 0) return (int)cudaSuccess;
+    if (f.skip.load(std::memory_order_relaxed) > 0 && f.skip.fetch_sub(1) > 0) return (int)cudaSuccess;
+    if (f.count.fetch_sub(1) <= 0) return (int)cudaSuccess;
+    return kFaultErrors[site];
+}
 
 uint32_t *alloc_words(size_t words)
 {
@@ -198,6 +218,24 @@ extern "C" {
 
 const char *scaph_last_error(void) { return g_last_error.c_str(); }
 const char *scaph_version(void) { return "scaph-b200 0.1 (sm_100a)"; }
+
+int scaph_fault_inject(const char *site, int skip, int count)
+{
+    if (!site) {
+        for (auto &f : g_faults) {
+            f.count.store(0);
+            f.skip.store(0);
+        }
+        return SCAPH_OK;
+    }
+    for (int i = 0; i < kFaultSites; i++) {
+        if (strcmp(site, kFaultNames[i]) != 0) continue;
+        g_faults[i].skip.store(skip > 0 ? skip : 0);
+        g_faults[i].count.store(count > 0 ? count : 0);
+        return SCAPH_OK;
+    }
+    return set_error(SCAPH_EINVAL, "unknown fault site '%s'", site);
+}
 
 int scaph_csr_from_arrays(uint32_t V, uint64_t E, const uint64_t *idx, const uint32_t *ngh,
                           const uint32_t *wgh, scaph_csr *out)

@@ -32,6 +32,7 @@ struct MsState {
     size_t out_words = 0;
     std::vector<scaph_level_trace> trace;
     std::vector<uint64_t> h2d;  // out of core: page bytes copied or read zero-copy per level
+    uint32_t *d_pc = nullptr, *h_pc = nullptr;  // resident page census: counts then words, per graph
 };
 
 void ms_release(MsState *m)
@@ -53,6 +54,8 @@ void ms_release(MsState *m)
     cudaFreeHost(m->h_ctr);
     cudaFree(m->d_src);
     cudaFree(m->out);
+    cudaFree(m->d_pc);
+    cudaFreeHost(m->h_pc);
     delete m;
 }
 
@@ -100,29 +103,64 @@ int ms_alloc(scaph_engine *e, int nw)
     SCAPH_CUDA(cudaMalloc(&m->d_src, sizeof(uint32_t) * SCAPH_MSBFS_MAX));
     SCAPH_CUDA(cudaMalloc(&m->d_ctr, sizeof(MsCounters) * kMaxLevels));
     SCAPH_CUDA(cudaMallocHost(&m->h_ctr, sizeof(MsCounters) * kMaxLevels));
+    const size_t npmax = std::max(e->g->pages.size(), e->gt ? e->gt->pages.size() : 0) + 1;
+    SCAPH_CUDA(cudaMalloc(&m->d_pc, 2 * npmax * 4));
+    SCAPH_CUDA(cudaMallocHost(&m->h_pc, 2 * npmax * 4));
     return SCAPH_OK;
 }
 
 }  // namespace
 
-// Page traffic (ms) a push over `act` and a pull over `inc` would cause.
-static int ms_transfer_ms(scaph_engine *e, const uint32_t *act, const uint32_t *inc, int grid, double &t_push,
-                          double &t_pull)
+// Page census of one multi-source level: the out-pages holding frontier
+// vertices (what a push reads) and the in-pages holding incomplete vertices
+// (what a pull reads), with counts and active words sum(deg+3).
+struct MsLevelPages {
+    std::vector<int> push_need, pull_need;
+    std::vector<uint32_t> push_datas, pull_datas, push_cnt, pull_cnt;
+    uint64_t incomplete = 0;
+};
+
+// Resident graphs count on the engine's own buffers; out of core the pager
+// counts (and later reuses the result for the level it runs).
+static int ms_level_pages(scaph_engine *e, const uint32_t *act, const uint32_t *inc, int grid, MsLevelPages &lp)
 {
     const int gin = e->symmetric ? 0 : 1;
     for (int d = 0; d < 2; d++) {
-        std::vector<int> need;
-        std::vector<uint32_t> datas;
-        const int gid = d == 0 ? 0 : gin;
-        int rc = pager_page_counts(e->pager, gid, d == 0 ? act : inc, false,
-                                   d == 0 || !e->d_indeg ? e->d_degree : e->d_indeg, 1, grid, e->st, need, datas);
-        if (rc) return rc;
-        std::vector<uint32_t> cnt(datas.size(), 0);
-        for (int p : need) cnt[p] = 1;
-        (d == 0 ? t_push : t_pull) =
-            pager_transfer_ms(e->pager, gid, cnt.data(), datas.data(), (int)cnt.size(), e->cfg.compact_threshold);
+        const uint32_t *bits = d == 0 ? act : inc;
+        const uint32_t *deg = d == 0 || !e->d_indeg ? e->d_degree : e->d_indeg;
+        std::vector<int> &need = d == 0 ? lp.push_need : lp.pull_need;
+        std::vector<uint32_t> &datas = d == 0 ? lp.push_datas : lp.pull_datas;
+        std::vector<uint32_t> &cnt = d == 0 ? lp.push_cnt : lp.pull_cnt;
+        if (e->pager) {
+            int rc = pager_page_counts(e->pager, d == 0 ? 0 : gin, bits, false, deg, 1, grid, e->st, need, datas, &cnt);
+            if (rc) return rc;
+        } else {
+            const GraphDev &gv = d == 0 ? e->dout.view : e->gin();
+            const int np = (int)gv.npages;
+            MsState *m = e->ms;
+            SCAPH_CUDA(page_counts(gv, bits, false, deg, 1, m->d_pc, m->d_pc + np, grid, e->st));
+            SCAPH_CUDA(cudaMemcpyAsync(m->h_pc, m->d_pc, 2ull * np * 4, cudaMemcpyDeviceToHost, e->st));
+            SCAPH_CUDA(cudaStreamSynchronize(e->st));
+            cnt.assign(m->h_pc, m->h_pc + np);
+            datas.assign(m->h_pc + np, m->h_pc + 2 * np);
+            need.clear();
+            for (int p = 0; p < np; p++)
+                if (cnt[p]) need.push_back(p);
+        }
     }
+    lp.incomplete = 0;
+    for (uint32_t c : lp.pull_cnt) lp.incomplete += c;
     return SCAPH_OK;
+}
+
+// Page traffic (ms at the link bandwidth) of a push and of a pull level.
+static void ms_transfer_ms(scaph_engine *e, const MsLevelPages &lp, double &t_push, double &t_pull)
+{
+    const int gin = e->symmetric ? 0 : 1;
+    t_push = pager_transfer_ms(e->pager, 0, lp.push_cnt.data(), lp.push_datas.data(), (int)lp.push_cnt.size(),
+                               e->cfg.compact_threshold);
+    t_pull = pager_transfer_ms(e->pager, gin, lp.pull_cnt.data(), lp.pull_datas.data(), (int)lp.pull_cnt.size(),
+                               e->cfg.compact_threshold);
 }
 
 // One out-of-core level: push sends from the pages holding frontier
@@ -130,15 +168,21 @@ static int ms_transfer_ms(scaph_engine *e, const uint32_t *act, const uint32_t *
 // then one finalize; pull reads the in-pages holding incomplete vertices.
 template <int NW>
 static int ms_ooc_level(scaph_engine *e, const MsDev &s, int dir, int level, int grid, uint64_t &launches,
-                        std::vector<uint64_t> &h2d)
+                        std::vector<uint64_t> &h2d, const MsLevelPages *lp)
 {
     cudaStream_t st = e->st;
     const int gid = (dir == 0 || e->symmetric) ? 0 : 1;
     std::vector<int> needed;
     std::vector<uint32_t> datas;
-    int rc = pager_page_counts(e->pager, gid, dir == 0 ? s.act_cur : s.inc, false,
+    int rc = SCAPH_OK;
+    if (lp) {
+        needed = dir == 0 ? lp->push_need : lp->pull_need;
+        datas = dir == 0 ? lp->push_datas : lp->pull_datas;
+    } else {
+        rc = pager_page_counts(e->pager, gid, dir == 0 ? s.act_cur : s.inc, false,
                                dir == 0 || !e->d_indeg ? e->d_degree : e->d_indeg, 1, grid, st, needed, datas);
-    if (rc) return rc;
+        if (rc) return rc;
+    }
     PageLaunch fn;
     fn.run = [&](const GraphDev &gv, int, const RangeList &rl, uint32_t, cudaStream_t cs) -> int {
         if (dir == 0) {
@@ -153,6 +197,7 @@ static int ms_ooc_level(scaph_engine *e, const MsDev &s, int dir, int level, int
         SCAPH_CUDA(cudaGetLastError());
         return SCAPH_OK;
     };
+    e->pcie_alg += 4 * pager_missing_words(e->pager, gid, needed, datas);
     uint64_t h0, z0, f0, pf, hits, lh;
     pager_counters(e->pager, &h0, &z0, &f0, &pf, &hits, &lh);
     if ((rc = pager_run_level(e->pager, gid, needed, datas, e->cfg.compact_threshold, fn, st))) return rc;
@@ -224,20 +269,85 @@ static int ms_run(scaph_engine *e, const uint32_t *srcs, int nsrc, uint32_t *out
     m->trace.clear();
     m->h2d.clear();
     if (e->pager) pager_reset_counters(e->pager);
+    e->pcie_alg = 0;
+    // The learned scheduler (SCAPH_DIR_LEARNED with a network set): before
+    // every level the same feature row as the single-source loop (16 globals,
+    // then the frontier's share of every out-page, counted over the union of
+    // the batch's frontiers) goes through the network; it picks the direction
+    // near the alpha/beta switch point and names the out-pages that will hold
+    // frontier vertices next level, which are prefetched into free pool
+    // slots while the level runs.  Out of core the exact page traffic of
+    // either direction overrides it where one side clearly dominates.  The
+    // rows are kept (scaph_bfs_features) with record_features.
+    const bool learned = e->cfg.direction == SCAPH_DIR_LEARNED;
+    const bool net_on = learned && e->sched;
+    const bool want_feat = net_on || e->cfg.record_features;
+    const size_t np = e->g->pages.size();
+    const int feat_dim = SCAPH_SCHED_GLOBALS + (int)np;
+    std::vector<float> f(feat_dim), y;
+    e->feat_log.clear();
+    e->feat_dim = want_feat ? feat_dim : 0;
+    if (net_on) {
+        int rc = mlp_host_snapshot(e->sched, e->sched_host);
+        if (rc) return rc;
+        int in = 0, out_dim = 0;
+        mlp_dims(e->sched, &in, &out_dim);
+        y.resize(out_dim);
+    }
+    uint64_t npref = 0;
     while (nf > 0 && level < kMaxLevels && (uint64_t)level + 1 < e->unreached) {
         const uint64_t mu = e->E > done_e ? e->E - done_e : 0;
+        const int prev_dir = dir;
+        const int ab = level == 0 ? 0 : alpha_beta_next(dir, nf, prev_nf, mf, mu, V, alpha, beta);
         switch (e->cfg.direction) {
         case SCAPH_DIR_PUSH: dir = 0; break;
         case SCAPH_DIR_PULL: dir = level == 0 ? 0 : 1; break;
-        default: dir = level == 0 ? 0 : alpha_beta_next(dir, nf, prev_nf, mf, mu, V, alpha, beta); break;
+        default: dir = ab; break;
         }
-        if (e->pager && e->cfg.direction == SCAPH_DIR_LEARNED && level > 0) {
-            // the scheduler's out-of-core rule: the page traffic each
-            // direction would cause is known exactly; it overrides the
-            // kernel-time choice when one side clearly dominates
-            double tp = 0, tq = 0;
-            int rc = ms_transfer_ms(e, m->act[cur], m->inc, grid, tp, tq);
+        MsLevelPages lp;
+        const bool census = want_feat || (e->pager && learned && level > 0);
+        std::vector<int> prefetch_pages;
+        if (census) {
+            int rc = ms_level_pages(e, m->act[cur], m->inc, grid, lp);
             if (rc) return rc;
+            launches += 2;
+        }
+        if (want_feat) {
+            sched_globals(f.data(), nf, mf, lp.incomplete, mu, V, e->E, level, prev_dir);
+            float res_out = 1.f, res_in = 1.f, res_push = 1.f, res_pull = 1.f;
+            if (e->pager) {
+                const int gin = e->symmetric ? 0 : 1;
+                res_out = pager_resident_fraction(e->pager, 0, nullptr);
+                res_in = pager_resident_fraction(e->pager, gin, nullptr);
+                res_push = pager_resident_fraction(e->pager, 0, &lp.push_need);
+                res_pull = pager_resident_fraction(e->pager, gin, &lp.pull_need);
+            }
+            f[10] = res_out;
+            f[11] = res_in;
+            f[12] = res_push;
+            f[13] = res_pull;
+            f[14] = (float)ab;
+            f[15] = 1.f;
+            for (size_t p = 0; p < np; p++)
+                f[SCAPH_SCHED_GLOBALS + p] = (float)lp.push_cnt[p] / (float)std::max(1u, e->g->pages[p].nodenum);
+            e->feat_log.insert(e->feat_log.end(), f.begin(), f.end());
+        }
+        if (net_on) {
+            mlp_forward_host(e->sched_host, f.data(), y.data());
+            if (level > 0) {
+                dir = y[0] > 0.f ? 1 : 0;
+                const int sure = alpha_beta_confident(prev_dir, nf, mf, mu, V, alpha, beta);
+                if (sure >= 0) dir = sure;
+            }
+            if (e->pager)
+                for (int p = 0; p + 1 < (int)y.size() && p < (int)np; p++)
+                    if (y[1 + p] > 2.f && lp.push_cnt[p] == 0) prefetch_pages.push_back(p);
+        }
+        if (e->pager && learned && level > 0) {
+            // the exact page traffic each direction would cause overrides
+            // the kernel-time choice when one side clearly dominates
+            double tp = 0, tq = 0;
+            ms_transfer_ms(e, lp, tp, tq);
             if (tp > 2 * tq + 1.0) dir = 1;
             else if (tq > 2 * tp + 1.0) dir = 0;
         }
@@ -266,7 +376,8 @@ static int ms_run(scaph_engine *e, const uint32_t *srcs, int nsrc, uint32_t *out
         // frontier has 16+ out-edges per vertex, so that the pull looks masks
         // up many times per mask gathered (RMAT-25, 64 sources: the first
         // pull level 7.95 -> 6.19 ms; the larger frontiers after it lost)
-        const bool compact = dir == 1 && nf * NW * 8 <= l2_bytes / 3 && mf >= 16 * nf;
+        const bool compact = dir == 1 && nf * NW * 8 <= l2_bytes / (uint64_t)e->cfg.ms_compact_l2_div &&
+                             mf >= (uint64_t)e->cfg.ms_compact_min_deg * nf;
         if (compact) {
             const uint32_t nb = (e->nwords + kRankWordsPerCta - 1) / kRankWordsPerCta;
             k_ms_rank_sums<<<nb, kMsBlock, 0, st>>>(s.act_cur, e->nwords, m->rank_sums);
@@ -282,9 +393,15 @@ static int ms_run(scaph_engine *e, const uint32_t *srcs, int nsrc, uint32_t *out
             // out of core: the pages holding frontier vertices (push) or
             // incomplete vertices (pull), in batches the pager makes ready
             // (resident, zero-copy, demand copies)
-            int rc = ms_ooc_level<NW>(e, s, dir, level, grid, launches, m->h2d);
+            int rc = ms_ooc_level<NW>(e, s, dir, level, grid, launches, m->h2d, census ? &lp : nullptr);
             if (rc) return rc;
             if (dir == 0) npush++; else npull++;
+            if (!prefetch_pages.empty()) {
+                // copies into free slots on the copy streams, behind this
+                // level's kernels in the queue of the link
+                if ((rc = pager_prefetch(e, e->pager, 0, prefetch_pages))) return rc;
+                npref += prefetch_pages.size();
+            }
         } else if (dir == 0) {
             k_ms_push<NW><<<grid, kMsBlock, 0, st>>>(e->dout.view, s, whole);
             k_ms_push_giant<NW><<<grid, kMsBlock, 0, st>>>(e->dout.view, s);
@@ -352,6 +469,8 @@ static int ms_run(scaph_engine *e, const uint32_t *srcs, int nsrc, uint32_t *out
             stats->h2d_bytes = h2d;
             stats->zc_bytes = zc;
             stats->page_faults = faults;
+            stats->prefetched = pf;
+            stats->pcie_alg_bytes = e->pcie_alg;
         }
         stats->levels = level;
         stats->push_levels = npush;

@@ -235,6 +235,7 @@ int Pager::setup_graph(int gid, const Graph &g)
     G.slot_of.assign(np, -1);
     G.protect.assign(np, -1);
     if (!g.pinned) {
+        SCAPH_CUDA((cudaError_t)injected_fault(kFaultHostRegister));
         SCAPH_CUDA(cudaHostRegister(g.data, g.data_words * 4, cudaHostRegisterMapped | cudaHostRegisterPortable));
         const_cast<Graph &>(g).pinned = true;  // unregistered by ~Graph
     }
@@ -345,20 +346,29 @@ int Pager::acquire_slot(int gid, bool for_prefetch)
     return best;
 }
 
+// Copies page p of graph gid into a slot; returns the slot, -1 when no slot
+// can be had, -2 (error recorded) when the copy could not be issued.
 int Pager::load(int gid, int p, bool prefetch_only)
 {
     GState &G = gs[gid];
     const int si = acquire_slot(gid, prefetch_only);
     if (si < 0) return -1;
     Slot &s = slots[si];
-    if (s.g >= 0) gs[s.g].slot_of[s.p] = -1;
     // the copy may not overwrite the slot before the kernels that read its
     // previous page are done (a never-recorded event is already complete)
     cudaStream_t cs = cst[next_cst];
     next_cst = (next_cst + 1) % ncst;
-    cudaStreamWaitEvent(cs, s.last_use, 0);
-    cudaMemcpyAsync(pool + (size_t)si * slot_words, G.host->page(p), slot_words * 4, cudaMemcpyHostToDevice, cs);
-    cudaEventRecord(s.ready, cs);
+    cudaError_t e = cudaStreamWaitEvent(cs, s.last_use, 0);
+    if (e == cudaSuccess) e = (cudaError_t)injected_fault(kFaultPageCopy);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(pool + (size_t)si * slot_words, G.host->page(p), slot_words * 4, cudaMemcpyHostToDevice,
+                            cs);
+    if (e == cudaSuccess) e = cudaEventRecord(s.ready, cs);
+    if (e != cudaSuccess) {
+        set_error(SCAPH_ECUDA, "page %d of graph %d: copy not issued: %s", p, gid, cudaGetErrorString(e));
+        return -2;  // the slot keeps its previous page
+    }
+    if (s.g >= 0) gs[s.g].slot_of[s.p] = -1;
     s.g = gid;
     s.p = p;
     s.used = clock;
@@ -475,7 +485,9 @@ int Pager::run_level(int gid, const std::vector<int> &needed, const std::vector<
     while (i < fetch.size()) {
         std::vector<int> b;
         while (b.size() < batch && i < fetch.size()) {
-            if (load(gid, fetch[i], false) < 0) break;
+            const int si = load(gid, fetch[i], false);
+            if (si == -2) return SCAPH_ECUDA;
+            if (si < 0) break;
             b.push_back(fetch[i]);
             faults++;
             i++;
@@ -500,7 +512,9 @@ int Pager::prefetch(int gid, const std::vector<int> &pages)
     GState &G = gs[gid];
     for (int p : pages) {
         if (p < 0 || p >= (int)G.slot_of.size() || G.slot_of[p] >= 0) continue;
-        if (load(gid, p, true) < 0) break;
+        const int si = load(gid, p, true);
+        if (si == -2) return SCAPH_ECUDA;
+        if (si < 0) break;
         prefetched++;
     }
     return SCAPH_OK;
@@ -590,7 +604,8 @@ int pager_prefetch(scaph_engine *, Pager *pg, int gid, const std::vector<int> &p
 }
 
 int pager_page_counts(Pager *pg, int gid, const uint32_t *bits, bool invert, const uint32_t *deg, uint32_t ew,
-                      int grid, cudaStream_t st, std::vector<int> &needed, std::vector<uint32_t> &datas)
+                      int grid, cudaStream_t st, std::vector<int> &needed, std::vector<uint32_t> &datas,
+                      std::vector<uint32_t> *counts)
 {
     Pager::GState &G = pg->gs[gid];
     const int np = (int)G.host->pages.size();
@@ -605,6 +620,7 @@ int pager_page_counts(Pager *pg, int gid, const uint32_t *bits, bool invert, con
             needed.push_back(p);
             datas[p] = G.h_datas[p];
         }
+    if (counts) counts->assign(G.h_cnt, G.h_cnt + np);
     return SCAPH_OK;
 }
 
@@ -647,6 +663,16 @@ float pager_resident_fraction(const Pager *pg, int gid, const std::vector<int> *
     int r = 0;
     for (int s : G.slot_of) r += s >= 0 ? 1 : 0;
     return G.slot_of.empty() ? 1.f : (float)r / (float)G.slot_of.size();
+}
+
+uint64_t pager_missing_words(const Pager *pg, int gid, const std::vector<int> &needed,
+                             const std::vector<uint32_t> &datas)
+{
+    const Pager::GState &G = pg->gs[gid];
+    uint64_t w = 0;
+    for (int p : needed)
+        if (G.slot_of[p] < 0) w += datas[p];
+    return w;
 }
 
 double pager_transfer_ms(const Pager *pg, int gid, const uint32_t *cnt, const uint32_t *datas, int npages,

@@ -92,6 +92,45 @@ def collect(g: PagedGraph, gt: PagedGraph | None, sources, **engine_kw) -> list[
     return out
 
 
+def collect_ms(g: PagedGraph, gt: PagedGraph | None, batches, depth_ptr: int | None = None,
+               **engine_kw) -> list[np.ndarray]:
+    """Feature rows of multi-source traversals (one array of levels x (G+P)
+    per batch of sources): the union of the batch's frontiers, counted per
+    out-page.  They teach the page outputs what a batched frontier spreads
+    to; their direction output is not trained (the multi-source kernels'
+    costs differ from the single-source labels).  depth_ptr: a device
+    buffer of len(batch) * V words for the depths (else host memory)."""
+    eng = Engine(g, gt, record_features=1, **engine_kw)
+    out = []
+    for b in batches:
+        b = [int(x) for x in b]
+        if depth_ptr is None:
+            eng.msbfs(b)
+        else:
+            eng.msbfs_device(b, depth_ptr)
+        out.append(eng.features())
+    eng.close()
+    return out
+
+
+def ms_dataset(rows_list, n_out: int, w_page=0.5):
+    """Training rows of multi-source traces: page labels are the next row's
+    frontier pages (none after the last level); direction weight 0."""
+    Xs, Ts, Ws = [], [], []
+    for F in rows_list:
+        L = len(F)
+        nxt = np.zeros((L, n_out), np.float32)
+        if L > 1:
+            nxt[:-1] = F[1:, G:] > 0
+        T = np.concatenate([np.zeros((L, 1), np.float32), nxt], axis=1)
+        W = np.zeros_like(T)
+        W[:, 1:] = w_page / n_out
+        Xs.append(F.astype(np.float32))
+        Ts.append(T)
+        Ws.append(W)
+    return np.concatenate(Xs), np.concatenate(Ts), np.concatenate(Ws)
+
+
 def alpha_beta(cur, nf, prev_nf, mf, mu, V, alpha=14.0, beta=24.0) -> int:
     """Beamer's rule, as the engine applies it (0 push, 1 pull)."""
     if cur == 0:
@@ -231,11 +270,20 @@ def dataset(traces, nslots, page_ms, V, n_out, n_in, symmetric, w_dir=1.0, w_pag
 
 
 def train(traces, g: PagedGraph, gt: PagedGraph | None, nslots: int, page_ms: float, epochs=300, lr=3e-3,
-          seed=7, device=0, compact_threshold=3) -> tuple[Mlp, dict]:
+          seed=7, device=0, compact_threshold=3, ms_rows=None) -> tuple[Mlp, dict]:
+    """Trains the network on the single-source traces (direction and page
+    labels) and, optionally, multi-source feature rows (collect_ms: page
+    labels only)."""
     n_out, n_in = g.npages, (gt or g).npages
     zc_words = compact_threshold * (g.pagesize // 32)
     X, T, W = dataset(traces, nslots, page_ms, g.V, n_out, n_in, gt is None, zc_words=zc_words,
                       page_words=g.pagesize)
+    if ms_rows:
+        Xm, Tm, Wm = ms_dataset(ms_rows, n_out)
+        # dataset() normalised its weights by its row count; the same for these
+        W = W * len(X)
+        X, T, W = np.concatenate([X, Xm]), np.concatenate([T, Tm]), np.concatenate([W, Wm])
+        W /= len(X)
     net = Mlp(G + n_out, 1 + n_out, seed=seed, device=device)
     loss0, _ = net.loss_grad(X, T, W)
     batch = min(256, len(X))

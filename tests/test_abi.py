@@ -49,3 +49,18 @@ def test_engine_without_gpu_fails_cleanly():
     with pytest.raises(S.ScaphError) as ei:
         S.Engine(g)
     assert ei.value.code == S.ECUDA
+
+
+def test_fault_injection_sites():
+    """The host-side fault injector knows its sites and rejects others."""
+    S.fault_inject("page_copy", 0, 0)
+    S.fault_inject(None)
+    with pytest.raises(S.ScaphError) as ex:
+        S.fault_inject("no_such_site")
+    assert ex.value.code == S.EINVAL
+    # an armed pinned allocation fails with ENOMEM (here there is no GPU
+    # either, so the call fails whether armed or not)
+    S.fault_inject("pinned_alloc", 0, 1)
+    assert S.lib().scaph_host_alloc(4096) is None
+    assert b"cudaMallocHost" in S.lib().scaph_last_error()
+    S.fault_inject(None)

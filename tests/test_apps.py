@@ -130,3 +130,28 @@ def test_reference_apps_build_unchanged_against_compat(tmp_path):
     assert r.returncode == 0, r.stderr[-3000:]
     for name in ("bfs", "sssp", "wcc"):
         assert os.access(out / "ref" / name, os.X_OK)
+
+
+def test_pagerank_oracle_against_the_google_matrix():
+    """The float64 PageRank oracle equals the power iteration of the explicit
+    Google matrix (dangling vertices spread uniformly) on a small directed
+    graph, and its ranks sum to 1."""
+    csr = G.random_graph(60, 200, seed=11, symmetric=False)
+    V = csr.V
+    M = np.zeros((V, V))
+    deg = csr.degree()
+    for u in range(V):
+        nb = csr.ngh[csr.idx[u]:csr.idx[u + 1]]
+        if len(nb):
+            M[nb, u] += 1.0 / len(nb)
+        else:
+            M[:, u] = 1.0 / V
+    d = 0.85
+    Gm = d * M + (1 - d) / V
+    r = np.full(V, 1.0 / V)
+    for _ in range(30):
+        r = Gm @ r
+    got = O.pagerank(csr.idx, csr.ngh, 30, d)
+    assert np.allclose(got, r, rtol=1e-12, atol=1e-15)
+    assert abs(got.sum() - 1.0) < 1e-12
+    assert (deg == 0).any()

@@ -125,3 +125,40 @@ def test_reference_bfs_and_sssp_apps_run(graphs):
     prefix, _ = graphs["wdir"]
     _, _, out = run_app("sssp", prefix, None, f"--src={src % 20000}", "--check", ref=True)
     assert "check passed!" in out
+
+
+def run_pr(prefix, out, *args):
+    exe = os.path.join(BUILD, "pr")
+    if not os.access(exe, os.X_OK):
+        pytest.skip(f"{exe} not built")
+    cmd = [exe, f"--graphfile={prefix}", f"--out={out}"] + list(args)
+    r = subprocess.run(cmd, capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, (cmd, r.stdout[-2000:], r.stderr[-2000:])
+    m = re.search(r"pagerank iters=(\d+) l1=(\S+) ms=\S+ resident=(\d) h2d=(\d+) zc=(\d+) faults=(\d+)", r.stdout)
+    assert m, r.stdout
+    return np.fromfile(out, np.float32), dict(iters=int(m.group(1)), l1=float(m.group(2)),
+                                             resident=int(m.group(3)), h2d=int(m.group(4)), zc=int(m.group(5)))
+
+
+# float32 ranks with float32 atomic sums against the float64 power iteration
+PR_RTOL, PR_ATOL = 1e-4, 1e-8
+
+
+@pytest.mark.parametrize("name", ["sym", "dir", "wdir"])
+@pytest.mark.parametrize("memory", [None, "1"], ids=["resident", "out-of-core"])
+def test_pagerank_app(graphs, tmp_path, name, memory):
+    """PageRank on the page store (§8(f)1: the reference's app/pr.cu does not
+    build): resident and out of core, symmetric, directed and weighted pages,
+    within PR_RTOL of the float64 oracle."""
+    prefix, csr = graphs[name]
+    args = ["--iters=25"] + (["--weighted"] if name == "wdir" else [])
+    if memory:
+        args += [f"--max_memory={memory}", "--threshold=1"]
+    got, info = run_pr(prefix, tmp_path / "r", *args)
+    ref = O.pagerank(csr.idx, csr.ngh, 25, 0.85)
+    assert got.shape == ref.shape
+    assert np.allclose(got, ref, rtol=PR_RTOL, atol=PR_ATOL), float(np.max(np.abs(got - ref) / ref))
+    assert abs(float(got.astype(np.float64).sum()) - 1.0) < 1e-3
+    assert info["resident"] == (0 if memory else 1)
+    if memory:
+        assert info["h2d"] + info["zc"] > 0

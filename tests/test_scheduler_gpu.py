@@ -75,3 +75,49 @@ def test_learned_graph_mode_in_hbm_is_exact_and_matches_host_loop(setup):
         assert [t["direction"] for t in eg.trace()] == [t["direction"] for t in eh.trace()]
     eg.close()
     eh.close()
+
+
+def test_learned_multi_source_out_of_core(setup):
+    """The network inside the multi-source loop, out of core: the feature
+    rows it sees (one per level, the union of the batch's frontiers), the
+    pages it names prefetched into free slots, and depths still bit-exact."""
+    csr, g, gt, train, held = setup
+    total = g.npages + gt.npages
+    pool = int(0.6 * total) * g.pagesize * 4
+    rows = scheduler.collect_ms(g, gt, [train[:8], train[8:16]])
+    assert all(r.shape[1] == scheduler.G + g.npages for r in rows)
+    traces = scheduler.collect(g, gt, train[:6])
+    net, info = scheduler.train(traces, g, gt, int(0.6 * total), 0.5, epochs=100, ms_rows=rows)
+    assert info["loss"] < info["loss0"]
+    eng = S.Engine(g, gt, pool_bytes=pool, direction=S.DIR_LEARNED, record_features=1)
+    eng.set_scheduler(net)
+    eng.evict_all()
+    depth, st = eng.msbfs(held)
+    F = eng.features()
+    assert F.shape == (st.levels, scheduler.G + g.npages)
+    for i, s in enumerate(held):
+        assert np.array_equal(depth[i], O.bfs(csr.idx, csr.ngh, s)), f"row {i}"
+    eng.close()
+
+
+def test_multi_source_prefetch_keeps_depths(setup):
+    """A network whose page outputs are all confident: every page not in the
+    current frontier is prefetched into free slots each level; the rows stay
+    exact and the prefetch count is reported."""
+    csr, g, gt, _, held = setup
+    net = S.Mlp(scheduler.G + g.npages, 1 + g.npages, seed=5)
+    p = net.params()
+    n3 = 64 * (1 + g.npages)
+    p[-(1 + g.npages) - n3:-(1 + g.npages)] = 0.0  # W3 = 0
+    p[-(1 + g.npages):] = 5.0                      # b3: every logit 5
+    p[-(1 + g.npages)] = 0.0                       # direction logit 0
+    net.set_params(p)
+    total = g.npages + gt.npages
+    eng = S.Engine(g, gt, pool_bytes=int(0.8 * total) * g.pagesize * 4, direction=S.DIR_LEARNED)
+    eng.set_scheduler(net)
+    eng.evict_all()
+    depth, st = eng.msbfs(held)
+    assert st.prefetched > 0
+    for i, s in enumerate(held):
+        assert np.array_equal(depth[i], O.bfs(csr.idx, csr.ngh, s)), f"row {i}"
+    eng.close()
