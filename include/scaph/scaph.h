@@ -140,6 +140,20 @@ int scaph_csr_read(const char *prefix, int with_weights, scaph_csr *out);
 int scaph_pages_write(const char *prefix, const scaph_csr *csr,
                       uint32_t pagesize_words, int weighted);
 
+/* The same page files written by streaming the flat CSR files
+ * <csr_prefix>_csr.idx/.ngh (and .wgh when weighted) - the edge arrays are
+ * read one page's range at a time, never held in memory - to <out_prefix>.
+ * With SCAPH_PAGES_GROW a list longer than a page makes the page grow:
+ * pagesize becomes the smallest multiple of 4 words that holds the longest
+ * list (the reference generator and scaph_pages_write reject such a vertex,
+ * tools/pagegencsr.cpp:106-163); *pagesize_out (may be NULL) receives the
+ * page size written.  Without growth, or when every list fits, the files
+ * are byte-identical to scaph_pages_write's. */
+#define SCAPH_PAGES_GROW 1
+int scaph_pages_write_stream(const char *csr_prefix, const char *out_prefix,
+                             uint32_t pagesize_words, int weighted, int flags,
+                             uint32_t *pagesize_out);
+
 typedef struct scaph_graph scaph_graph;
 
 /* Loads a paged CSR written by pagegencsr / scaph_pages_write into host

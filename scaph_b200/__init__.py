@@ -104,6 +104,7 @@ def lib() -> C.CDLL:
         "scaph_csr_write": ([C.c_char_p, P(_Csr)], i32),
         "scaph_csr_read": ([C.c_char_p, i32, P(_Csr)], i32),
         "scaph_pages_write": ([C.c_char_p, P(_Csr), u32, i32], i32),
+        "scaph_pages_write_stream": ([C.c_char_p, C.c_char_p, u32, i32, i32, P(u32)], i32),
         "scaph_csr_export": ([C.c_char_p, i32], i32),
         "scaph_graph_open": ([C.c_char_p, i32, P(vp)], i32),
         "scaph_graph_from_csr": ([P(_Csr), u32, i32, P(vp)], i32),
@@ -296,6 +297,17 @@ class Csr:
 
     def write_pages(self, prefix: str, pagesize_words: int, weighted: bool = False) -> None:
         _check(lib().scaph_pages_write(prefix.encode(), C.byref(self._c), pagesize_words, int(weighted)))
+
+
+def pages_write_stream(csr_prefix: str, out_prefix: str, pagesize_words: int, weighted: bool = False,
+                       grow: bool = False) -> int:
+    """Pages the flat CSR files <csr_prefix>_csr.* into <out_prefix>page*,
+    reading the edges a page at a time (scaph_pages_write_stream); with grow
+    a list longer than a page enlarges the page.  Returns the page size."""
+    ps = C.c_uint32()
+    _check(lib().scaph_pages_write_stream(csr_prefix.encode(), out_prefix.encode(), pagesize_words, int(weighted),
+                                          1 if grow else 0, C.byref(ps)))
+    return ps.value
 
 
 def csr_export(prefix: str, kind: int) -> str:

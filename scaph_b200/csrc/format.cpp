@@ -344,6 +344,101 @@ int scaph_pages_write(const char *prefix, const scaph_csr *csr, uint32_t pagesiz
     return write_file(p + "graph.info", &gi, sizeof(gi));
 }
 
+// Streaming writer: the flat CSR files are read page by page (the offsets
+// whole, the edges one page's range at a time with pread), so the edge
+// arrays are never held in memory; the page cut and page contents are the
+// ones scaph_pages_write (and tools/pagegencsr.cpp:197-252) produce.
+int scaph_pages_write_stream(const char *csr_prefix, const char *out_prefix, uint32_t pagesize, int weighted,
+                             int flags, uint32_t *pagesize_out)
+{
+    clear_error();
+    if (!csr_prefix || !out_prefix) return set_error(SCAPH_EINVAL, "null argument");
+    if (flags & ~SCAPH_PAGES_GROW) return set_error(SCAPH_EINVAL, "unknown flags 0x%x", flags);
+    const std::string in(csr_prefix), outp(out_prefix);
+    const long long isz = file_size(in + "_csr.idx"), nsz = file_size(in + "_csr.ngh");
+    if (isz < 8 || isz % 4 || nsz < 0 || nsz % 4) return set_error(SCAPH_EIO, "%s_csr.idx/.ngh missing or malformed", csr_prefix);
+    const uint64_t V = (uint64_t)isz / 4 - 1;
+    if (V == 0 || V > 0xFFFFFFFEull) return set_error(SCAPH_EFORMAT, "%s_csr.idx: bad vertex count", csr_prefix);
+    std::vector<uint64_t> idx(V + 1);
+    {
+        std::vector<uint32_t> i32(V + 1);
+        int rc = read_file(in + "_csr.idx", i32.data(), (size_t)isz);
+        if (rc) return rc;
+        for (uint64_t v = 0; v <= V; v++) idx[v] = i32[v];
+    }
+    const uint64_t E = (uint64_t)nsz / 4;
+    for (uint64_t v = 0; v < V; v++)
+        if (idx[v + 1] < idx[v]) return set_error(SCAPH_EFORMAT, "%s_csr.idx not monotone at %llu", csr_prefix,
+                                                  (unsigned long long)v);
+    if (idx[0] != 0 || idx[V] != E) return set_error(SCAPH_EFORMAT, "%s_csr.idx does not span _csr.ngh", csr_prefix);
+    const uint64_t ew = weighted ? 2 : 1;
+    if (weighted && file_size(in + "_csr.wgh") != (long long)(4 * E))
+        return set_error(SCAPH_EIO, "%s_csr.wgh missing or short", csr_prefix);
+    if (flags & SCAPH_PAGES_GROW) {
+        // the page grows to hold the longest list: 3 + deg*ew < pagesize
+        uint64_t maxdeg = 0;
+        for (uint64_t v = 0; v < V; v++) maxdeg = std::max<uint64_t>(maxdeg, idx[v + 1] - idx[v]);
+        const uint64_t need = (3 + maxdeg * ew + 1 + 3) & ~3ull;
+        if (need > 0xFFFFFFF0ull) return set_error(SCAPH_EUNSUPPORTED, "a list of %llu edges", (unsigned long long)maxdeg);
+        if (need > pagesize) pagesize = (uint32_t)need;
+    }
+    scaph_csr view{};
+    view.V = (uint32_t)V;
+    view.E = E;
+    view.idx = idx.data();
+    std::vector<scaph_page_info> pages;
+    int rc = cut_pages(&view, pagesize, weighted, pages);
+    if (rc) return rc;
+    FILE *fn = fopen((in + "_csr.ngh").c_str(), "rb");
+    FILE *fw = weighted ? fopen((in + "_csr.wgh").c_str(), "rb") : nullptr;
+    if (!fn || (weighted && !fw)) {
+        if (fn) fclose(fn);
+        if (fw) fclose(fw);
+        return set_error(SCAPH_EIO, "cannot open %s_csr.ngh/.wgh", csr_prefix);
+    }
+    std::unique_ptr<uint32_t[]> buf(new (std::nothrow) uint32_t[pagesize]), eb(new (std::nothrow) uint32_t[pagesize]),
+        wb(new (std::nothrow) uint32_t[weighted ? pagesize : 1]);
+    if (!buf || !eb || !wb) rc = set_error(SCAPH_ENOMEM, "page buffers");
+    for (size_t i = 0; !rc && i < pages.size(); i++) {
+        const scaph_page_info &pi = pages[i];
+        const uint64_t base = idx[pi.left];
+        memset(buf.get(), 0, (size_t)pagesize * 4);
+        for (uint32_t v = pi.left; v <= pi.right; v++) {
+            const size_t k = (size_t)(v - pi.left) * 3;
+            buf[k + 0] = v;
+            buf[k + 1] = (uint32_t)(idx[v] - base);
+            buf[k + 2] = (uint32_t)(idx[v + 1] - idx[v]);
+        }
+        const size_t n = pi.edgenum;
+        if (n && (fseeko(fn, (off_t)(base * 4), SEEK_SET) != 0 || fread(eb.get(), 4, n, fn) != n)) {
+            rc = set_error(SCAPH_EIO, "%s_csr.ngh: short read", csr_prefix);
+            break;
+        }
+        if (n && weighted && (fseeko(fw, (off_t)(base * 4), SEEK_SET) != 0 || fread(wb.get(), 4, n, fw) != n)) {
+            rc = set_error(SCAPH_EIO, "%s_csr.wgh: short read", csr_prefix);
+            break;
+        }
+        uint32_t *edges = buf.get() + (size_t)pi.nodenum * 3;
+        for (size_t e = 0; e < n; e++) {
+            if (eb[e] >= V) {
+                rc = set_error(SCAPH_EFORMAT, "%s_csr.ngh: neighbour %u out of range", csr_prefix, eb[e]);
+                break;
+            }
+            edges[e * ew] = eb[e];
+            if (weighted) edges[e * ew + 1] = wb[e];
+        }
+        if (!rc) rc = write_file(outp + "page" + std::to_string(i), buf.get(), (size_t)pagesize * 4);
+    }
+    fclose(fn);
+    if (fw) fclose(fw);
+    if (rc) return rc;
+    if ((rc = write_file(outp + "page.info", pages.data(), pages.size() * sizeof(scaph_page_info)))) return rc;
+    struct { uint32_t pagesize, nodenum; uint64_t edgenum; } gi = {pagesize, (uint32_t)V, E};
+    if ((rc = write_file(outp + "graph.info", &gi, sizeof(gi)))) return rc;
+    if (pagesize_out) *pagesize_out = pagesize;
+    return SCAPH_OK;
+}
+
 // Validates page records against the Node triples (the reference trusts
 // them blindly; a corrupt file here is an error, not undefined behaviour).
 static int check_pages(Graph &g)

@@ -247,3 +247,24 @@ def test_bad_source_is_an_error(rmat16):
         eng.bfs(csr.V)
     assert ei.value.code == S.EINVAL
     eng.close()
+
+
+def test_grown_page_for_a_giant_vertex(tmp_path):
+    """Pages written with growth (the page enlarged to hold a list longer
+    than the requested page) run through the engine, resident and out of
+    core, with exact depths."""
+    csr = G.star(5000, center=17)
+    extra = G.random_graph(5000, 8000, seed=9)
+    csr = G.csr_from_edges(5000, np.concatenate([np.repeat(np.arange(5000), np.diff(csr.idx).astype(np.int64)),
+                                                 np.repeat(np.arange(5000), np.diff(extra.idx).astype(np.int64))]),
+                           np.concatenate([csr.ngh, extra.ngh]))
+    csr.write(str(tmp_path / "g"))
+    ps = S.pages_write_stream(str(tmp_path / "g"), str(tmp_path / "p"), 2048, grow=True)
+    assert ps > 2048
+    g = S.PagedGraph.open(str(tmp_path / "p"))
+    for pool in (0, 2 * ps * 4):
+        eng = S.Engine(g, pool_bytes=pool)
+        for src in (17, 3, 4999):
+            d, _, _ = eng.bfs(src)
+            assert np.array_equal(d, O.bfs(csr.idx, csr.ngh, src))
+        eng.close()

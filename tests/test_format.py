@@ -201,3 +201,58 @@ def test_transpose():
     a = np.sort(src.astype(np.int64) * c.V + c.ngh)
     b = np.sort(t.ngh.astype(np.int64) * c.V + tsrc)
     assert np.array_equal(a, b)
+
+
+@pytest.mark.parametrize("weighted", [False, True])
+@pytest.mark.parametrize("scale,ef,seed,pagesize", [(12, 16, 4, 1 << 12), (15, 8, 5, 1 << 16), (16, 16, 7, 1 << 20)])
+def test_streaming_writer_byte_identical(tmp_path, weighted, scale, ef, seed, pagesize):
+    """scaph_pages_write_stream (edges read from the flat files a page at a
+    time) writes the same bytes as scaph_pages_write, itself pinned to
+    tools/pagegencsr.cpp above; and, where it was built, the same bytes as
+    the reference generator run on the same flat files."""
+    csr = S.Csr.rmat(scale, ef, seed=seed)
+    if weighted:
+        rng = np.random.default_rng(seed)
+        csr = S.Csr.from_arrays(csr.idx, csr.ngh, rng.integers(1, 100, csr.E).astype(np.uint32))
+    a, b, c = tmp_path / "a", tmp_path / "b", tmp_path / "c"
+    for d in (a, b, c):
+        d.mkdir()
+    csr.write(str(c / "g"))
+    assert S.pages_write_stream(str(c / "g"), str(a / "g"), pagesize, weighted) == pagesize
+    csr.write_pages(str(b / "g"), pagesize, weighted=weighted)
+    da = _digests(a)
+    assert da == _digests(b) and len(da) >= 3
+    if os.path.exists(O.REF_PAGEGEN) and pagesize == 1 << 20:
+        subprocess.run([O.REF_PAGEGEN, str(c / "g"), "1", "w" if weighted else "u"], check=True, capture_output=True)
+        assert da == _digests(c)
+
+
+def test_streaming_writer_grows_the_page_for_a_giant_vertex(tmp_path):
+    """A list longer than the page: rejected without growth, with growth the
+    page becomes the smallest multiple of 4 words that holds it; the pages
+    read back to the same CSR."""
+    csr = G.star(3000, center=10)  # the centre has 2999 edges
+    csr.write(str(tmp_path / "g"))
+    with pytest.raises(S.ScaphError) as ei:
+        S.pages_write_stream(str(tmp_path / "g"), str(tmp_path / "p"), 2048)
+    assert ei.value.code == S.EUNSUPPORTED
+    ps = S.pages_write_stream(str(tmp_path / "g"), str(tmp_path / "p"), 2048, grow=True)
+    assert ps == (3 + 2999 + 1 + 3) // 4 * 4 and ps % 4 == 0
+    g = S.PagedGraph.open(str(tmp_path / "p"))
+    back = g.to_csr()
+    assert np.array_equal(back.idx, csr.idx) and np.array_equal(back.ngh, csr.ngh)
+    assert np.array_equal(g.degree(), csr.degree())
+
+
+def test_streaming_writer_rejects_bad_files(tmp_path):
+    csr = S.Csr.rmat(10, 8, seed=6)
+    csr.write(str(tmp_path / "g"))
+    ngh = np.fromfile(str(tmp_path / "g_csr.ngh"), np.uint32)
+    ngh[5] = 1 << 20  # neighbour out of range
+    ngh.tofile(str(tmp_path / "g_csr.ngh"))
+    with pytest.raises(S.ScaphError) as ei:
+        S.pages_write_stream(str(tmp_path / "g"), str(tmp_path / "p"), 1 << 12)
+    assert ei.value.code == S.EFORMAT
+    with pytest.raises(S.ScaphError) as ei:
+        S.pages_write_stream(str(tmp_path / "missing"), str(tmp_path / "p"), 1 << 12)
+    assert ei.value.code == S.EIO
