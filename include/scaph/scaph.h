@@ -363,6 +363,13 @@ int scaph_mlp_adam_step(scaph_mlp *m, const float *X, const float *T, const floa
 int scaph_mlp_train(scaph_mlp *m, const float *X, const float *T, const float *W, int n,
                     int epochs, int batch, float lr, uint64_t seed, float *final_loss);
 int scaph_mlp_save(const scaph_mlp *m, const char *path);
+/* Device time in microseconds (CUDA events, mean over reps) of a forward
+ * pass over n rows (out_us[0]), one training step on n rows (out_us[1]:
+ * forward, loss, backward, Adam) and the single-row inference kernel
+ * (out_us[2], the network part of the graph-mode learned decision), on zero
+ * rows already on the device.  Parameters and Adam state are left as
+ * they were. */
+int scaph_mlp_time(scaph_mlp *m, int n, int reps, float *out_us);
 int scaph_mlp_load(scaph_mlp *m, const char *path);
 
 /* Makes SCAPH_DIR_LEARNED engines use `m` (NULL: back to alpha/beta): the

@@ -133,6 +133,7 @@ def lib() -> C.CDLL:
         "scaph_mlp_adam_step": ([vp, vp, vp, vp, i32, C.c_float, P(C.c_float)], i32),
         "scaph_mlp_train": ([vp, vp, vp, vp, i32, i32, i32, C.c_float, u64, P(C.c_float)], i32),
         "scaph_mlp_save": ([vp, C.c_char_p], i32),
+        "scaph_mlp_time": ([vp, i32, i32, vp], i32),
         "scaph_mlp_load": ([vp, C.c_char_p], i32),
         "scaph_engine_set_scheduler": ([vp, vp], i32),
         "scaph_bfs_features": ([vp, vp, i32, P(i32)], i32),
@@ -424,6 +425,13 @@ class Mlp:
         _check(lib().scaph_mlp_train(self._h, _ptr(X), _ptr(T), _ptr(W), X.shape[0], epochs, batch, lr, seed,
                                      C.byref(loss)))
         return float(loss.value)
+
+    def time(self, n: int = 256, reps: int = 20) -> dict:
+        """Device microseconds (CUDA events) of a forward pass and a training
+        step over n rows, and of the single-row inference kernel."""
+        out = np.zeros(3, np.float32)
+        _check(lib().scaph_mlp_time(self._h, n, reps, _ptr(out)))
+        return {"forward_us": float(out[0]), "train_step_us": float(out[1]), "infer1_us": float(out[2]), "rows": n}
 
     def save(self, path: str) -> None:
         _check(lib().scaph_mlp_save(self._h, path.encode()))

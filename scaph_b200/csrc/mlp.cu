@@ -484,6 +484,69 @@ int scaph_mlp_adam_step(scaph_mlp *m, const float *X, const float *T, const floa
     return SCAPH_OK;
 }
 
+// Device time (CUDA events on the network's stream, mean over `reps`) of:
+// out_us[0] a forward pass over n rows, out_us[1] one training step on n
+// rows (forward, loss, backward, Adam), out_us[2] the single-row inference
+// kernel (the network part of the graph-mode learned decision).  Inputs are
+// zero rows already on the device, so no host copy is timed; the parameters
+// and Adam state are restored afterwards.
+int scaph_mlp_time(scaph_mlp *m, int n, int reps, float *out_us)
+{
+    clear_error();
+    if (!m || n < 1 || reps < 1 || !out_us) return set_error(SCAPH_EINVAL, "bad argument");
+    SCAPH_CUDA(cudaSetDevice(m->device));
+    int rc = m->ensure(n);
+    if (rc) return rc;
+    SCAPH_CUDA(cudaMemsetAsync(m->X, 0, sizeof(float) * n * m->in, m->st));
+    SCAPH_CUDA(cudaMemsetAsync(m->T, 0, sizeof(float) * n * m->out, m->st));
+    SCAPH_CUDA(cudaMemsetAsync(m->Wt, 0, sizeof(float) * n * m->out, m->st));
+    float *save = nullptr;
+    SCAPH_CUDA(cudaMalloc(&save, sizeof(float) * 3 * m->nparams));
+    SCAPH_CUDA(cudaMemcpyAsync(save, m->w, sizeof(float) * m->nparams, cudaMemcpyDeviceToDevice, m->st));
+    SCAPH_CUDA(cudaMemcpyAsync(save + m->nparams, m->m, sizeof(float) * m->nparams, cudaMemcpyDeviceToDevice, m->st));
+    SCAPH_CUDA(cudaMemcpyAsync(save + 2 * m->nparams, m->v, sizeof(float) * m->nparams, cudaMemcpyDeviceToDevice,
+                               m->st));
+    cudaEvent_t e[2];
+    SCAPH_CUDA(cudaEventCreate(&e[0]));
+    SCAPH_CUDA(cudaEventCreate(&e[1]));
+    auto timed = [&](auto &&body, float *us) -> int {
+        int r = body();  // warm
+        if (r) return r;
+        SCAPH_CUDA(cudaEventRecord(e[0], m->st));
+        for (int i = 0; i < reps && !r; i++) r = body();
+        SCAPH_CUDA(cudaEventRecord(e[1], m->st));
+        SCAPH_CUDA(cudaEventSynchronize(e[1]));
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e[0], e[1]);
+        *us = ms * 1e3f / (float)reps;
+        return r;
+    };
+    rc = timed([&]() { return m->forward(n); }, &out_us[0]);
+    if (!rc)
+        rc = timed([&]() -> int {
+            int r = m->forward(n);
+            if (r || (r = m->backward(n))) return r;
+            k_adam<<<grid_of(m->nparams), 256, 0, m->st>>>(m->w, m->g, m->m, m->v, m->nparams, 1e-3f, 0.9f, 0.999f,
+                                                           1e-8f, 0.5f, 0.5f);
+            return cudaGetLastError() == cudaSuccess ? SCAPH_OK : set_error(SCAPH_ECUDA, "adam launch");
+        }, &out_us[1]);
+    if (!rc)
+        rc = timed([&]() -> int {
+            k_forward1<<<1, 256, sizeof(float) * m->in, m->st>>>(m->w, m->in, m->out, m->off_w1, m->off_b1,
+                                                                  m->off_w2, m->off_b2, m->off_w3, m->off_b3, m->X,
+                                                                  m->Y);
+            return cudaGetLastError() == cudaSuccess ? SCAPH_OK : set_error(SCAPH_ECUDA, "forward1 launch");
+        }, &out_us[2]);
+    cudaMemcpyAsync(m->w, save, sizeof(float) * m->nparams, cudaMemcpyDeviceToDevice, m->st);
+    cudaMemcpyAsync(m->m, save + m->nparams, sizeof(float) * m->nparams, cudaMemcpyDeviceToDevice, m->st);
+    cudaMemcpyAsync(m->v, save + 2 * m->nparams, sizeof(float) * m->nparams, cudaMemcpyDeviceToDevice, m->st);
+    cudaStreamSynchronize(m->st);
+    cudaFree(save);
+    cudaEventDestroy(e[0]);
+    cudaEventDestroy(e[1]);
+    return rc;
+}
+
 // Minibatch training: `epochs` passes over the n rows in a seeded order.
 int scaph_mlp_train(scaph_mlp *m, const float *X, const float *T, const float *W, int n, int epochs, int batch,
                     float lr, uint64_t seed, float *final_loss)

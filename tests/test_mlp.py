@@ -74,3 +74,14 @@ def test_gpu_training_fits_a_separable_task(tmp_path):
     other = S.Mlp(n_in, n_out, seed=9)
     other.load(path)
     assert np.array_equal(other.params(), net.params())
+
+
+@pytest.mark.gpu
+def test_device_timing_leaves_the_network_unchanged():
+    """scaph_mlp_time reports CUDA-event times of a forward pass, a training
+    step and the single-row inference kernel, and restores the parameters."""
+    net = S.Mlp(16 + 40, 41, seed=9)
+    p0 = net.params().copy()
+    t = net.time(n=128, reps=5)
+    assert t["forward_us"] > 0 and t["train_step_us"] > t["forward_us"] and t["infer1_us"] > 0
+    assert np.array_equal(net.params(), p0)
