@@ -249,6 +249,22 @@ __device__ __forceinline__ void visit4(LevelSmem &sm, const BfsDev &s, ThreadAcc
 #pragma unroll
     for (int j = 0; j < 4; j++)
         vw[j] = (in[j] && u[j] < s.V) ? *((volatile const uint32_t *)&s.visited[u[j] >> 5]) : 0xFFFFFFFFu;
+    if (s.push_defer) {
+        // deferred claims: visited does not change during the level, so an
+        // unvisited neighbour's bit goes straight into the next frontier
+        // (fire-and-forget reduction); k_push_finalize does the rest
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            if (!in[j]) continue;
+            if (u[j] >= s.V) {
+                atomicOr(&s.ctr->error, 1u);
+                continue;
+            }
+            if (!((vw[j] >> (u[j] & 31)) & 1u))
+                asm volatile("red.global.or.b32 [%0], %1;" ::"l"(s.next + (u[j] >> 5)), "r"(1u << (u[j] & 31)));
+        }
+        return;
+    }
 #pragma unroll
     for (int j = 0; j < 4; j++) {
         if (!in[j]) continue;
@@ -761,6 +777,41 @@ __device__ __forceinline__ void pull_body(const GraphDev &g, const BfsDev &s, ui
     level_epilogue<BLOCK>(sm, s, t);
 }
 
+// Deferred-claim push levels: the next frontier holds every unvisited
+// vertex some frontier vertex reached; each is claimed here, word by word
+// (depth written for 32 consecutive vertices at a time, visited updated
+// with a plain store: one thread owns each word), with the level's counters
+// and page histograms.
+template <int BLOCK>
+__device__ __forceinline__ void finalize_body(const BfsDev &s)
+{
+    __shared__ LevelSmem sm;
+    level_prologue<BLOCK>(sm, s);
+    const PageLut lut = stage_lut<BLOCK>(s.hg, sm);
+    __syncthreads();
+    ThreadAcc t;
+    for (uint32_t w = blockIdx.x * BLOCK + threadIdx.x; w < s.nwords; w += gridDim.x * BLOCK) {
+        const uint32_t nx = s.next[w];
+        if (!nx) continue;
+        const uint32_t vis = s.visited[w];
+        uint32_t n = nx & ~vis;
+        if (n != nx) s.next[w] = n;
+        if (!n) continue;
+        s.visited[w] = vis | n;
+        while (n) {
+            const uint32_t v = (w << 5) + (__ffs(n) - 1);
+            n &= n - 1;
+            s.depth[v] = s.level + 1;
+            const uint32_t dv = __ldg(&s.degree[v]);
+            t.next++;
+            t.next_edges += dv;
+            if (s.page_nodes) hist_add(sm, s, lut.of(v), dv + 3);
+            hist_in_add(sm, s, v);
+        }
+    }
+    level_epilogue<BLOCK>(sm, s, t);
+}
+
 // graph mode: the level's state from the device control block
 __device__ __forceinline__ BfsDev level_state(const BfsGraphArgs &a)
 {
@@ -774,6 +825,7 @@ __device__ __forceinline__ BfsDev level_state(const BfsGraphArgs &a)
     s.next = a.bm3 + (size_t)((L + 1) % 3) * s.nwords;
     s.ctr = a.ctr0 + L;
     s.pull_gather = c->pull_gather;
+    s.push_defer = c->push_defer;
     if (a.hist0 && L < a.hist_levels) {
         s.page_nodes = a.hist0 + (size_t)L * 2 * a.npages_h;
         s.page_datas = s.page_nodes + a.npages_h;
@@ -821,6 +873,12 @@ __global__ void __launch_bounds__(BLOCK, kPullMinThreads / BLOCK) k_pull(GraphDe
     pull_body<BLOCK>(g, s, vlo, vhi, rl);
 }
 
+template <int BLOCK>
+__global__ void __launch_bounds__(BLOCK) k_push_finalize(BfsDev s)
+{
+    finalize_body<BLOCK>(s);
+}
+
 // ---------------------------------------------------------------------------
 // kernels: graph mode
 // ---------------------------------------------------------------------------
@@ -841,6 +899,13 @@ __global__ void __launch_bounds__(BLOCK) k_push_giant_g(GraphDev g, BfsGraphArgs
 {
     if (a.ctl->dir != 0) return;
     giant_body<BLOCK>(g, level_state(a));
+}
+
+template <int BLOCK>
+__global__ void __launch_bounds__(BLOCK) k_push_finalize_g(BfsGraphArgs a)
+{
+    if (a.ctl->dir != 0 || !a.ctl->push_defer) return;
+    finalize_body<BLOCK>(level_state(a));
 }
 
 template <int BLOCK>
@@ -867,6 +932,7 @@ __global__ void k_graph_init(BfsGraphArgs a, uint32_t *depth, uint32_t *parent, 
         c->dir = 0;
         c->done = 0;
         c->pull_gather = 0;
+        c->push_defer = 0;
         c->t_start = globaltimer();
     }
     const size_t stride = (size_t)gridDim.x * blockDim.x;
@@ -931,6 +997,7 @@ __global__ void k_decide(BfsGraphArgs a, DecideArgs d, cudaGraphConditionalHandl
     else if (d.mode == 2) nd = 1;
     else nd = alpha_beta_next(c->dir, c->nf, c->prev_nf, c->mf, mu, d.V, d.alpha, d.beta);
     c->dir = nd;
+    c->push_defer = nd == 0 && d.defer_edges && c->mf >= d.defer_edges && !c->parent ? 1u : 0u;
     {
         const uint32_t src = c->src;
         const unsigned long long src_dead = (d.dead_bm[src >> 5] >> (src & 31)) & 1u;
@@ -1022,6 +1089,7 @@ __global__ void __launch_bounds__(64) k_decide_learned(BfsGraphArgs a, DecideArg
         const int nd = d.mode == 1 ? 0 : d.mode == 2 ? 1 : s_guard >= 0 ? s_guard : (y > 0.f ? 1 : 0);
         c->dir = nd;
         c->pull_gather = s_unv * d.gather_ratio < d.V ? 1u : 0u;
+        c->push_defer = nd == 0 && d.defer_edges && c->mf >= d.defer_edges && !c->parent ? 1u : 0u;
         c->level = L + 1;
         cudaGraphSetConditional(h_loop, 1);
     }
@@ -1090,6 +1158,25 @@ cudaError_t run_ranges(int dir, int block, int grid, const GraphDev &g, const Bf
     case 128: return launch_ranges<128>(dir, grid, g, s, rl, st);
     case 512: return launch_ranges<512>(dir, grid, g, s, rl, st);
     default: return launch_ranges<256>(dir, grid, g, s, rl, st);
+    }
+}
+
+cudaError_t run_push_finalize(int block, int grid, const BfsDev &s, cudaStream_t st)
+{
+    switch (block) {
+    case 128: k_push_finalize<128><<<grid, 128, 0, st>>>(s); break;
+    case 512: k_push_finalize<512><<<grid, 512, 0, st>>>(s); break;
+    default: k_push_finalize<256><<<grid, 256, 0, st>>>(s); break;
+    }
+    return cudaGetLastError();
+}
+
+const void *push_finalize_graph_kernel(int block)
+{
+    switch (block) {
+    case 128: return (const void *)k_push_finalize_g<128>;
+    case 512: return (const void *)k_push_finalize_g<512>;
+    default: return (const void *)k_push_finalize_g<256>;
     }
 }
 

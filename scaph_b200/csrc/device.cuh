@@ -93,6 +93,10 @@ struct BfsDev {
     GraphDev hgi;
     uint32_t pull_gather;      // sparse pull level: gather several tiles per queue
     uint32_t giant_edges;      // push: adjacency longer than this becomes chunks (0: kGiantEdges)
+    // push: 1 = the level defers its claims: the neighbours' bits are OR-ed
+    // into `next` (no per-edge atomic round trip, no scattered depth write)
+    // and k_push_finalize then writes depths and counters word by word
+    uint32_t push_defer;
 };
 
 // Second word of a pull record: the in-degree capped at 15 in the top four
@@ -120,7 +124,7 @@ struct BfsCtl {
     int32_t dir;               // 0 push, 1 pull
     int32_t done;
     uint32_t pull_gather;      // the level is a sparse pull (BfsDev::pull_gather)
-    uint32_t _pad;
+    uint32_t push_defer;       // the level is a deferred-claim push (BfsDev::push_defer)
     unsigned long long nf, prev_nf, mf, vis_n, vis_e;
     unsigned long long t_start;
 };
@@ -155,6 +159,7 @@ struct DecideArgs {
     float alpha, beta;
     int32_t max_levels;
     uint32_t gather_ratio;          // pull levels gather tiles below 1 unvisited per this many
+    unsigned long long defer_edges; // push levels with this many frontier edges defer claims (0 never)
 };
 
 // Beamer's direction-optimizing rule (SC'12): leave top-down when the

@@ -151,6 +151,7 @@ int scaph_engine::create(const Graph *g_, const Graph *gt_, const scaph_config *
     if (cfg.pull_gather_ratio <= 0) cfg.pull_gather_ratio = (int32_t)kPullGatherRatio;
     if (cfg.ms_compact_l2_div <= 0) cfg.ms_compact_l2_div = 3;
     if (cfg.ms_compact_min_deg <= 0) cfg.ms_compact_min_deg = 16;
+    if (cfg.push_defer_edges < 0) cfg.push_defer_edges = 0;
     device = cfg.device;
     if (g->weighted) return set_error(SCAPH_EUNSUPPORTED, "BFS engine needs unweighted pages");
     if (gt && (gt->V != V || gt->E != E || gt->weighted))
@@ -543,6 +544,9 @@ int scaph_engine::run_host_loop(uint32_t src, uint32_t *dd, uint32_t *dp)
             const uint64_t unv_now = (uint64_t)V - n_dead - vis_n + (src_dead ? 1 : 0);
             s.pull_gather = unv_now * (uint64_t)cfg.pull_gather_ratio < V ? 1u : 0u;
         }
+        // deferred claims on big push levels (resident graphs, no parents)
+        s.push_defer = !pager && !dp && !dual && cfg.push_defer_edges > 0 && mf >= (uint64_t)cfg.push_defer_edges
+                           ? 1u : 0u;
         s.page_nodes_in = s.page_datas_in = nullptr;
         if (incr && d_hist_in && level < kHistLevels) {
             s.page_nodes_in = d_hist_in + (size_t)level * 2 * npi;
@@ -596,6 +600,7 @@ int scaph_engine::run_host_loop(uint32_t src, uint32_t *dd, uint32_t *dp)
         } else {
             const GraphDev &gv = run_dir == 0 ? dout.view : gin();
             SCAPH_CUDA(run_level(run_dir, block, run_dir == 0 ? grid_push : grid_pull, gv, s, 0, V, st));
+            if (run_dir == 0 && s.push_defer) SCAPH_CUDA(run_push_finalize(block, num_sms * 4, s, st));
         }
         SCAPH_CUDA(cudaEventRecord(ev_level[2 * level + 1], st));
         SCAPH_CUDA(cudaMemcpyAsync(h_ctr + level, d_ctr + level, sizeof(LevelCounters), cudaMemcpyDeviceToHost, st));
@@ -670,6 +675,7 @@ int scaph_engine::build_graph()
     dargs.beta = cfg.beta;
     dargs.max_levels = kMaxLevels;
     dargs.gather_ratio = (uint32_t)cfg.pull_gather_ratio;
+    dargs.defer_edges = (unsigned long long)cfg.push_defer_edges;
 
     // init (run inputs are this node's arguments, replaced per launch)
     uint32_t *depth0 = d_depth, *parent0 = nullptr, src0 = 0, unr = unreached, nclear = kMaxLevels;
@@ -715,10 +721,23 @@ int scaph_engine::build_graph()
     SCAPH_CUDA(cudaGraphAddKernelNode(&n_push, body, nullptr, 0, &lp));
     lp.func = const_cast<void *>(f_giant);
     SCAPH_CUDA(cudaGraphAddKernelNode(&n_giant, body, &n_push, 1, &lp));
+    cudaGraphNode_t n_before_pull = n_giant;
+    void *fin_args[] = {&gargs};
+    if (cfg.push_defer_edges > 0) {
+        // deferred-claim push levels: the finalize pass after the giant chunks
+        cudaGraphNode_t n_fin;
+        cudaKernelNodeParams fp{};
+        fp.func = const_cast<void *>(push_finalize_graph_kernel(block));
+        fp.gridDim = dim3(num_sms * 4);
+        fp.blockDim = dim3(block);
+        fp.kernelParams = fin_args;
+        SCAPH_CUDA(cudaGraphAddKernelNode(&n_fin, body, &n_giant, 1, &fp));
+        n_before_pull = n_fin;
+    }
     lp.func = const_cast<void *>(f_pull);
     lp.gridDim = dim3(grid_pull);
     lp.kernelParams = pull_args;
-    SCAPH_CUDA(cudaGraphAddKernelNode(&n_pull, body, &n_giant, 1, &lp));
+    SCAPH_CUDA(cudaGraphAddKernelNode(&n_pull, body, &n_before_pull, 1, &lp));
 
     const bool learned = cfg.direction == SCAPH_DIR_LEARNED && sched;
     MlpDev net{};
@@ -1019,6 +1038,7 @@ int scaph_engine_tune(scaph_engine *e, const scaph_config *c)
     k.ms_compact_l2_div = c->ms_compact_l2_div > 0 ? c->ms_compact_l2_div : 3;
     k.ms_compact_min_deg = c->ms_compact_min_deg > 0 ? c->ms_compact_min_deg : 16;
     k.ctas_per_sm = c->ctas_per_sm;
+    k.push_defer_edges = c->push_defer_edges > 0 ? c->push_defer_edges : 0;
     e->block = c->block_size ? c->block_size : 256;
     const int occ_push = std::max(1, level_occupancy(0, e->block)), occ_pull = std::max(1, level_occupancy(1, e->block));
     e->grid_push = k.ctas_per_sm > 0 ? k.ctas_per_sm * e->num_sms : occ_push * e->num_sms;

@@ -15,6 +15,11 @@ cudaError_t run_level(int dir, int block, int grid, const GraphDev &g, const Bfs
 cudaError_t run_ranges(int dir, int block, int grid, const GraphDev &g, const BfsDev &s, const RangeList &rl,
                        cudaStream_t st);
 cudaError_t run_giant(int block, int grid, const GraphDev &g, const BfsDev &s, cudaStream_t st);
+// Deferred-claim push levels (BfsDev::push_defer): claims the next frontier
+// word by word after the push (and giant-chunk) kernels.
+cudaError_t run_push_finalize(int block, int grid, const BfsDev &s, cudaStream_t st);
+// k_push_finalize_g(BfsGraphArgs): the graph-mode node, after the giant chunks
+const void *push_finalize_graph_kernel(int block);
 // k_graph_init(BfsGraphArgs, u32* depth, u32* parent, u32 src, u32 unreached, const u32* dead, u32 nlevels_clear)
 // Graph mode: the push, giant-chunk and pull kernels of a level (each leaves
 // at once unless the level's direction selects it).

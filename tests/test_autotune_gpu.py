@@ -21,8 +21,12 @@ def rmat15():
 
 @pytest.mark.parametrize("kw", [dict(giant_edges=128), dict(giant_edges=8192), dict(pull_gather_ratio=1),
                                 dict(pull_gather_ratio=100000), dict(ctas_per_sm=1, block_size=512),
-                                dict(alpha=2.0, beta=200.0)])
+                                dict(alpha=2.0, beta=200.0), dict(push_defer_edges=1),
+                                dict(push_defer_edges=1, giant_edges=256, alpha=1000.0)])
 def test_tunables_keep_depths(rmat15, kw):
+    """push_defer_edges=1 defers the claims of every push level (neighbours
+    OR-ed into the next frontier, depths written by the finalize pass);
+    with alpha 1000 every level pushes."""
     csr, g = rmat15
     for use_graph in (0, 2):
         eng = S.Engine(g, use_graph=use_graph)
@@ -74,4 +78,17 @@ def test_autotune_engine_single_and_multi(rmat15):
         assert np.array_equal(d, O.bfs(csr.idx, csr.ngh, s))
     r = autotune.tune_engine(eng, srcs, buf.data_ptr(), multi=True, repeats=2)
     assert r["ms"] <= r["default_ms"]
+    eng.close()
+
+
+def test_deferred_push_with_parents_falls_back_to_claims(rmat15):
+    """Parents need a claim winner: with parents requested the deferred path
+    is not taken, and the tree is valid."""
+    csr, g = rmat15
+    eng = S.Engine(g, push_defer_edges=1)
+    src = G.sources(csr, 1, 83)[0]
+    d, p, _ = eng.bfs(src, parents=True)
+    assert np.array_equal(d, O.bfs(csr.idx, csr.ngh, src))
+    rc, bad = O.validate_tree(csr.idx, csr.ngh, src, d, p)
+    assert rc == 0, (rc, bad)
     eng.close()
