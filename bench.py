@@ -439,7 +439,7 @@ def _run_set(S, g, gt, srcs, pool, net=None, cold=False, warm_pass=True, digests
     if warm_pass and not cold:
         for s in srcs:
             eng.bfs(s)
-    ms, h2d, zc, levels = 0.0, 0, 0, 0
+    ms, h2d, zc, alg, levels = 0.0, 0, 0, 0, 0
     for s in srcs:
         if cold:
             eng.evict_all()
@@ -447,11 +447,12 @@ def _run_set(S, g, gt, srcs, pool, net=None, cold=False, warm_pass=True, digests
         ms += st.ms
         h2d += st.h2d_bytes
         zc += st.zc_bytes
+        alg += st.pcie_alg_bytes
         levels += st.levels
         if digests is not None and s in digests:
             digests[s].append(_digest(d))
     eng.close()
-    return {"ms": ms, "h2d_bytes": h2d, "zc_bytes": zc, "levels": levels}
+    return {"ms": ms, "h2d_bytes": h2d, "zc_bytes": zc, "pcie_alg_bytes": alg, "levels": levels}
 
 
 def extra_config3(nsrc_train=32, nsrc_eval=32, nsrc_oracle=16):
@@ -495,7 +496,14 @@ def extra_config3(nsrc_train=32, nsrc_eval=32, nsrc_oracle=16):
             "speedup": plain["ms"] / learned["ms"],
             "plain_pcie_bytes_per_level": plain["h2d_bytes"] / max(1, plain["levels"]),
             "learned_pcie_bytes_per_level": learned["h2d_bytes"] / max(1, learned["levels"]),
-            "plain_zero_copy_bytes": plain["zc_bytes"], "learned_zero_copy_bytes": learned["zc_bytes"]}
+            "plain_zero_copy_bytes": plain["zc_bytes"], "learned_zero_copy_bytes": learned["zc_bytes"],
+            # the least the levels had to move over the link (non-resident
+            # active words, get_page_info's datas) against what moved
+            "plain_pcie_alg_bytes_per_level": plain["pcie_alg_bytes"] / max(1, plain["levels"]),
+            "learned_pcie_alg_bytes_per_level": learned["pcie_alg_bytes"] / max(1, learned["levels"]),
+            "plain_ms": plain["ms"], "learned_ms": learned["ms"],
+            "plain_moved_bytes": plain["h2d_bytes"] + plain["zc_bytes"],
+            "learned_moved_bytes": learned["h2d_bytes"] + learned["zc_bytes"]}
     # the checker: oracle depths of the checked held-out sources against the
     # six runs of each (plain and learned, three regimes)
     from oracle import oracle as O
