@@ -238,7 +238,9 @@ typedef struct scaph_config {
                                   compacted when they fit L2 / this; 0 = 3  */
     int32_t  ms_compact_min_deg;/* ... and the frontier has at least this
                                   many out-edges per vertex; 0 = 16        */
-    int32_t  _reserved0;
+    int32_t  pull_warp;        /* 1: pull levels run warp-centric (each warp
+                                  owns 512-vertex chunks, no CTA barriers);
+                                  0: CTA tiles of 4096 vertices             */
     int64_t  push_defer_edges; /* a push level whose frontier has at least
                                   this many out-edges defers its claims: the
                                   neighbours' bits are OR-ed into the next
@@ -293,8 +295,8 @@ int scaph_bfs(scaph_engine *e, uint32_t src, uint32_t *depths, uint32_t *parents
               int out_on_device, scaph_bfs_stats *stats);
 /* Sets an engine's run-time tunables from cfg: alpha, beta, block_size,
  * ctas_per_sm, giant_edges, pull_gather_ratio, ms_compact_l2_div,
- * ms_compact_min_deg and push_defer_edges (0 = default; the other fields
- * are ignored).  They
+ * ms_compact_min_deg, pull_warp and push_defer_edges (0 = default; the
+ * other fields are ignored).  They
  * change the schedule only, never the depths.  Waits for the engine's work
  * and drops its CUDA graph (the next run rebuilds it).  Replaces setting
  * FLAGS_num_blks / FLAGS_num_thds between runs (src/app.cuh:38-52). */

@@ -136,6 +136,7 @@ GATHER = (16, 32, 64, 128, 256)
 CTAS = (0, 2, 3, 4, 6, 8)  # 0: the occupancy limit
 MS_L2_DIV = (2, 3, 4, 6, 8)
 MS_MIN_DEG = (4, 8, 16, 32, 64)
+DEFER = (0, 1 << 16, 1 << 20, 1 << 24)  # frontier out-edges from which push defers its claims
 
 
 def _engine_run(eng: Engine, sources, ptr: int, multi: bool) -> float:
@@ -162,7 +163,8 @@ def tune_engine(eng: Engine, sources, ptr: int, multi: bool = False, repeats: in
     workload: `sources` run one by one (single-source; `ptr` a device
     buffer of V words) or as one multi-source batch (`ptr`: len(sources) * V
     words).  Single-source: CTAs per SM, the giant-chunk cut, the pull
-    gather ratio, alpha, beta; multi-source: the mask-compaction thresholds,
+    gather ratio, the warp-centric pull, the deferred-claim push threshold,
+    alpha, beta; multi-source: the mask-compaction thresholds,
     alpha, beta.  Each candidate is timed best of `repeats` (device time);
     the default's spread over `repeats` more runs is reported beside the
     result, so a gain can be told from noise.  The chosen tunables must
@@ -188,8 +190,8 @@ def tune_engine(eng: Engine, sources, ptr: int, multi: bool = False, repeats: in
         axes = (("ms_compact_l2_div", MS_L2_DIV), ("ms_compact_min_deg", MS_MIN_DEG), ("alpha", ALPHAS),
                 ("beta", BETAS))
     else:
-        axes = (("ctas_per_sm", CTAS), ("giant_edges", GIANT), ("pull_gather_ratio", GATHER), ("alpha", ALPHAS),
-                ("beta", BETAS))
+        axes = (("pull_warp", (0, 1)), ("push_defer_edges", DEFER), ("ctas_per_sm", CTAS), ("giant_edges", GIANT),
+                ("pull_gather_ratio", GATHER), ("alpha", ALPHAS), ("beta", BETAS))
     for name, values in axes:
         for v in values:
             if v != best[name]:

@@ -455,6 +455,19 @@ __device__ __forceinline__ void pull_body(const GraphDev &g, const BfsDev &s, ui
                                  : (((uint32_t)(((unsigned long long)vhi + 31) >> 5)) - (vlo >> 5) + kPullTileWords - 1) /
                                        kPullTileWords;
 
+    // where vertex v's in-list lives (false: its page is missing)
+    auto list_start_w = [&](uint32_t v, int &p, unsigned long long &st) -> bool {
+        p = lut.of(v);
+        const PageDev pd = lut.pages[p];
+        if (pd.base == kNotResident) {
+            atomicOr(&s.ctr->error, 4u);
+            return false;
+        }
+        st = pd.base + 3ull * pd.nodenum + g.pool[pd.base + 3ull * (v - pd.left) + 1];
+        t.headers++;
+        return true;
+    };
+
     // Runs phases A and B over q[0, total): found vertices go to the tile's
     // shared bitmap fnd (tbase = the tile's first word), or, gathering
     // several sparse tiles, straight to the visited / next words.
@@ -714,6 +727,161 @@ __device__ __forceinline__ void pull_body(const GraphDev &g, const BfsDev &s, ui
             __syncthreads();
         }
     };
+
+    // Warp-centric variant (s.pull_warp, 8-byte records present): every
+    // warp owns chunks of 16 bitmap words (512 vertices) on its own -
+    // compaction by warp scan into its 512-entry slice of q, found bits in
+    // its 16-word slice of fnd, phase B by the whole warp - so no CTA
+    // barrier stands between a warp and its next chunk.
+    if (BLOCK <= 256 && s.pull_warp && s.prec) {
+        constexpr uint32_t kChunkWords = 16, kChunks = kPullTileWords / kChunkWords;
+        static_assert(kChunkWords * 32 * (256 / 32) <= kPullTileWords * 32, "per-warp queues fit q");
+        const int warp = threadIdx.x >> 5;
+        uint32_t *qw = q + warp * (kChunkWords * 32);
+        uint32_t *fw = fnd + warp * kChunkWords;
+        const uint32_t nchunks = ntiles * kChunks, warps = gridDim.x * (BLOCK / 32);
+        for (uint32_t c = blockIdx.x * (BLOCK / 32) + warp; c < nchunks; c += warps) {
+            uint32_t rlo = vlo, rhi = vhi, local;
+            range_of_tile(rl, c / kChunks, rlo, rhi, local);
+            const uint32_t rwhi = (uint32_t)(((unsigned long long)rhi + 31) >> 5);
+            const uint32_t wbase = (rlo >> 5) + local * kPullTileWords + (c % kChunks) * kChunkWords;
+            const uint32_t w = wbase + lane;
+            uint32_t unv = 0;
+            if (lane < (int)kChunkWords) {
+                fw[lane] = 0;
+                if (w < rwhi) unv = ~s.visited[w] & range_mask(w, rlo, rhi);
+            }
+            const uint32_t cnt = __popc(unv);
+            uint32_t inc = cnt;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, inc, o);
+                if (lane >= o) inc += y;
+            }
+            const uint32_t total = __shfl_sync(0xFFFFFFFFu, inc, 31);
+            if (total == 0) continue;
+            {
+                uint32_t at = inc - cnt, m = unv;
+                while (m) {
+                    qw[at++] = (w << 5) + (__ffs(m) - 1);
+                    m &= m - 1;
+                }
+            }
+            __syncwarp();
+            auto found_w = [&](uint32_t v, uint32_t par, uint32_t dv) {
+                s.depth[v] = s.level + 1;
+                if (s.parent) s.parent[v] = par;
+                atomicOr(&fw[(v >> 5) - wbase], 1u << (v & 31));
+                t.next++;
+                t.next_edges += dv;
+                if (s.page_nodes) hist_add(sm, s, hist_same ? lut.of(v) : page_of(s.hg, v), dv + 3);
+                hist_in_add(sm, s, v);
+            };
+            for (uint32_t k0 = 0; k0 < total; k0 += 32 * kPPT) {
+                uint32_t vv[kPPT], dg[kPPT];
+                uint2 rec[kPPT];
+                bool slow[kPPT];
+#pragma unroll
+                for (int i = 0; i < kPPT; i++) {
+                    const uint32_t k = k0 + i * 32 + lane;
+                    vv[i] = k < total ? qw[k] : 0xFFFFFFFFu;
+                    rec[i] = vv[i] != 0xFFFFFFFFu ? ld_nc_v2(s.prec + vv[i]) : make_uint2(0xFFFFFFFFu, 0u);
+                }
+#pragma unroll
+                for (int i = 0; i < kPPT; i++) {
+                    slow[i] = false;
+                    dg[i] = rec[i].y & kPrecDegMax;
+                    if (vv[i] == 0xFFFFFFFFu) continue;
+                    const uint32_t h0 = rec[i].x, nin = rec[i].y >> 28;
+                    if (h0 < s.V && test_bit(s.front, h0)) {
+                        t.inspected += 1;
+                        found_w(vv[i], h0, dg[i] == kPrecDegMax ? __ldg(&s.degree[vv[i]]) : dg[i]);
+                    } else if (nin <= 1) {
+                        t.inspected += nin;
+                    } else {
+                        slow[i] = true;
+                    }
+                }
+                // the rest: in-degree, ranked head row, then (rarely) the
+                // whole in-list, scanned by the warp
+#pragma unroll
+                for (int i = 0; i < kPPT; i++) {
+                    uint32_t need = 0, len = 0;
+                    unsigned long long st = 0;
+                    if (slow[i]) {
+                        const uint32_t v = vv[i];
+                        len = __ldg(&s.indeg[v]);
+                        const uint4 h = ld_nc_v4(s.head + (size_t)kPullHead * v);
+                        if (dg[i] == kPrecDegMax) dg[i] = __ldg(&s.degree[v]);
+                        uint32_t par = kNoParent, j = 0;
+                        if (h.y < s.V && test_bit(s.front, h.y)) par = h.y, j = 2;
+                        else if (h.z < s.V && test_bit(s.front, h.z)) par = h.z, j = 3;
+                        else if (h.w < s.V && test_bit(s.front, h.w)) par = h.w, j = 4;
+                        if (par != kNoParent) {
+                            t.inspected += j;
+                            found_w(v, par, dg[i]);
+                        } else {
+                            t.inspected += min(len, kPullSerial);
+                            int pg = -1;
+                            need = len > kPullSerial && list_start_w(v, pg, st) ? 1u : 0u;
+                        }
+                    }
+                    uint32_t todo = __ballot_sync(0xFFFFFFFFu, need);
+                    while (todo) {
+                        const int src_lane = __ffs(todo) - 1;
+                        todo &= todo - 1;
+                        const uint32_t v = __shfl_sync(0xFFFFFFFFu, vv[i], src_lane);
+                        const uint32_t n = __shfl_sync(0xFFFFFFFFu, len, src_lane);
+                        const unsigned long long a = __shfl_sync(0xFFFFFFFFu, st, src_lane);
+                        const uint32_t dv = __shfl_sync(0xFFFFFFFFu, dg[i], src_lane);
+                        const unsigned long long b = a + n, qa = a >> 2, qb = (b + 3) >> 2;
+                        uint32_t hit_par = kNoParent;
+                        unsigned long long hit_word = b;
+                        for (unsigned long long q0 = qa; q0 < qb; q0 += 32) {
+                            const unsigned long long qd = q0 + lane;
+                            uint32_t myhit = 0;
+                            uint4 val = make_uint4(0, 0, 0, 0);
+                            if (qd < qb) {
+                                val = ld_nc_v4(g.pool + qd * 4);
+                                const uint32_t vals[4] = {val.x, val.y, val.z, val.w};
+#pragma unroll
+                                for (int j = 0; j < 4; j++) {
+                                    const unsigned long long word = qd * 4 + j;
+                                    if (word >= a && word < b && vals[j] < s.V && test_bit(s.front, vals[j]))
+                                        myhit |= 1u << j;
+                                }
+                            }
+                            const uint32_t bal = __ballot_sync(0xFFFFFFFFu, myhit != 0);
+                            if (bal) {
+                                const int first = __ffs(bal) - 1;
+                                const uint32_t fh = __shfl_sync(0xFFFFFFFFu, myhit, first);
+                                const int j = __ffs(fh) - 1;
+                                const uint32_t pick = j == 0 ? val.x : j == 1 ? val.y : j == 2 ? val.z : val.w;
+                                hit_par = __shfl_sync(0xFFFFFFFFu, pick, first);
+                                hit_word = (q0 + first) * 4 + j;
+                                break;
+                            }
+                        }
+                        if (lane == src_lane) {
+                            t.inspected += (uint32_t)(hit_word - a) + (hit_par != kNoParent ? 1u : 0u);
+                            if (hit_par != kNoParent) found_w(v, hit_par, dv);
+                        }
+                    }
+                }
+            }
+            __syncwarp();
+            if (lane < (int)kChunkWords && w < rwhi) {
+                const uint32_t f = fw[lane];
+                if (f) {
+                    atomicOr(&s.visited[w], f);
+                    atomicOr(&s.next[w], f);
+                }
+            }
+            __syncwarp();
+        }
+        level_epilogue<BLOCK>(sm, s, t);
+        return;
+    }
 
     // Sparse levels (few unvisited vertices, a handful per tile): the
     // vertices of several tiles are gathered into one queue before phases A

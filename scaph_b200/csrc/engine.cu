@@ -128,6 +128,7 @@ BfsDev scaph_engine::base_state(uint32_t *dd, uint32_t *dp) const
     s.head_ranked = head_ranked ? 1u : 0u;
     s.prec = d_prec;
     s.giant_edges = (uint32_t)cfg.giant_edges;
+    s.pull_warp = cfg.pull_warp ? 1u : 0u;
     return s;
 }
 
@@ -1039,6 +1040,7 @@ int scaph_engine_tune(scaph_engine *e, const scaph_config *c)
     k.ms_compact_min_deg = c->ms_compact_min_deg > 0 ? c->ms_compact_min_deg : 16;
     k.ctas_per_sm = c->ctas_per_sm;
     k.push_defer_edges = c->push_defer_edges > 0 ? c->push_defer_edges : 0;
+    k.pull_warp = c->pull_warp ? 1 : 0;
     e->block = c->block_size ? c->block_size : 256;
     const int occ_push = std::max(1, level_occupancy(0, e->block)), occ_pull = std::max(1, level_occupancy(1, e->block));
     e->grid_push = k.ctas_per_sm > 0 ? k.ctas_per_sm * e->num_sms : occ_push * e->num_sms;
