@@ -956,6 +956,7 @@ __device__ __forceinline__ void finalize_body(const BfsDev &s)
     __shared__ LevelSmem sm;
     level_prologue<BLOCK>(sm, s);
     const PageLut lut = stage_lut<BLOCK>(s.hg, sm);
+    if (blockIdx.x == 0 && threadIdx.x == 0) s.ctr->deferred = 1u;
     __syncthreads();
     ThreadAcc t;
     for (uint32_t w = blockIdx.x * BLOCK + threadIdx.x; w < s.nwords; w += gridDim.x * BLOCK) {

@@ -47,7 +47,7 @@ struct LevelCounters {
     unsigned int error;             // nonzero: a kernel saw a bad index / overflow
     unsigned long long zc_words;    // words read zero-copy from host pages
     int dir;                        // direction the level ran (graph mode)
-    unsigned int _pad;
+    unsigned int deferred;          // 1: a deferred-claim push (k_push_finalize ran)
     unsigned long long t_end;       // %globaltimer when the level was decided (graph mode)
 };
 

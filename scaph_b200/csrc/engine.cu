@@ -828,12 +828,14 @@ int scaph_engine::collect(bool from_graph)
         if (from_graph) {
             t.ms = (double)(lc.t_end - tprev) * 1e-6;
             tprev = lc.t_end;
-            launches += 4;  // push, giant, pull and decide run every level (two leave at once)
+            // push, giant, pull and decide (and the finalize node when deferred
+            // claims are on) run every level; the unselected ones leave at once
+            launches += cfg.push_defer_edges > 0 ? 5 : 4;
         } else {
             float ms = 0;
             cudaEventElapsedTime(&ms, ev_level[2 * l], ev_level[2 * l + 1]);
             t.ms = ms;
-            launches += lc.dir == 0 ? 2 : 1;
+            launches += (lc.dir == 0 ? 2 : 1) + lc.deferred;
             if ((size_t)l < level_h2d.size()) t.h2d_bytes = level_h2d[l];
             if ((size_t)l < dual_ms.size()) {
                 t.push_ms = dual_ms[l].first;
