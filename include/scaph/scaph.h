@@ -246,6 +246,12 @@ typedef struct scaph_config {
                                   neighbours' bits are OR-ed into the next
                                   frontier and one pass then writes depths
                                   word by word (not with parents); 0 = never */
+    int32_t  pull_records;     /* pull phase A from the 8-byte per-vertex
+                                  records: 0 = on levels whose frontier has
+                                  at least a quarter as many vertices as the
+                                  unvisited set (the top-ranked probe mostly
+                                  hits there), 1 = every level, 2 = never   */
+    int32_t  _reserved1;
 } scaph_config;
 
 typedef struct scaph_engine scaph_engine;
@@ -295,8 +301,8 @@ int scaph_bfs(scaph_engine *e, uint32_t src, uint32_t *depths, uint32_t *parents
               int out_on_device, scaph_bfs_stats *stats);
 /* Sets an engine's run-time tunables from cfg: alpha, beta, block_size,
  * ctas_per_sm, giant_edges, pull_gather_ratio, ms_compact_l2_div,
- * ms_compact_min_deg, pull_warp and push_defer_edges (0 = default; the
- * other fields are ignored).  They
+ * ms_compact_min_deg, pull_warp, push_defer_edges and pull_records (0 =
+ * default; the other fields are ignored).  They
  * change the schedule only, never the depths.  Waits for the engine's work
  * and drops its CUDA graph (the next run rebuilds it).  Replaces setting
  * FLAGS_num_blks / FLAGS_num_thds between runs (src/app.cuh:38-52). */

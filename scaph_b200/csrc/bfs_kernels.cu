@@ -995,6 +995,7 @@ __device__ __forceinline__ BfsDev level_state(const BfsGraphArgs &a)
     s.ctr = a.ctr0 + L;
     s.pull_gather = c->pull_gather;
     s.push_defer = c->push_defer;
+    if (!c->pull_rec) s.prec = nullptr;
     if (a.hist0 && L < a.hist_levels) {
         s.page_nodes = a.hist0 + (size_t)L * 2 * a.npages_h;
         s.page_datas = s.page_nodes + a.npages_h;
@@ -1102,6 +1103,7 @@ __global__ void k_graph_init(BfsGraphArgs a, uint32_t *depth, uint32_t *parent, 
         c->done = 0;
         c->pull_gather = 0;
         c->push_defer = 0;
+        c->pull_rec = 0;
         c->t_start = globaltimer();
     }
     const size_t stride = (size_t)gridDim.x * blockDim.x;
@@ -1172,6 +1174,7 @@ __global__ void k_decide(BfsGraphArgs a, DecideArgs d, cudaGraphConditionalHandl
         const unsigned long long src_dead = (d.dead_bm[src >> 5] >> (src & 31)) & 1u;
         const unsigned long long unv = (unsigned long long)d.V - d.dead - c->vis_n + src_dead;
         c->pull_gather = unv * d.gather_ratio < d.V ? 1u : 0u;
+        c->pull_rec = pull_use_records(d.pull_records, c->nf, unv) ? 1u : 0u;
     }
     c->level = L + 1;
     cudaGraphSetConditional(h_loop, 1);
@@ -1258,6 +1261,7 @@ __global__ void __launch_bounds__(64) k_decide_learned(BfsGraphArgs a, DecideArg
         const int nd = d.mode == 1 ? 0 : d.mode == 2 ? 1 : s_guard >= 0 ? s_guard : (y > 0.f ? 1 : 0);
         c->dir = nd;
         c->pull_gather = s_unv * d.gather_ratio < d.V ? 1u : 0u;
+        c->pull_rec = pull_use_records(d.pull_records, c->nf, s_unv) ? 1u : 0u;
         c->push_defer = nd == 0 && d.defer_edges && c->mf >= d.defer_edges && !c->parent ? 1u : 0u;
         c->level = L + 1;
         cudaGraphSetConditional(h_loop, 1);

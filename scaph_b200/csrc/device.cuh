@@ -126,6 +126,8 @@ struct BfsCtl {
     int32_t done;
     uint32_t pull_gather;      // the level is a sparse pull (BfsDev::pull_gather)
     uint32_t push_defer;       // the level is a deferred-claim push (BfsDev::push_defer)
+    uint32_t pull_rec;         // the level's pull reads the 8-byte records (BfsDev::prec)
+    uint32_t _pad2;
     unsigned long long nf, prev_nf, mf, vis_n, vis_e;
     unsigned long long t_start;
 };
@@ -161,7 +163,17 @@ struct DecideArgs {
     int32_t max_levels;
     uint32_t gather_ratio;          // pull levels gather tiles below 1 unvisited per this many
     unsigned long long defer_edges; // push levels with this many frontier edges defer claims (0 never)
+    int32_t pull_records;           // scaph_config.pull_records
 };
+
+// Whether a pull level reads the 8-byte records (scaph_config.pull_records):
+// where the frontier is small next to the unvisited set, the top-ranked
+// in-neighbour misses often and the record's second round trip (head row)
+// costs more than reading everything at once.
+__host__ __device__ inline bool pull_use_records(int mode, unsigned long long nf, unsigned long long unvisited)
+{
+    return mode == 1 || (mode == 0 && 4 * nf >= unvisited);
+}
 
 // Beamer's direction-optimizing rule (SC'12): leave top-down when the
 // frontier's out-edges exceed the unexplored edges / alpha; leave bottom-up

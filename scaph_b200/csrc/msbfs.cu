@@ -333,15 +333,11 @@ static int ms_run(scaph_engine *e, const uint32_t *srcs, int nsrc, uint32_t *out
             e->feat_log.insert(e->feat_log.end(), f.begin(), f.end());
         }
         if (net_on) {
+            // the network's direction output is trained on single-source
+            // level costs, which a batch's levels do not share (a pull level
+            // serves every source at once): the batch keeps alpha/beta and
+            // the traffic rule for direction, and takes the page outputs
             mlp_forward_host(e->sched_host, f.data(), y.data());
-            if (level > 0) {
-                dir = y[0] > 0.f ? 1 : 0;
-                const int sure = alpha_beta_confident(prev_dir, nf, mf, mu, V, alpha, beta);
-                if (sure >= 0) dir = sure;
-            }
-            if (e->pager)
-                for (int p = 0; p + 1 < (int)y.size() && p < (int)np; p++)
-                    if (y[1 + p] > 2.f && lp.push_cnt[p] == 0) prefetch_pages.push_back(p);
         }
         if (e->pager && learned && level > 0) {
             // the exact page traffic each direction would cause overrides
@@ -350,6 +346,14 @@ static int ms_run(scaph_engine *e, const uint32_t *srcs, int nsrc, uint32_t *out
             ms_transfer_ms(e, lp, tp, tq);
             if (tp > 2 * tq + 1.0) dir = 1;
             else if (tq > 2 * tp + 1.0) dir = 0;
+        }
+        if (net_on && e->pager && dir == 0) {
+            // during a push level: the out-pages the network expects to hold
+            // frontier vertices next level that this level does not read
+            // itself (a batch's union frontier makes a page it enters dense,
+            // so such a page is copied whole anyway)
+            for (int p = 0; p + 1 < (int)y.size() && p < (int)np; p++)
+                if (y[1 + p] > 2.f && lp.push_cnt[p] == 0) prefetch_pages.push_back(p);
         }
         const uint32_t d = (uint32_t)level + 1;
         for (int k = 0; k < kMsPlanes; k++) {

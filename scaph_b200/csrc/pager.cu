@@ -668,10 +668,12 @@ float pager_resident_fraction(const Pager *pg, int gid, const std::vector<int> *
 uint64_t pager_missing_words(const Pager *pg, int gid, const std::vector<int> &needed,
                              const std::vector<uint32_t> &datas)
 {
+    // a page prefetched for this level and not yet used by any level counts
+    // as missing: the link still had to carry it for this level
     const Pager::GState &G = pg->gs[gid];
     uint64_t w = 0;
     for (int p : needed)
-        if (G.slot_of[p] < 0) w += datas[p];
+        if (G.slot_of[p] < 0 || !pg->slots[G.slot_of[p]].published) w += datas[p];
     return w;
 }
 

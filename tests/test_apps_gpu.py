@@ -159,6 +159,8 @@ def test_pagerank_app(graphs, tmp_path, name, memory):
     assert got.shape == ref.shape
     assert np.allclose(got, ref, rtol=PR_RTOL, atol=PR_ATOL), float(np.max(np.abs(got - ref) / ref))
     assert abs(float(got.astype(np.float64).sum()) - 1.0) < 1e-3
-    assert info["resident"] == (0 if memory else 1)
-    if memory:
+    page_bytes = S.PagedGraph.open(prefix, weighted=name == "wdir").npages * PAGE * 4
+    out_of_core = memory is not None and page_bytes > int(memory) << 20
+    assert info["resident"] == (0 if out_of_core else 1)
+    if out_of_core:
         assert info["h2d"] + info["zc"] > 0

@@ -154,9 +154,10 @@ def test_deeper_than_level_cap_is_an_error(use_graph):
     with pytest.raises(S.ScaphError) as ex:
         eng.bfs(0)
     assert ex.value.code == S.EUNSUPPORTED and "deeper than 4096" in str(ex.value)
-    # from the middle the traversal is 2100 levels deep: exact
+    # from the middle the depths reach 2100 (2101 levels, the last finding
+    # nothing): exact
     d, _, st = eng.bfs(2100)
-    assert np.array_equal(d, O.bfs(csr.idx, csr.ngh, 2100)) and st.levels == 2100
+    assert np.array_equal(d, O.bfs(csr.idx, csr.ngh, 2100)) and st.levels == 2101
     with pytest.raises(S.ScaphError) as ex:
         eng.msbfs([0, 5])
     assert ex.value.code == S.EUNSUPPORTED
