@@ -238,9 +238,13 @@ typedef struct scaph_config {
                                   compacted when they fit L2 / this; 0 = 3  */
     int32_t  ms_compact_min_deg;/* ... and the frontier has at least this
                                   many out-edges per vertex; 0 = 16        */
-    int32_t  pull_warp;        /* 1: pull levels run warp-centric (each warp
-                                  owns 512-vertex chunks, no CTA barriers);
-                                  0: CTA tiles of 4096 vertices             */
+    int32_t  pull_warp;        /* pull kernel shape: 0 CTA tiles of 4096
+                                  vertices; 1 warp-centric (each warp
+                                  compacts its own 512-vertex chunks); 2
+                                  vertex-parallel (lane = bit of the bitmap
+                                  word, coalesced records and depths, found
+                                  bits by ballot); 1 and 2 on levels that
+                                  read the 8-byte records                  */
     int64_t  push_defer_edges; /* a push level whose frontier has at least
                                   this many out-edges defers its claims: the
                                   neighbours' bits are OR-ed into the next

@@ -733,7 +733,148 @@ __device__ __forceinline__ void pull_body(const GraphDev &g, const BfsDev &s, ui
     // compaction by warp scan into its 512-entry slice of q, found bits in
     // its 16-word slice of fnd, phase B by the whole warp - so no CTA
     // barrier stands between a warp and its next chunk.
-    if (BLOCK <= 256 && s.pull_warp && s.prec) {
+    // Vertex-parallel variant (s.pull_warp == 2, records present): a warp
+    // takes kDenseWords bitmap words at a time and lane i handles bit i of
+    // each, so the record loads and depth stores of a word are one coalesced
+    // 256- or 128-byte access, the found bits are a warp ballot (one atomic
+    // per word), and there is no queue, scan or barrier at all; lanes whose
+    // vertex is visited idle instead.
+    if (s.pull_warp == 2 && s.prec) {
+        constexpr uint32_t kDenseWords = 4, kGroups = kPullTileWords / kDenseWords;
+        const int warp = threadIdx.x >> 5;
+        const uint32_t ngroups = ntiles * kGroups, warps = gridDim.x * (BLOCK / 32);
+        for (uint32_t gi = blockIdx.x * (BLOCK / 32) + warp; gi < ngroups; gi += warps) {
+            uint32_t rlo = vlo, rhi = vhi, local;
+            range_of_tile(rl, gi / kGroups, rlo, rhi, local);
+            const uint32_t rwhi = (uint32_t)(((unsigned long long)rhi + 31) >> 5);
+            const uint32_t w0 = (rlo >> 5) + local * kPullTileWords + (gi % kGroups) * kDenseWords;
+            uint32_t unv[kDenseWords];
+            uint32_t any = 0;
+#pragma unroll
+            for (uint32_t j = 0; j < kDenseWords; j++) {
+                const uint32_t w = w0 + j;
+                unv[j] = w < rwhi ? ~s.visited[w] & range_mask(w, rlo, rhi) : 0u;
+                any |= unv[j];
+            }
+            if (!any) continue;  // uniform: every lane read the same words
+            uint2 rec[kDenseWords];
+            uint32_t stat = 0;  // bit j: lane's vertex of word j is unvisited
+#pragma unroll
+            for (uint32_t j = 0; j < kDenseWords; j++) {
+                const bool act = (unv[j] >> lane) & 1u;
+                stat |= act ? 1u << j : 0u;
+                rec[j] = act ? ld_nc_v2(s.prec + (((w0 + j) << 5) + lane)) : make_uint2(0xFFFFFFFFu, 0u);
+            }
+            uint32_t found = 0, slow = 0, par[kDenseWords], dgs[kDenseWords];
+#pragma unroll
+            for (uint32_t j = 0; j < kDenseWords; j++) {
+                par[j] = kNoParent;
+                dgs[j] = rec[j].y & kPrecDegMax;
+                if (!((stat >> j) & 1u)) continue;
+                const uint32_t h0 = rec[j].x, nin = rec[j].y >> 28;
+                if (h0 < s.V && test_bit(s.front, h0)) {
+                    t.inspected += 1;
+                    par[j] = h0;
+                    found |= 1u << j;
+                } else if (nin <= 1) {
+                    t.inspected += nin;
+                } else {
+                    slow |= 1u << j;
+                }
+            }
+            // the rest: in-degree and ranked head row, then (rarely) the
+            // whole in-list, scanned by the warp
+#pragma unroll
+            for (uint32_t j = 0; j < kDenseWords; j++) {
+                const uint32_t v = ((w0 + j) << 5) + lane;
+                uint32_t need = 0, len = 0;
+                unsigned long long st = 0;
+                if ((slow >> j) & 1u) {
+                    len = __ldg(&s.indeg[v]);
+                    const uint4 h = ld_nc_v4(s.head + (size_t)kPullHead * v);
+                    uint32_t jj = 0;
+                    if (h.y < s.V && test_bit(s.front, h.y)) par[j] = h.y, jj = 2;
+                    else if (h.z < s.V && test_bit(s.front, h.z)) par[j] = h.z, jj = 3;
+                    else if (h.w < s.V && test_bit(s.front, h.w)) par[j] = h.w, jj = 4;
+                    if (jj) {
+                        t.inspected += jj;
+                        found |= 1u << j;
+                    } else {
+                        t.inspected += min(len, kPullSerial);
+                        int pg = -1;
+                        need = len > kPullSerial && list_start_w(v, pg, st) ? 1u : 0u;
+                    }
+                }
+                uint32_t todo = __ballot_sync(0xFFFFFFFFu, need);
+                while (todo) {
+                    const int src_lane = __ffs(todo) - 1;
+                    todo &= todo - 1;
+                    const uint32_t n = __shfl_sync(0xFFFFFFFFu, len, src_lane);
+                    const unsigned long long a = __shfl_sync(0xFFFFFFFFu, st, src_lane);
+                    const unsigned long long b = a + n, qa = a >> 2, qb = (b + 3) >> 2;
+                    uint32_t hit_par = kNoParent;
+                    unsigned long long hit_word = b;
+                    for (unsigned long long q0 = qa; q0 < qb; q0 += 32) {
+                        const unsigned long long qd = q0 + lane;
+                        uint32_t myhit = 0;
+                        uint4 val = make_uint4(0, 0, 0, 0);
+                        if (qd < qb) {
+                            val = ld_nc_v4(g.pool + qd * 4);
+                            const uint32_t vals[4] = {val.x, val.y, val.z, val.w};
+#pragma unroll
+                            for (int k = 0; k < 4; k++) {
+                                const unsigned long long word = qd * 4 + k;
+                                if (word >= a && word < b && vals[k] < s.V && test_bit(s.front, vals[k]))
+                                    myhit |= 1u << k;
+                            }
+                        }
+                        const uint32_t bal = __ballot_sync(0xFFFFFFFFu, myhit != 0);
+                        if (bal) {
+                            const int first = __ffs(bal) - 1;
+                            const uint32_t fh = __shfl_sync(0xFFFFFFFFu, myhit, first);
+                            const int k = __ffs(fh) - 1;
+                            const uint32_t pick = k == 0 ? val.x : k == 1 ? val.y : k == 2 ? val.z : val.w;
+                            hit_par = __shfl_sync(0xFFFFFFFFu, pick, first);
+                            hit_word = (q0 + first) * 4 + k;
+                            break;
+                        }
+                    }
+                    if (lane == src_lane) {
+                        t.inspected += (uint32_t)(hit_word - a) + (hit_par != kNoParent ? 1u : 0u);
+                        if (hit_par != kNoParent) {
+                            par[j] = hit_par;
+                            found |= 1u << j;
+                        }
+                    }
+                }
+            }
+#pragma unroll
+            for (uint32_t j = 0; j < kDenseWords; j++) {
+                const uint32_t v = ((w0 + j) << 5) + lane;
+                const bool f = (found >> j) & 1u;
+                const uint32_t mask = __ballot_sync(0xFFFFFFFFu, f);
+                if (!mask) continue;
+                if (f) {
+                    s.depth[v] = s.level + 1;
+                    if (s.parent) s.parent[v] = par[j];
+                    const uint32_t dv = dgs[j] == kPrecDegMax ? __ldg(&s.degree[v]) : dgs[j];
+                    t.next++;
+                    t.next_edges += dv;
+                    if (s.page_nodes) hist_add(sm, s, hist_same ? lut.of(v) : page_of(s.hg, v), dv + 3);
+                    hist_in_add(sm, s, v);
+                }
+                if (lane == 0) {
+                    // a word at a range boundary may belong to two ranges
+                    atomicOr(&s.visited[w0 + j], mask);
+                    atomicOr(&s.next[w0 + j], mask);
+                }
+            }
+        }
+        level_epilogue<BLOCK>(sm, s, t);
+        return;
+    }
+
+    if (BLOCK <= 256 && s.pull_warp == 1 && s.prec) {
         constexpr uint32_t kChunkWords = 16, kChunks = kPullTileWords / kChunkWords;
         static_assert(kChunkWords * 32 * (256 / 32) <= kPullTileWords * 32, "per-warp queues fit q");
         const int warp = threadIdx.x >> 5;

@@ -97,7 +97,7 @@ struct BfsDev {
     // into `next` (no per-edge atomic round trip, no scattered depth write)
     // and k_push_finalize then writes depths and counters word by word
     uint32_t push_defer;
-    uint32_t pull_warp;        // pull: warp-centric chunks instead of CTA tiles (needs prec)
+    uint32_t pull_warp;        // pull: 1 warp-centric chunks, 2 vertex-parallel words (needs prec)
 };
 
 // Second word of a pull record: the in-degree capped at 15 in the top four
