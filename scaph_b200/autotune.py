@@ -168,7 +168,9 @@ def tune_engine(eng: Engine, sources, ptr: int, multi: bool = False, repeats: in
     alpha, beta.  Each candidate is timed best of `repeats` (device time);
     the default's spread over `repeats` more runs is reported beside the
     result, so a gain can be told from noise.  The chosen tunables must
-    reproduce the default's depths (checksum).  Sets and returns them."""
+    reproduce the default's depths (checksum).  The best setting is adopted
+    only if it beats the default by more than the default's spread; the
+    adopted one is set and returned under "params"."""
     t0 = time.time()
     start = eng.tunables()
     ref_sum = _engine_checksum(eng, sources, multi)
@@ -196,10 +198,15 @@ def tune_engine(eng: Engine, sources, ptr: int, multi: bool = False, repeats: in
         for v in values:
             if v != best[name]:
                 trial(dict(best, **{name: v}))
-    eng.tune(**best)
+    # a setting is adopted only if its gain exceeds the default's own
+    # run-to-run spread; otherwise the defaults stay (a gain within noise
+    # on the tuning sources does not carry over to other sources)
+    beyond = best_ms < min(runs) - (max(runs) - min(runs))
+    chosen = best if beyond else start
+    eng.tune(**chosen)
     if _engine_checksum(eng, sources, multi) != ref_sum:
         eng.tune(**start)
         raise RuntimeError("tuned engine parameters changed the depths")
-    return {"params": best, "ms": best_ms, "default_ms": default_ms,
+    return {"params": chosen, "best_params": best, "ms": best_ms, "default_ms": default_ms,
             "default_spread_ms": [min(runs), max(runs)], "tried": tried, "seconds": time.time() - t0,
-            "gain_beyond_noise": best_ms < min(runs) - (max(runs) - min(runs))}
+            "gain_beyond_noise": beyond, "adopted": "tuned" if beyond else "defaults"}
