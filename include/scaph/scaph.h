@@ -238,18 +238,19 @@ typedef struct scaph_config {
                                   compacted when they fit L2 / this; 0 = 3  */
     int32_t  ms_compact_min_deg;/* ... and the frontier has at least this
                                   many out-edges per vertex; 0 = 16        */
-    int32_t  pull_warp;        /* pull kernel shape: 0 CTA tiles of 4096
-                                  vertices; 1 warp-centric (each warp
+    int32_t  pull_warp;        /* pull kernel shape on levels that read the
+                                  8-byte records: 1 warp-centric (each warp
                                   compacts its own 512-vertex chunks); 2
                                   vertex-parallel (lane = bit of the bitmap
                                   word, coalesced records and depths, found
-                                  bits by ballot); 1 and 2 on levels that
-                                  read the 8-byte records                  */
+                                  bits by ballot); 3 CTA tiles of 4096
+                                  vertices; 0 = 1 (other levels: tiles)     */
     int64_t  push_defer_edges; /* a push level whose frontier has at least
                                   this many out-edges defers its claims: the
                                   neighbours' bits are OR-ed into the next
                                   frontier and one pass then writes depths
-                                  word by word (not with parents); 0 = never */
+                                  word by word (not with parents); 0 = 2^20,
+                                  negative = never                         */
     int32_t  pull_records;     /* pull phase A from the 8-byte per-vertex
                                   records: 0 = on levels whose frontier has
                                   at least a quarter as many vertices as the

@@ -580,7 +580,7 @@ class Engine:
         _check(lib().scaph_engine_tune(self._h, C.byref(self._cfg)))
 
     _TUNABLE_DEFAULTS = {"giant_edges": 1024, "pull_gather_ratio": 64, "ms_compact_l2_div": 3,
-                         "ms_compact_min_deg": 16}
+                         "ms_compact_min_deg": 16, "push_defer_edges": 1 << 20, "pull_warp": 1}
 
     def tunables(self) -> dict:
         """The tunables in force (0 fields shown as the defaults they mean)."""

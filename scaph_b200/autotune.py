@@ -136,7 +136,7 @@ GATHER = (16, 32, 64, 128, 256)
 CTAS = (0, 2, 3, 4, 6, 8)  # 0: the occupancy limit
 MS_L2_DIV = (2, 3, 4, 6, 8)
 MS_MIN_DEG = (4, 8, 16, 32, 64)
-DEFER = (0, 1 << 16, 1 << 20, 1 << 24)  # frontier out-edges from which push defers its claims
+DEFER = (-1, 1 << 16, 1 << 20, 1 << 24)  # frontier out-edges from which push defers its claims (-1 never)
 
 
 def _engine_run(eng: Engine, sources, ptr: int, multi: bool) -> float:
@@ -192,7 +192,7 @@ def tune_engine(eng: Engine, sources, ptr: int, multi: bool = False, repeats: in
         axes = (("ms_compact_l2_div", MS_L2_DIV), ("ms_compact_min_deg", MS_MIN_DEG), ("alpha", ALPHAS),
                 ("beta", BETAS))
     else:
-        axes = (("pull_records", (0, 1, 2)), ("pull_warp", (0, 1, 2)), ("push_defer_edges", DEFER), ("ctas_per_sm", CTAS), ("giant_edges", GIANT),
+        axes = (("pull_records", (0, 1, 2)), ("pull_warp", (1, 2, 3)), ("push_defer_edges", DEFER), ("ctas_per_sm", CTAS), ("giant_edges", GIANT),
                 ("pull_gather_ratio", GATHER), ("alpha", ALPHAS), ("beta", BETAS))
     for name, values in axes:
         for v in values:

@@ -58,6 +58,13 @@ constexpr int kPushTileWords = 128;                  // frontier-bitmap words pe
 constexpr int kPullPerThread = SCAPH_PULL_PER_THREAD;  // unvisited vertices each thread takes per pull round
 constexpr int kPullTileWords = 128;                  // visited-bitmap words per pull tile (the range-list tile)
 constexpr int kPullMinThreads = SCAPH_PULL_MINB;     // resident threads per SM the pull kernel is compiled for
+#ifndef SCAPH_PUSH_MINB
+#define SCAPH_PUSH_MINB 1024
+#endif
+// resident threads per SM the push kernels are compiled for: 4 CTAs of 256
+// threads get 64 registers (the graph-mode kernel's level-state setup
+// spilled at the 48 registers that 5 CTAs allow)
+constexpr int kPushMinThreads = SCAPH_PUSH_MINB;
 constexpr uint32_t kPullSerial = SCAPH_PULL_SERIAL;  // in-edges each lane probes before the warp helps
 static_assert(kPullSerial == kPullHead, "phase A reads one dense head row of in-edges");
 
@@ -261,7 +268,7 @@ __device__ __forceinline__ void visit4(LevelSmem &sm, const BfsDev &s, ThreadAcc
                 continue;
             }
             if (!((vw[j] >> (u[j] & 31)) & 1u))
-                asm volatile("red.global.or.b32 [%0], %1;" ::"l"(s.next + (u[j] >> 5)), "r"(1u << (u[j] & 31)));
+                atomicOr(s.next + (u[j] >> 5), 1u << (u[j] & 31));  // result unused: a reduction
         }
         return;
     }
@@ -1166,7 +1173,7 @@ __device__ __forceinline__ unsigned long long globaltimer()
 // kernels: host-argument versions
 // ---------------------------------------------------------------------------
 template <int BLOCK>
-__global__ void __launch_bounds__(BLOCK) k_push(GraphDev g, BfsDev s, uint32_t vlo, uint32_t vhi, RangeList rl)
+__global__ void __launch_bounds__(BLOCK, kPushMinThreads / BLOCK) k_push(GraphDev g, BfsDev s, uint32_t vlo, uint32_t vhi, RangeList rl)
 {
     push_body<BLOCK>(g, s, vlo, vhi, rl);
 }
@@ -1197,7 +1204,7 @@ __global__ void __launch_bounds__(BLOCK) k_push_finalize(BfsDev s)
 // the level's direction (decided on the device) does not select leaves at
 // once, which costs less than a conditional node per direction.
 template <int BLOCK>
-__global__ void __launch_bounds__(BLOCK) k_push_g(GraphDev g, BfsGraphArgs a)
+__global__ void __launch_bounds__(BLOCK, kPushMinThreads / BLOCK) k_push_g(GraphDev g, BfsGraphArgs a)
 {
     if (a.ctl->dir != 0) return;
     const BfsDev s = level_state(a);

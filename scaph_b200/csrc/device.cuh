@@ -100,6 +100,11 @@ struct BfsDev {
     uint32_t pull_warp;        // pull: 1 warp-centric chunks, 2 vertex-parallel words (needs prec)
 };
 
+// Default of scaph_config.push_defer_edges: push levels whose frontier has
+// at least 2^20 out-edges defer their claims (RMAT-24, 8 sources, graph
+// mode: 508 -> 521 GTEPS alone, 537 with the warp-centric pull).
+constexpr long long kDeferEdgesDefault = 1ll << 20;
+
 // Second word of a pull record: the in-degree capped at 15 in the top four
 // bits (phase A needs to know only whether it exceeds the probes already
 // made), the out-degree below them; an out-degree of kPrecDegMax or more is

@@ -128,7 +128,7 @@ BfsDev scaph_engine::base_state(uint32_t *dd, uint32_t *dp) const
     s.head_ranked = head_ranked ? 1u : 0u;
     s.prec = d_prec;
     s.giant_edges = (uint32_t)cfg.giant_edges;
-    s.pull_warp = (uint32_t)cfg.pull_warp;
+    s.pull_warp = cfg.pull_warp == 3 ? 0u : (uint32_t)cfg.pull_warp;  // kernel: 0 tiles, 1 warp, 2 lanes
     return s;
 }
 
@@ -152,9 +152,9 @@ int scaph_engine::create(const Graph *g_, const Graph *gt_, const scaph_config *
     if (cfg.pull_gather_ratio <= 0) cfg.pull_gather_ratio = (int32_t)kPullGatherRatio;
     if (cfg.ms_compact_l2_div <= 0) cfg.ms_compact_l2_div = 3;
     if (cfg.ms_compact_min_deg <= 0) cfg.ms_compact_min_deg = 16;
-    if (cfg.push_defer_edges < 0) cfg.push_defer_edges = 0;
+    if (cfg.push_defer_edges == 0) cfg.push_defer_edges = kDeferEdgesDefault;
     if (cfg.pull_records < 0 || cfg.pull_records > 2) cfg.pull_records = 0;
-    if (cfg.pull_warp < 0 || cfg.pull_warp > 2) cfg.pull_warp = 0;
+    if (cfg.pull_warp < 1 || cfg.pull_warp > 3) cfg.pull_warp = 1;
     device = cfg.device;
     if (g->weighted) return set_error(SCAPH_EUNSUPPORTED, "BFS engine needs unweighted pages");
     if (gt && (gt->V != V || gt->E != E || gt->weighted))
@@ -679,7 +679,7 @@ int scaph_engine::build_graph()
     dargs.beta = cfg.beta;
     dargs.max_levels = kMaxLevels;
     dargs.gather_ratio = (uint32_t)cfg.pull_gather_ratio;
-    dargs.defer_edges = (unsigned long long)cfg.push_defer_edges;
+    dargs.defer_edges = cfg.push_defer_edges > 0 ? (unsigned long long)cfg.push_defer_edges : 0ull;
     dargs.pull_records = cfg.pull_records;
 
     // init (run inputs are this node's arguments, replaced per launch)
@@ -1045,8 +1045,8 @@ int scaph_engine_tune(scaph_engine *e, const scaph_config *c)
     k.ms_compact_l2_div = c->ms_compact_l2_div > 0 ? c->ms_compact_l2_div : 3;
     k.ms_compact_min_deg = c->ms_compact_min_deg > 0 ? c->ms_compact_min_deg : 16;
     k.ctas_per_sm = c->ctas_per_sm;
-    k.push_defer_edges = c->push_defer_edges > 0 ? c->push_defer_edges : 0;
-    k.pull_warp = c->pull_warp >= 0 && c->pull_warp <= 2 ? c->pull_warp : 0;
+    k.push_defer_edges = c->push_defer_edges == 0 ? kDeferEdgesDefault : c->push_defer_edges;
+    k.pull_warp = c->pull_warp >= 1 && c->pull_warp <= 3 ? c->pull_warp : 1;
     k.pull_records = c->pull_records >= 0 && c->pull_records <= 2 ? c->pull_records : 0;
     e->block = c->block_size ? c->block_size : 256;
     const int occ_push = std::max(1, level_occupancy(0, e->block)), occ_pull = std::max(1, level_occupancy(1, e->block));

@@ -26,7 +26,8 @@ def rmat15():
                                 dict(pull_warp=1, alpha=0.01, beta=0.001), dict(pull_warp=1, block_size=128),
                                 dict(pull_records=1), dict(pull_records=2), dict(pull_records=1, pull_warp=1),
                                 dict(pull_warp=2, pull_records=1), dict(pull_warp=2, pull_records=1, alpha=0.01, beta=0.001),
-                                dict(pull_warp=2, pull_records=1, block_size=512)])
+                                dict(pull_warp=2, pull_records=1, block_size=512), dict(pull_warp=3, pull_records=1),
+                                dict(push_defer_edges=-1)])
 def test_tunables_keep_depths(rmat15, kw):
     """push_defer_edges=1 defers the claims of every push level (neighbours
     OR-ed into the next frontier, depths written by the finalize pass);
