@@ -881,7 +881,7 @@ __device__ __forceinline__ void pull_body(const GraphDev &g, const BfsDev &s, ui
         return;
     }
 
-    if (BLOCK <= 256 && s.pull_warp == 1 && s.prec) {
+    if (BLOCK <= 256 && s.pull_warp == 1 && (s.prec || s.head)) {
         constexpr uint32_t kChunkWords = 16, kChunks = kPullTileWords / kChunkWords;
         static_assert(kChunkWords * 32 * (256 / 32) <= kPullTileWords * 32, "per-warp queues fit q");
         const int warp = threadIdx.x >> 5;
@@ -933,7 +933,18 @@ __device__ __forceinline__ void pull_body(const GraphDev &g, const BfsDev &s, ui
                 for (int i = 0; i < kPPT; i++) {
                     const uint32_t k = k0 + i * 32 + lane;
                     vv[i] = k < total ? qw[k] : 0xFFFFFFFFu;
-                    rec[i] = vv[i] != 0xFFFFFFFFu ? ld_nc_v2(s.prec + vv[i]) : make_uint2(0xFFFFFFFFu, 0u);
+                    if (vv[i] == 0xFFFFFFFFu) {
+                        rec[i] = make_uint2(0xFFFFFFFFu, 0u);
+                    } else if (s.prec) {
+                        rec[i] = ld_nc_v2(s.prec + vv[i]);
+                    } else {
+                        // level without records: the head row, in-degree and
+                        // out-degree issued together, folded into a record
+                        // (a miss re-reads the row from L1)
+                        const uint32_t h0 = __ldg(s.head + (size_t)kPullHead * vv[i]);
+                        const uint32_t n = __ldg(&s.indeg[vv[i]]), d = __ldg(&s.degree[vv[i]]);
+                        rec[i] = make_uint2(h0, pull_meta(n, d));
+                    }
                 }
 #pragma unroll
                 for (int i = 0; i < kPPT; i++) {
