@@ -1267,12 +1267,22 @@ __global__ void k_graph_init(BfsGraphArgs a, uint32_t *depth, uint32_t *parent, 
     }
     const size_t stride = (size_t)gridDim.x * blockDim.x;
     const size_t i0 = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-    for (size_t i = i0; i < b.V; i += stride) {
-        depth[i] = unreached;
-        if (parent) parent[i] = kNoParent;
-    }
+    // 16-byte stores where the array allows (the depth fill is most of this
+    // kernel: 4 bytes per vertex)
+    auto fill = [&](uint32_t *p, uint32_t value, size_t n) {
+        size_t done = 0;
+        if ((reinterpret_cast<uintptr_t>(p) & 15) == 0) {
+            const uint4 v4 = make_uint4(value, value, value, value);
+            const size_t n4 = n / 4;
+            for (size_t i = i0; i < n4; i += stride) reinterpret_cast<uint4 *>(p)[i] = v4;
+            done = n4 * 4;
+        }
+        for (size_t i = done + i0; i < n; i += stride) p[i] = value;
+    };
+    fill(depth, unreached, b.V);
+    if (parent) fill(parent, kNoParent, b.V);
     for (size_t i = i0; i < b.nwords; i += stride) b.visited[i] = dead ? dead[i] : 0u;
-    for (size_t i = i0; i < 3ull * b.nwords; i += stride) a.bm3[i] = 0u;
+    fill(a.bm3, 0u, 3ull * b.nwords);
     uint32_t *cw = reinterpret_cast<uint32_t *>(a.ctr0);
     const size_t nc = (size_t)nlevels_clear * sizeof(LevelCounters) / 4;
     for (size_t i = i0; i < nc; i += stride) cw[i] = 0u;
