@@ -339,9 +339,13 @@ static int ms_run(scaph_engine *e, const uint32_t *srcs, int nsrc, uint32_t *out
             // the traffic rule for direction, and takes the page outputs
             mlp_forward_host(e->sched_host, f.data(), y.data());
         }
-        if (e->pager && learned && level > 0) {
+        if (e->pager && learned && !net_on && level > 0) {
             // the exact page traffic each direction would cause overrides
-            // the kernel-time choice when one side clearly dominates
+            // the kernel-time choice when one side clearly dominates (not
+            // with the network's prefetch: prefetched out-pages make every
+            // push look free of traffic, and the batch then pushes levels
+            // that pull serves faster - measured on config 5: 8 push levels,
+            // 0.77x of alpha/beta cold)
             double tp = 0, tq = 0;
             ms_transfer_ms(e, lp, tp, tq);
             if (tp > 2 * tq + 1.0) dir = 1;
