@@ -238,14 +238,13 @@ typedef struct scaph_config {
                                   compacted when they fit L2 / this; 0 = 3  */
     int32_t  ms_compact_min_deg;/* ... and the frontier has at least this
                                   many out-edges per vertex; 0 = 16        */
-    int32_t  pull_warp;        /* pull kernel shape: 1 warp-centric (each
-                                  warp compacts its own 512-vertex chunks;
-                                  every level); 2 vertex-parallel (lane =
-                                  bit of the bitmap word, coalesced records
-                                  and depths, found bits by ballot; levels
-                                  that read the 8-byte records, tiles on the
-                                  others); 3 CTA tiles of 4096 vertices;
-                                  0 = 1                                    */
+    int32_t  pull_warp;        /* pull kernel shape on levels that read the
+                                  8-byte records (CTA tiles on the others):
+                                  1 warp-centric (each warp compacts its own
+                                  512-vertex chunks); 2 vertex-parallel (lane
+                                  = bit of the bitmap word, coalesced records
+                                  and depths, found bits by ballot); 3 CTA
+                                  tiles of 4096 vertices; 0 = 1             */
     int64_t  push_defer_edges; /* a push level whose frontier has at least
                                   this many out-edges defers its claims: the
                                   neighbours' bits are OR-ed into the next

@@ -199,9 +199,19 @@ def tune_engine(eng: Engine, sources, ptr: int, multi: bool = False, repeats: in
             if v != best[name]:
                 trial(dict(best, **{name: v}))
     # a setting is adopted only if its gain exceeds the default's own
-    # run-to-run spread; otherwise the defaults stay (a gain within noise
-    # on the tuning sources does not carry over to other sources)
+    # run-to-run spread and holds up when the two are timed again in turns
+    # (the best of many noisy candidates beats the default by luck alone);
+    # otherwise the defaults stay
     beyond = best_ms < min(runs) - (max(runs) - min(runs))
+    if beyond and best != start:
+        wins = 0
+        for _ in range(3):
+            eng.tune(**start)
+            d = min(_engine_run(eng, sources, ptr, multi) for _ in range(repeats))
+            eng.tune(**best)
+            b = min(_engine_run(eng, sources, ptr, multi) for _ in range(repeats))
+            wins += b < 0.99 * d
+        beyond = wins == 3
     chosen = best if beyond else start
     eng.tune(**chosen)
     if _engine_checksum(eng, sources, multi) != ref_sum:

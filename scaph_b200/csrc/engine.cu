@@ -487,8 +487,21 @@ int scaph_engine::run_host_loop(uint32_t src, uint32_t *dd, uint32_t *dp)
                 y.resize(out);
                 mlp_forward_host(sched_host, f.data(), y.data());
                 if (level > 0) {
-                    // the network models kernel time (trained resident)
-                    dir = y[0] > 0.f ? 1 : 0;
+                    // the network models kernel time (trained on resident
+                    // rows, residency features 1): out of core its direction
+                    // comes from the same row with the residency features at
+                    // 1 (the traffic rule below prices the pages); fed the
+                    // real residency it strayed out of its training inputs
+                    // (config 3 warm: same bytes moved, 0.81x of alpha/beta)
+                    float ydir = y[0];
+                    if (pager) {
+                        std::vector<float> fr(f);
+                        fr[10] = fr[11] = fr[12] = fr[13] = 1.f;
+                        std::vector<float> yr(y.size());
+                        mlp_forward_host(sched_host, fr.data(), yr.data());
+                        ydir = yr[0];
+                    }
+                    dir = ydir > 0.f ? 1 : 0;
                     // far from the alpha/beta threshold the rule decides
                     const int sure = alpha_beta_confident(prev_dir, nf, mf, mu, V, cfg.alpha, cfg.beta);
                     if (sure >= 0) dir = sure;
