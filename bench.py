@@ -59,7 +59,7 @@ def parse_args():
     ap.add_argument("--no-config5", action="store_true",
                     help="skip the 105M-vertex / 3.7B-edge web graph (about a minute to generate)")
     ap.add_argument("--only-extra", default=None, help=argparse.SUPPRESS)
-    ap.add_argument("--no-tune", action="store_true", help="keep the engine's default tunables")
+    ap.add_argument("--no-tune", action="store_true", help="skip the autotuner report")
     ap.add_argument("--host-loop", action="store_true",
                     help="time the host-driven level loop (one launch per level kernel) instead of one "
                          "CUDA-graph launch per BFS; for profilers that time kernels one launch at a time")
@@ -439,7 +439,7 @@ def _run_set(S, g, gt, srcs, pool, net=None, cold=False, warm_pass=True, digests
     if warm_pass and not cold:
         for s in srcs:
             eng.bfs(s)
-    ms, h2d, zc, alg, levels = 0.0, 0, 0, 0, 0
+    ms, h2d, zc, alg, levels, level_ms = 0.0, 0, 0, 0, 0, 0.0
     for s in srcs:
         if cold:
             eng.evict_all()
@@ -449,10 +449,11 @@ def _run_set(S, g, gt, srcs, pool, net=None, cold=False, warm_pass=True, digests
         zc += st.zc_bytes
         alg += st.pcie_alg_bytes
         levels += st.levels
+        level_ms += sum(t["ms"] for t in eng.trace())
         if digests is not None and s in digests:
             digests[s].append(_digest(d))
     eng.close()
-    return {"ms": ms, "h2d_bytes": h2d, "zc_bytes": zc, "pcie_alg_bytes": alg, "levels": levels}
+    return {"ms": ms, "h2d_bytes": h2d, "zc_bytes": zc, "pcie_alg_bytes": alg, "levels": levels, "level_ms": level_ms}
 
 
 def extra_config3(nsrc_train=32, nsrc_eval=32, nsrc_oracle=16):
@@ -502,6 +503,9 @@ def extra_config3(nsrc_train=32, nsrc_eval=32, nsrc_oracle=16):
             "plain_pcie_alg_bytes_per_level": plain["pcie_alg_bytes"] / max(1, plain["levels"]),
             "learned_pcie_alg_bytes_per_level": learned["pcie_alg_bytes"] / max(1, learned["levels"]),
             "plain_ms": plain["ms"], "learned_ms": learned["ms"],
+            # device time inside the levels (the rest of ms is the host loop
+            # between them: page decisions, features, the network)
+            "plain_level_ms": plain["level_ms"], "learned_level_ms": learned["level_ms"],
             "plain_moved_bytes": plain["h2d_bytes"] + plain["zc_bytes"],
             "learned_moved_bytes": learned["h2d_bytes"] + learned["zc_bytes"]}
     # the checker: oracle depths of the checked held-out sources against the
@@ -695,14 +699,18 @@ def run_ours(args, world):
     torch.cuda.set_stream(stream)
     eng = S.Engine(g, device=local_rank, stream=stream.cuda_stream, use_graph=2 if args.host_loop else 0)
     depth = torch.empty(V, dtype=torch.int32, device="cuda")
-    # the engine's tunables, picked by the autotuner on 8 other sources of
-    # the same graph (untimed)
+    # The autotuner on 8 other sources of the same graph, on a separate
+    # engine, reported beside the line: the timed engine keeps the library's
+    # defaults (A/B runs on whole traversals chose them; a winner on 8
+    # tuning sources did not carry over to the timed ones in earlier runs).
     tune = None
     if not args.no_tune:
         from scaph_b200 import autotune
 
-        tune = autotune.tune_engine(eng, workloads.random_sources(csr, 8, workloads.SEED_BASE + 201),
+        eng_t = S.Engine(g, device=local_rank, stream=stream.cuda_stream)
+        tune = autotune.tune_engine(eng_t, workloads.random_sources(csr, 8, workloads.SEED_BASE + 201),
                                     depth.data_ptr())
+        eng_t.close()
 
     order = replicas.rank_sources(srcs, rank, max(args.steps, args.warmup))
 
@@ -788,8 +796,6 @@ def run_ours(args, world):
     # source (separate, untimed pass)
     per_dir = {0: [0, 0.0, 0], 1: [0, 0.0, 0]}  # alg bytes, ms, launches
     eng_h = S.Engine(g, device=local_rank, stream=stream.cuda_stream, use_graph=2)  # per-level CUDA events
-    if tune:
-        eng_h.tune(**tune["params"])
     for s in srcs:
         eng_h.bfs(s)
         for t in eng_h.trace():

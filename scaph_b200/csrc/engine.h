@@ -75,6 +75,8 @@ int pager_nslots(const Pager *pg);
 // Slots holding no page.
 int pager_free_slots(const Pager *pg);
 float pager_resident_fraction(const Pager *pg, int gid, const std::vector<int> *pages);
+// Page p of graph gid holds a pool slot (copied, or being copied).
+bool pager_is_resident(const Pager *pg, int gid, int p);
 // Active words sum(deg*ew+3) of the needed pages that are not resident: the
 // least a level must bring over the link (get_page_info's `datas`,
 // src/gpu_engine.cuh:413-419, over the pages the pool lacks).

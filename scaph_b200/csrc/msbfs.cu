@@ -8,6 +8,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
 #include <cstring>
 
 #include "engine.h"
@@ -355,19 +356,20 @@ static int ms_run(scaph_engine *e, const uint32_t *srcs, int nsrc, uint32_t *out
             // during a push level: the out-pages the network expects to hold
             // frontier vertices next level that this level does not read
             // itself (a batch's union frontier makes a page it enters dense,
-            // so such a page is copied whole anyway) - but only while the
-            // free slots can also take every page the rest of the traversal
-            // may still load (the in-pages for pull levels, the missing
-            // out-pages): a prefetched page evicted before its use is read
-            // twice (config 5 cold without this rule: 27.6 GB moved against
+            // so such a page is copied whole anyway) - but only into the
+            // free slots beyond those the missing in-pages will need for the
+            // pull levels: a prefetched page evicted before its use is read
+            // twice (config 5 cold with no reserve: 27.6 GB moved against
             // alpha/beta's 16.1 GB, 0.65x)
             const int gin = e->symmetric ? 0 : 1;
-            const float miss_out = 1.f - pager_resident_fraction(e->pager, 0, nullptr);
-            const float miss_in = gin ? 1.f - pager_resident_fraction(e->pager, gin, nullptr) : 0.f;
-            const double still = miss_out * (double)np + miss_in * (double)(e->gt ? e->gt->pages.size() : 0);
-            if ((double)pager_free_slots(e->pager) >= still)
-                for (int p = 0; p + 1 < (int)y.size() && p < (int)np; p++)
-                    if (y[1 + p] > 2.f && lp.push_cnt[p] == 0) prefetch_pages.push_back(p);
+            const double miss_in =
+                gin ? (1.0 - pager_resident_fraction(e->pager, gin, nullptr)) * (double)e->gt->pages.size() : 0.0;
+            long long room = (long long)pager_free_slots(e->pager) - (long long)std::ceil(miss_in);
+            for (int p = 0; p + 1 < (int)y.size() && p < (int)np && room > 0; p++)
+                if (y[1 + p] > 2.f && lp.push_cnt[p] == 0 && !pager_is_resident(e->pager, 0, p)) {
+                    prefetch_pages.push_back(p);
+                    room--;
+                }
         }
         const uint32_t d = (uint32_t)level + 1;
         for (int k = 0; k < kMsPlanes; k++) {

@@ -651,6 +651,8 @@ int pager_free_slots(const Pager *pg)
     return n;
 }
 
+bool pager_is_resident(const Pager *pg, int gid, int p) { return pg->gs[gid].slot_of[p] >= 0; }
+
 float pager_resident_fraction(const Pager *pg, int gid, const std::vector<int> *pages)
 {
     const Pager::GState &G = pg->gs[gid];
