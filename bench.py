@@ -456,6 +456,53 @@ def _run_set(S, g, gt, srcs, pool, net=None, cold=False, warm_pass=True, digests
     return {"ms": ms, "h2d_bytes": h2d, "zc_bytes": zc, "pcie_alg_bytes": alg, "levels": levels, "level_ms": level_ms}
 
 
+def extra_config2_learned(stream, nsrc_train=16):
+    """The headline graph (RMAT-24 in HBM) with the learned direction: the
+    network trained on dual-timed plain runs of 16 other sources, evaluated
+    on the 64 headline sources as one CUDA-graph launch each (the decision
+    runs on the device, k_decide_learned), against the plain alpha/beta
+    engine on the same sources; depths compared with the plain engine's."""
+    import torch
+
+    import scaph_b200 as S
+    from scaph_b200 import scheduler, workloads
+
+    csr, srcs = workloads.config2()
+    g = workloads.paged(csr)
+    train = [s for s in workloads.random_sources(csr, nsrc_train + len(srcs), workloads.SEED_BASE + 205)
+             if s not in set(srcs)][:nsrc_train]
+    traces = scheduler.collect(g, None, train)
+    net, info = scheduler.train(traces, g, None, g.npages, 0.0, epochs=200)
+    d0 = torch.empty(csr.V, dtype=torch.int32, device="cuda")
+    d1 = torch.empty(csr.V, dtype=torch.int32, device="cuda")
+    plain = S.Engine(g, stream=stream.cuda_stream)
+    learned = S.Engine(g, stream=stream.cuda_stream, direction=S.DIR_LEARNED)
+    learned.set_scheduler(net)
+    exact = True
+    for s in srcs:
+        plain.bfs_device(s, d0.data_ptr())
+        learned.bfs_device(s, d1.data_ptr())
+        exact &= bool(torch.equal(d0, d1))
+    out = {"graph": "RMAT-24 ef16 (the headline graph)", "train_sources": len(train), "eval_sources": len(srcs),
+           "training": info, "depths_equal_plain": exact}
+    for name, eng, d in (("plain", plain, d0), ("learned", learned, d1)):
+        for s in srcs[:3]:
+            eng.bfs_async(s, d.data_ptr())
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(4):
+            for s in srcs:
+                eng.bfs_async(s, d.data_ptr())
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / (4 * len(srcs))
+        out[name] = {"ms_per_bfs": ms, "gteps": csr.E / (ms / 1e3) / 1e9}
+        eng.close()
+    out["speedup"] = out["plain"]["ms_per_bfs"] / out["learned"]["ms_per_bfs"]
+    return out
+
+
 def extra_config3(nsrc_train=32, nsrc_eval=32, nsrc_oracle=16):
     """Directed power law 41.6M / 1.47B: the learned scheduler (trained on
     dual-timed plain runs of 32 sources) against alpha/beta + demand paging
@@ -844,7 +891,7 @@ def run_ours(args, world):
         # each configuration in its own process: a fresh host heap for the big
         # generated graphs, and a failure there cannot take the headline down
         extras = {}
-        names = ["pcie", "config1", "config4a_batched", "config4b_mixed", "config3_learned"]
+        names = ["pcie", "config1", "config4a_batched", "config4b_mixed", "config2_learned", "config3_learned"]
         if not args.no_config5:
             names.append("config5_ooc_batched")
         for name in names:
@@ -872,6 +919,7 @@ EXTRAS = {
     "config4a_batched": lambda st: extra_config4a(st),
     "config4b_mixed": lambda st: extra_config4b(st),
     "config3_learned": lambda st: extra_config3(),
+    "config2_learned": lambda st: extra_config2_learned(st),
     "config5_ooc_batched": lambda st: extra_config5(st),
 }
 
