@@ -575,8 +575,9 @@ def extra_config5(stream, nsrc=128, nplain=8, ntrain=8):
     pool: 128 sources per multi-source launch - with alpha/beta, with the
     scheduler's page-traffic rule alone, and with the learned scheduler
     (network trained on this graph's plain-engine traces and on two
-    multi-source batches of other sources; it picks directions near the
-    switch point and prefetches the pages it predicts for the next level) -
+    multi-source batches of other sources; direction stays alpha/beta, and
+    the push levels the network or the frontier's growth mark as leading
+    into the pull levels prefetch the in-pages the first pull level reads) -
     against the plain engine (one source per launch, alpha/beta + demand
     paging), warm and cold pools."""
     import torch
@@ -628,7 +629,9 @@ def extra_config5(stream, nsrc=128, nplain=8, ntrain=8):
                            "page_faults": st.page_faults, "prefetched": st.prefetched, "levels": st.levels,
                            "pcie_bytes_per_level": (st.h2d_bytes + st.zc_bytes) / max(1, st.levels),
                            "pcie_alg_bytes_per_level": st.pcie_alg_bytes / max(1, st.levels),
-                           "directions": "".join("p" if t["direction"] else "P" for t in tr)}
+                           "directions": "".join("p" if t["direction"] else "P" for t in tr),
+                           "level_ms": [round(float(t["ms"]), 2) for t in tr],
+                           "level_h2d_mb": [round(int(t["h2d_bytes"]) / 1e6, 1) for t in tr]}
         out[name] = res
         eng.close()
     # plain engine, one source per launch, on the first sources

@@ -256,7 +256,19 @@ typedef struct scaph_config {
                                   at least a quarter as many vertices as the
                                   unvisited set (the top-ranked probe mostly
                                   hits there), 1 = every level, 2 = never   */
-    int32_t  _reserved1;
+    int32_t  pull_rows;        /* pull phase A on levels without the 8-byte
+                                  records: 1 = one 16-byte row per vertex
+                                  (three ranked in-neighbours and the
+                                  degrees; 16 bytes of HBM per vertex, built
+                                  when first asked for); 0 or 2 = the
+                                  in-degree, 16-byte head row (four ranked
+                                  in-neighbours) and out-degree arrays      */
+    int32_t  push_sparse_ratio;/* a push level whose frontier has fewer than
+                                  one vertex per this many reads its
+                                  frontier words as one contiguous run per
+                                  CTA and expands them together (whole-
+                                  graph ranges); 0 = 16, negative = never  */
+    int32_t  _reserved2;
 } scaph_config;
 
 typedef struct scaph_engine scaph_engine;
@@ -306,8 +318,9 @@ int scaph_bfs(scaph_engine *e, uint32_t src, uint32_t *depths, uint32_t *parents
               int out_on_device, scaph_bfs_stats *stats);
 /* Sets an engine's run-time tunables from cfg: alpha, beta, block_size,
  * ctas_per_sm, giant_edges, pull_gather_ratio, ms_compact_l2_div,
- * ms_compact_min_deg, pull_warp, push_defer_edges and pull_records (0 =
- * default; the other fields are ignored).  They
+ * ms_compact_min_deg, pull_warp, push_defer_edges, pull_records,
+ * pull_rows and push_sparse_ratio (0 = default; the other fields are
+ * ignored).  They
  * change the schedule only, never the depths.  Waits for the engine's work
  * and drops its CUDA graph (the next run rebuilds it).  Replaces setting
  * FLAGS_num_blks / FLAGS_num_thds between runs (src/app.cuh:38-52). */

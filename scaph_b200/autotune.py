@@ -192,7 +192,9 @@ def tune_engine(eng: Engine, sources, ptr: int, multi: bool = False, repeats: in
         axes = (("ms_compact_l2_div", MS_L2_DIV), ("ms_compact_min_deg", MS_MIN_DEG), ("alpha", ALPHAS),
                 ("beta", BETAS))
     else:
-        axes = (("pull_records", (0, 1, 2)), ("pull_warp", (1, 2, 3)), ("push_defer_edges", DEFER), ("ctas_per_sm", CTAS), ("giant_edges", GIANT),
+        axes = (("pull_records", (0, 1, 2)), ("pull_rows", (1, 2)), ("push_sparse_ratio", (-1, 4, 16, 64)),
+                ("pull_warp", (1, 2, 3)),
+                ("push_defer_edges", DEFER), ("ctas_per_sm", CTAS), ("giant_edges", GIANT),
                 ("pull_gather_ratio", GATHER), ("alpha", ALPHAS), ("beta", BETAS))
     for name, values in axes:
         for v in values:

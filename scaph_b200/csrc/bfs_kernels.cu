@@ -313,22 +313,9 @@ __device__ __forceinline__ void push_body(const GraphDev &g, const BfsDev &s, ui
                                  : (((uint32_t)(((unsigned long long)vhi + 31) >> 5)) - (vlo >> 5) + kPushTileWords - 1) /
                                        kPushTileWords;
 
-    for (uint32_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-        uint32_t rlo = vlo, rhi = vhi, local;
-        range_of_tile(rl, tile, rlo, rhi, local);
-        const uint32_t rwhi = (uint32_t)(((unsigned long long)rhi + 31) >> 5);
-        const uint32_t w = (rlo >> 5) + local * kPushTileWords + threadIdx.x;
-        uint32_t f = 0;
-        if (threadIdx.x < kPushTileWords && w < rwhi) f = s.front[w] & range_mask(w, rlo, rhi);
-        if (!__syncthreads_or(f != 0)) continue;
-        uint32_t total;
-        uint32_t off = block_exclusive_scan<BLOCK>(__popc(f), wsum, total);
-        if (total == 0) continue;
-        while (f) {
-            q[off++] = (w << 5) + (__ffs(f) - 1);
-            f &= f - 1;
-        }
-        __syncthreads();
+    // expands the frontier vertices q[0, total), BLOCK at a time (every
+    // thread of the CTA calls it)
+    auto run_queue = [&](uint32_t total) {
         for (uint32_t c0 = 0; c0 < total; c0 += BLOCK) {
             const uint32_t k = c0 + threadIdx.x;
             uint32_t nq = 0;
@@ -391,6 +378,64 @@ __device__ __forceinline__ void push_body(const GraphDev &g, const BfsDev &s, ui
                 visit4(sm, s, t, vals, in, src, hist_same, lut);
             }
             __syncthreads();
+        }
+    };
+
+    if (s.push_sparse && rl.n == 0) {
+        // ---- sparse level: the CTA owns one contiguous run of frontier
+        // words and reads it BLOCK*4 words per round (each thread four
+        // coalesced words), so that its few frontier vertices are found with
+        // one round trip and expanded together, not one tile after another
+        const uint32_t wlo = vlo >> 5, whi = (uint32_t)(((unsigned long long)vhi + 31) >> 5);
+        const uint32_t per = (whi - wlo + gridDim.x - 1) / gridDim.x;
+        const uint32_t w0 = wlo + blockIdx.x * per, w1 = min(whi, w0 + per);
+        constexpr uint32_t kCap = kPushTileWords * 32;  // q's capacity
+        for (uint32_t cw = w0; cw < w1; cw += 4 * BLOCK) {
+            uint32_t f[4], n = 0;
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+                const uint32_t w = cw + k * BLOCK + threadIdx.x;
+                f[k] = w < w1 ? s.front[w] & range_mask(w, vlo, vhi) : 0u;
+                n += __popc(f[k]);
+            }
+            if (!__syncthreads_or(n != 0)) continue;
+            uint32_t total;
+            const uint32_t off = block_exclusive_scan<BLOCK>(n, wsum, total);
+            // more vertices than q holds (a dense run): windows of kCap
+            for (uint32_t lo = 0; lo < total; lo += kCap) {
+                uint32_t at = off;
+#pragma unroll
+                for (int k = 0; k < 4; k++) {
+                    uint32_t m = f[k];
+                    const uint32_t base = (cw + k * BLOCK + threadIdx.x) << 5;
+                    while (m) {
+                        if (at >= lo && at < lo + kCap) q[at - lo] = base + (__ffs(m) - 1);
+                        at++;
+                        m &= m - 1;
+                    }
+                }
+                __syncthreads();
+                run_queue(min(kCap, total - lo));
+            }
+        }
+    } else {
+        for (uint32_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+            uint32_t rlo = vlo, rhi = vhi, local;
+            range_of_tile(rl, tile, rlo, rhi, local);
+            const uint32_t rwhi = (uint32_t)(((unsigned long long)rhi + 31) >> 5);
+            const uint32_t w = (rlo >> 5) + local * kPushTileWords + threadIdx.x;
+            uint32_t f = 0;
+            if (threadIdx.x < kPushTileWords && w < rwhi) f = s.front[w] & range_mask(w, rlo, rhi);
+            if (!__syncthreads_or(f != 0)) continue;
+            uint32_t total;
+            uint32_t off = block_exclusive_scan<BLOCK>(__popc(f), wsum, total);
+            if (total == 0) continue;
+            while (f) {
+                q[off++] = (w << 5) + (__ffs(f) - 1);
+                f &= f - 1;
+            }
+            __syncthreads();
+            run_queue(total);
         }
     }
     level_epilogue<BLOCK>(sm, s, t);
@@ -514,6 +559,20 @@ __device__ __forceinline__ void pull_body(const GraphDev &g, const BfsDev &s, ui
             t.headers++;
             return true;
         };
+        // the same with the in-list's length read from the header
+        auto list_start_len = [&](uint32_t v, int &p, unsigned long long &st, uint32_t &len) -> bool {
+            p = lut.of(v);
+            const PageDev pd = lut.pages[p];
+            if (pd.base == kNotResident) {
+                atomicOr(&s.ctr->error, 4u);
+                return false;
+            }
+            const uint32_t *node = g.pool + pd.base + 3ull * (v - pd.left);
+            st = pd.base + 3ull * pd.nodenum + node[1];
+            len = node[2];
+            t.headers++;
+            return true;
+        };
         for (uint32_t c0 = 0; c0 < total; c0 += kPPT * BLOCK) {
             uint32_t vv[kPPT], len[kPPT], need[kPPT], dg[kPPT];
             unsigned long long st[kPPT];
@@ -582,6 +641,38 @@ __device__ __forceinline__ void pull_body(const GraphDev &g, const BfsDev &s, ui
                     } else {
                         t.inspected += min(len[i], kPullSerial);
                         need[i] = len[i] > kPullSerial && list_start(vv[i], p[i], st[i]);
+                    }
+                }
+            } else if (s.prow) {
+                // ---- phase A from the 16-byte rows: one load per vertex
+                // brings the three top-ranked in-neighbours and the degrees;
+                // the top one is probed first, the other two on a miss.  An
+                // in-degree of three or less is then decided; the rest read
+                // their whole in-list in phase B (its length from the header)
+                uint4 r[kPPT];
+#pragma unroll
+                for (int i = 0; i < kPPT; i++)
+                    r[i] = ok[i] ? ld_nc_v4(reinterpret_cast<const uint32_t *>(s.prow + vv[i])) : make_uint4(0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu, 0u);
+#pragma unroll
+                for (int i = 0; i < kPPT; i++) {
+                    if (!ok[i]) continue;
+                    const uint32_t nin = r[i].w >> 28;
+                    dg[i] = r[i].w & kPrecDegMax;
+                    uint32_t hit = 0;
+                    if (r[i].x < s.V && test_bit(s.front, r[i].x)) {
+                        hit = 1u;
+                    } else {
+                        if (r[i].y < s.V && test_bit(s.front, r[i].y)) hit |= 2u;
+                        if (r[i].z < s.V && test_bit(s.front, r[i].z)) hit |= 4u;
+                    }
+                    if (hit) {
+                        const uint32_t j = __ffs(hit) - 1;
+                        t.inspected += j + 1;
+                        if (dg[i] == kPrecDegMax) dg[i] = __ldg(&s.degree[vv[i]]);
+                        found(vv[i], j == 0 ? r[i].x : j == 1 ? r[i].y : r[i].z, dg[i], -1);
+                    } else {
+                        t.inspected += min(nin, 3u);
+                        need[i] = nin > 3 && list_start_len(vv[i], p[i], st[i], len[i]);
                     }
                 }
             } else {
@@ -1156,6 +1247,7 @@ __device__ __forceinline__ BfsDev level_state(const BfsGraphArgs &a)
     s.ctr = a.ctr0 + L;
     s.pull_gather = c->pull_gather;
     s.push_defer = c->push_defer;
+    s.push_sparse = c->push_sparse;
     if (!c->pull_rec) s.prec = nullptr;
     if (a.hist0 && L < a.hist_levels) {
         s.page_nodes = a.hist0 + (size_t)L * 2 * a.npages_h;
@@ -1265,6 +1357,7 @@ __global__ void k_graph_init(BfsGraphArgs a, uint32_t *depth, uint32_t *parent, 
         c->pull_gather = 0;
         c->push_defer = 0;
         c->pull_rec = 0;
+        c->push_sparse = b.push_sparse;  // level 0: one frontier vertex
         c->t_start = globaltimer();
     }
     const size_t stride = (size_t)gridDim.x * blockDim.x;
@@ -1340,6 +1433,7 @@ __global__ void k_decide(BfsGraphArgs a, DecideArgs d, cudaGraphConditionalHandl
     else nd = alpha_beta_next(c->dir, c->nf, c->prev_nf, c->mf, mu, d.V, d.alpha, d.beta);
     c->dir = nd;
     c->push_defer = nd == 0 && d.defer_edges && c->mf >= d.defer_edges && !c->parent ? 1u : 0u;
+    c->push_sparse = nd == 0 && push_use_sparse(d.push_sparse_ratio, c->nf, d.V) ? 1u : 0u;
     {
         const uint32_t src = c->src;
         const unsigned long long src_dead = (d.dead_bm[src >> 5] >> (src & 31)) & 1u;
@@ -1355,6 +1449,8 @@ __global__ void k_decide(BfsGraphArgs a, DecideArgs d, cudaGraphConditionalHandl
 // the coming level - the same 16 globals the host loop computes (scaph.h),
 // page residency 1 (graph resident), then the new frontier's share of every
 // out-page - through the network's three layers; output 0 > 0 means pull.
+// Where alpha/beta is far from its switch point its choice stands and the
+// network is not run (the host loop does the same).
 __global__ void __launch_bounds__(64) k_decide_learned(BfsGraphArgs a, DecideArgs d, MlpDev net,
                                                        cudaGraphConditionalHandle h_loop)
 {
@@ -1399,13 +1495,6 @@ __global__ void __launch_bounds__(64) k_decide_learned(BfsGraphArgs a, DecideArg
         f[14] = (float)s_ab;
         f[15] = 1.f;
     }
-    // frontier of level L+1 = vertices discovered by level L (histogram slot L)
-    const int np = net.in - kG;
-    const PageDev *pg = a.base.hg.pages;
-    for (int p = t; p < np; p += 64) {
-        const uint32_t hn = (a.hist0 && L < a.hist_levels) ? a.hist0[(size_t)L * 2 * a.npages_h + p] : 0u;
-        f[kG + p] = (float)hn / (float)max(1u, pg[p].nodenum);
-    }
     __syncthreads();
     if (s_stop) {
         if (t == 0) {
@@ -1414,6 +1503,29 @@ __global__ void __launch_bounds__(64) k_decide_learned(BfsGraphArgs a, DecideArg
         }
         return;
     }
+    auto finish = [&](int nd) {
+        c->dir = nd;
+        c->pull_gather = s_unv * d.gather_ratio < d.V ? 1u : 0u;
+        c->pull_rec = pull_use_records(d.pull_records, c->nf, s_unv) ? 1u : 0u;
+        c->push_defer = nd == 0 && d.defer_edges && c->mf >= d.defer_edges && !c->parent ? 1u : 0u;
+        c->push_sparse = nd == 0 && push_use_sparse(d.push_sparse_ratio, c->nf, d.V) ? 1u : 0u;
+        c->level = L + 1;
+        cudaGraphSetConditional(h_loop, 1);
+    };
+    if (d.mode == 1 || d.mode == 2 || s_guard >= 0) {
+        // far from the alpha/beta threshold (or a fixed direction) the rule
+        // decides, and the network is not run
+        if (t == 0) finish(d.mode == 1 ? 0 : d.mode == 2 ? 1 : s_guard);
+        return;
+    }
+    // frontier of level L+1 = vertices discovered by level L (histogram slot L)
+    const int np = net.in - kG;
+    const PageDev *pg = a.base.hg.pages;
+    for (int p = t; p < np; p += 64) {
+        const uint32_t hn = (a.hist0 && L < a.hist_levels) ? a.hist0[(size_t)L * 2 * a.npages_h + p] : 0u;
+        f[kG + p] = (float)hn / (float)max(1u, pg[p].nodenum);
+    }
+    __syncthreads();
     // weights (and GEMM operands) rounded to bf16, FP32 accumulation, as in
     // the training kernels
     auto bf = [](float x) { return __bfloat162float(__float2bfloat16_rn(x)); };
@@ -1429,13 +1541,7 @@ __global__ void __launch_bounds__(64) k_decide_learned(BfsGraphArgs a, DecideArg
     if (t == 0) {
         float y = net.w[net.off_b3];
         for (int j = 0; j < 64; j++) y += bf(h2[j]) * bf(W3[(size_t)j * net.out]);
-        const int nd = d.mode == 1 ? 0 : d.mode == 2 ? 1 : s_guard >= 0 ? s_guard : (y > 0.f ? 1 : 0);
-        c->dir = nd;
-        c->pull_gather = s_unv * d.gather_ratio < d.V ? 1u : 0u;
-        c->pull_rec = pull_use_records(d.pull_records, c->nf, s_unv) ? 1u : 0u;
-        c->push_defer = nd == 0 && d.defer_edges && c->mf >= d.defer_edges && !c->parent ? 1u : 0u;
-        c->level = L + 1;
-        cudaGraphSetConditional(h_loop, 1);
+        finish(y > 0.f ? 1 : 0);
     }
 }
 

@@ -85,6 +85,11 @@ struct BfsDev {
     // A reads the in-degree and head row directly): x = the top-ranked
     // in-neighbour (head row entry 0), y = pull_meta(in-degree, out-degree)
     const uint2 *prec;
+    // pull: one 16-byte row per vertex read by phase A on levels without the
+    // 8-byte records (null: the in-degree, head row and out-degree arrays):
+    // x, y, z = the three top-ranked in-neighbours (0xFFFFFFFF past the
+    // in-degree), w = pull_meta(in-degree, out-degree)
+    const uint4 *prow;
     // histogram of the discovered vertices over the IN-edge graph's pages
     // (count, sum(indeg+3)): keeps the pull-side page counts current without
     // a pass over all vertices (directed graphs; null when not wanted)
@@ -98,6 +103,11 @@ struct BfsDev {
     // and k_push_finalize then writes depths and counters word by word
     uint32_t push_defer;
     uint32_t pull_warp;        // pull: 1 warp-centric chunks, 2 vertex-parallel words (needs prec)
+    // push: 1 = sparse level: each CTA reads one contiguous run of frontier
+    // words at once and expands all its vertices together, instead of one
+    // 128-word tile after another (whole-graph ranges only)
+    uint32_t push_sparse;
+    uint32_t _pad;
 };
 
 // Default of scaph_config.push_defer_edges: push levels whose frontier has
@@ -120,6 +130,15 @@ __host__ __device__ inline uint32_t pull_meta(uint32_t indeg, uint32_t outdeg)
 // scaph_config.pull_gather_ratio overrides it).
 constexpr unsigned long long kPullGatherRatio = 64;
 
+// A push level reads its frontier words as one contiguous run per CTA when
+// the frontier has fewer than one vertex per kPushSparseRatio
+// (scaph_config.push_sparse_ratio overrides it; negative: never).
+constexpr unsigned long long kPushSparseRatio = 16;
+__host__ __device__ inline bool push_use_sparse(long long ratio, unsigned long long nf, unsigned long long V)
+{
+    return ratio > 0 && nf * (unsigned long long)ratio < V;
+}
+
 // Graph mode: state of one traversal kept on the device, so a whole BFS runs
 // as one CUDA-graph launch with the level loop in a conditional WHILE node.
 struct BfsCtl {
@@ -132,7 +151,7 @@ struct BfsCtl {
     uint32_t pull_gather;      // the level is a sparse pull (BfsDev::pull_gather)
     uint32_t push_defer;       // the level is a deferred-claim push (BfsDev::push_defer)
     uint32_t pull_rec;         // the level's pull reads the 8-byte records (BfsDev::prec)
-    uint32_t _pad2;
+    uint32_t push_sparse;      // the level is a sparse push (BfsDev::push_sparse)
     unsigned long long nf, prev_nf, mf, vis_n, vis_e;
     unsigned long long t_start;
 };
@@ -169,6 +188,7 @@ struct DecideArgs {
     uint32_t gather_ratio;          // pull levels gather tiles below 1 unvisited per this many
     unsigned long long defer_edges; // push levels with this many frontier edges defer claims (0 never)
     int32_t pull_records;           // scaph_config.pull_records
+    int32_t push_sparse_ratio;      // push levels below 1 frontier vertex per this many are sparse (<= 0 never)
 };
 
 // Whether a pull level reads the 8-byte records (scaph_config.pull_records):

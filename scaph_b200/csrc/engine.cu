@@ -127,9 +127,34 @@ BfsDev scaph_engine::base_state(uint32_t *dd, uint32_t *dp) const
     s.indeg = d_indeg;
     s.head_ranked = head_ranked ? 1u : 0u;
     s.prec = d_prec;
+    s.prow = cfg.pull_rows == 1 && head_ranked ? d_prow : nullptr;  // phase B rescans ranked rows from 0
+    s.push_sparse = push_use_sparse(cfg.push_sparse_ratio, 1, V) ? 1u : 0u;  // level 0
     s.giant_edges = (uint32_t)cfg.giant_edges;
     s.pull_warp = cfg.pull_warp == 3 ? 0u : (uint32_t)cfg.pull_warp;  // kernel: 0 tiles, 1 warp, 2 lanes
     return s;
+}
+
+// The 16-byte pull rows (scaph_config.pull_rows = 1): the first three ranked
+// in-neighbours of the head row and the records' degree word, one load per
+// vertex instead of the in-degree, the head row and the out-degree.  Built
+// on the device from those two arrays when first asked for.
+static __global__ void k_build_prow(const uint32_t *head, const uint2 *prec, uint4 *prow, uint32_t V)
+{
+    static_assert(kPullHead == 4, "the rows keep three of the four head entries");
+    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < V; v += gridDim.x * blockDim.x) {
+        const uint4 h = reinterpret_cast<const uint4 *>(head)[v];
+        prow[v] = make_uint4(h.x, h.y, h.z, prec[v].y);
+    }
+}
+
+int scaph_engine::build_prow()
+{
+    if (d_prow || !d_head || !d_prec) return SCAPH_OK;
+    SCAPH_CUDA(cudaMalloc(&d_prow, (size_t)V * sizeof(uint4)));
+    k_build_prow<<<num_sms * 8, 256, 0, st>>>(d_head, d_prec, d_prow, V);
+    SCAPH_CUDA(cudaGetLastError());
+    SCAPH_CUDA(cudaStreamSynchronize(st));
+    return SCAPH_OK;
 }
 
 int scaph_engine::create(const Graph *g_, const Graph *gt_, const scaph_config *c)
@@ -155,6 +180,8 @@ int scaph_engine::create(const Graph *g_, const Graph *gt_, const scaph_config *
     if (cfg.push_defer_edges == 0) cfg.push_defer_edges = kDeferEdgesDefault;
     if (cfg.pull_records < 0 || cfg.pull_records > 2) cfg.pull_records = 0;
     if (cfg.pull_warp < 1 || cfg.pull_warp > 3) cfg.pull_warp = 1;
+    if (cfg.pull_rows < 0 || cfg.pull_rows > 2) cfg.pull_rows = 0;
+    if (cfg.push_sparse_ratio == 0) cfg.push_sparse_ratio = (int32_t)kPushSparseRatio;
     device = cfg.device;
     if (g->weighted) return set_error(SCAPH_EUNSUPPORTED, "BFS engine needs unweighted pages");
     if (gt && (gt->V != V || gt->E != E || gt->weighted))
@@ -208,6 +235,7 @@ int scaph_engine::create(const Graph *g_, const Graph *gt_, const scaph_config *
             prec[v] = make_uint2(head[(size_t)v * kPullHead], pull_meta(indeg[v], g->degree[v]));
         SCAPH_CUDA(cudaMalloc(&d_prec, (size_t)V * sizeof(uint2)));
         SCAPH_CUDA(cudaMemcpy(d_prec, prec.data(), (size_t)V * sizeof(uint2), cudaMemcpyHostToDevice));
+        if (cfg.pull_rows == 1 && (rc = build_prow())) return rc;
     }
 
     // vertices no edge reaches (in-degree 0) are never discovered: they start
@@ -278,6 +306,7 @@ void scaph_engine::destroy()
     cudaFree(d_indeg);
     cudaFree(d_head);
     cudaFree(d_prec);
+    cudaFree(d_prow);
     cudaFree(d_snap);
     cudaFree(d_pcnt);
     cudaFree(d_pdatas);
@@ -404,7 +433,18 @@ int scaph_engine::run_host_loop(uint32_t src, uint32_t *dd, uint32_t *dp)
 {
     const int fill_grid = num_sms * 4;
     const size_t np = g->pages.size();
-    const bool learned = cfg.direction == SCAPH_DIR_LEARNED && sched;
+    // The pool holds the in-edge pages with half the out-edge pages beside
+    // them: what a level brings in stays for later levels and traversals.
+    const bool keep_pool = pager && !symmetric && 2 * gin().npages + np <= 2 * (size_t)pager_nslots(pager);
+    // The network's direction output models the resident level kernels'
+    // time (its labels come from timing both directions on a resident
+    // graph); the paged kernels cost differently (config 3, pool kept, warm:
+    // same bytes moved, its directions 0.81x of alpha/beta).  Out of core it
+    // names pages to prefetch, and only where pages do not stay in the pool
+    // (in one that keeps them, demand paging already reads a single
+    // traversal's sparse pages zero-copy and keeps the dense ones): a pool
+    // that keeps pages runs the plain loop.
+    const bool learned = cfg.direction == SCAPH_DIR_LEARNED && sched && !keep_pool;
     const bool want_feat = learned || cfg.record_features;
     const bool dual = cfg.dual_timing && !pager;
     // per-level page histograms (get_page_info's counts) cost a shared-memory
@@ -461,9 +501,6 @@ int scaph_engine::run_host_loop(uint32_t src, uint32_t *dd, uint32_t *dp)
     }
     // page counts of the last feature pass, reused by the pager
     std::vector<uint32_t> feat_pc, feat_hist;
-    // The pool holds the in-edge pages with half the out-edge pages beside
-    // them: what a level brings in stays for later levels and traversals.
-    const bool keep_pool = pager && !symmetric && 2 * npi + np <= 2 * (size_t)pager_nslots(pager);
     while (nf > 0 && level < kMaxLevels && (uint64_t)level + 1 < unreached) {
         const uint64_t used = vis_e + dead_edges;
         const uint64_t mu = E > used ? E - used : 0;
@@ -486,58 +523,27 @@ int scaph_engine::run_host_loop(uint32_t src, uint32_t *dd, uint32_t *dp)
                 mlp_dims(sched, &in, &out);
                 y.resize(out);
                 mlp_forward_host(sched_host, f.data(), y.data());
-                if (level > 0) {
-                    // the network models kernel time (trained on resident
-                    // rows, residency features 1): out of core its direction
-                    // comes from the same row with the residency features at
-                    // 1 (the traffic rule below prices the pages); fed the
-                    // real residency it strayed out of its training inputs
-                    // (config 3 warm: same bytes moved, 0.81x of alpha/beta)
-                    float ydir = y[0];
-                    if (pager) {
-                        std::vector<float> fr(f);
-                        fr[10] = fr[11] = fr[12] = fr[13] = 1.f;
-                        std::vector<float> yr(y.size());
-                        mlp_forward_host(sched_host, fr.data(), yr.data());
-                        ydir = yr[0];
-                    }
-                    dir = ydir > 0.f ? 1 : 0;
+                if (level > 0 && !pager) {
+                    dir = y[0] > 0.f ? 1 : 0;
                     // far from the alpha/beta threshold the rule decides
                     const int sure = alpha_beta_confident(prev_dir, nf, mf, mu, V, cfg.alpha, cfg.beta);
                     if (sure >= 0) dir = sure;
-                    if (pager) {
-                        // out of core the page traffic each direction would
-                        // cause is known exactly.  In a pool that keeps what
-                        // levels bring in (keep_pool), its contents follow
-                        // the directions taken: there, where either direction
-                        // would move pages, the rule decides (a level-local
-                        // choice by traffic leaves the pool worse for the
-                        // traversals after it).  In a smaller pool pages do
-                        // not stay, and a direction whose traffic is more
-                        // than twice the other's (and 1 ms more) is turned
-                        // around.
-                        const int npc = (int)pc.size() / 2;
-                        const double t_push = pager_transfer_ms(pager, 0, hist.data(), hist.data() + np, (int)np,
-                                                                cfg.compact_threshold);
-                        const double t_pull = pager_transfer_ms(pager, symmetric ? 0 : 1, pc.data(), pc.data() + npc,
-                                                                npc, cfg.compact_threshold);
-                        if (keep_pool) {
-                            if (t_push > 0 || t_pull > 0) dir = ab;
-                        } else if (t_push > 2 * t_pull + 1.0) {
-                            dir = 1;
-                        } else if (t_pull > 2 * t_push + 1.0) {
-                            dir = 0;
-                        }
-                    }
+                } else if (level > 0) {
+                    // out of core (a pool that does not keep pages): the page
+                    // traffic each direction would cause is known exactly; a
+                    // direction whose traffic is more than twice the other's
+                    // (and 1 ms more) is turned around
+                    const int npc = (int)pc.size() / 2;
+                    const double t_push = pager_transfer_ms(pager, 0, hist.data(), hist.data() + np, (int)np,
+                                                            cfg.compact_threshold);
+                    const double t_pull = pager_transfer_ms(pager, symmetric ? 0 : 1, pc.data(), pc.data() + npc,
+                                                            npc, cfg.compact_threshold);
+                    if (t_push > 2 * t_pull + 1.0) dir = 1;
+                    else if (t_pull > 2 * t_push + 1.0) dir = 0;
                 }
                 // prefetch only pages the network is confident about (into
-                // free slots; never at the expense of resident pages), and
-                // only in a pool that does not keep what levels bring in: in
-                // one that does, demand paging reads the sparse pages of a
-                // single traversal zero-copy and keeps the dense ones, and a
-                // prefetch copies sparse pages whole (measured on config 3
-                // warm: 2.45 GB moved against alpha/beta's 1.10 GB, 0.89x)
-                if (!keep_pool)
+                // free slots; never at the expense of resident pages)
+                if (pager)
                     for (int p = 0; p + 1 < out && p < (int)np; p++)
                         if (y[1 + p] > 2.f) prefetch_pages.push_back(p);
             }
@@ -564,6 +570,7 @@ int scaph_engine::run_host_loop(uint32_t src, uint32_t *dd, uint32_t *dp)
         // deferred claims on big push levels (resident graphs, no parents)
         s.push_defer = !pager && !dp && !dual && cfg.push_defer_edges > 0 && mf >= (uint64_t)cfg.push_defer_edges
                            ? 1u : 0u;
+        s.push_sparse = push_use_sparse(cfg.push_sparse_ratio, nf, V) ? 1u : 0u;
         s.page_nodes_in = s.page_datas_in = nullptr;
         if (incr && d_hist_in && level < kHistLevels) {
             s.page_nodes_in = d_hist_in + (size_t)level * 2 * npi;
@@ -694,6 +701,7 @@ int scaph_engine::build_graph()
     dargs.gather_ratio = (uint32_t)cfg.pull_gather_ratio;
     dargs.defer_edges = cfg.push_defer_edges > 0 ? (unsigned long long)cfg.push_defer_edges : 0ull;
     dargs.pull_records = cfg.pull_records;
+    dargs.push_sparse_ratio = cfg.push_sparse_ratio;
 
     // init (run inputs are this node's arguments, replaced per launch)
     uint32_t *depth0 = d_depth, *parent0 = nullptr, src0 = 0, unr = unreached, nclear = kMaxLevels;
@@ -1061,6 +1069,12 @@ int scaph_engine_tune(scaph_engine *e, const scaph_config *c)
     k.push_defer_edges = c->push_defer_edges == 0 ? kDeferEdgesDefault : c->push_defer_edges;
     k.pull_warp = c->pull_warp >= 1 && c->pull_warp <= 3 ? c->pull_warp : 1;
     k.pull_records = c->pull_records >= 0 && c->pull_records <= 2 ? c->pull_records : 0;
+    k.pull_rows = c->pull_rows >= 0 && c->pull_rows <= 2 ? c->pull_rows : 0;
+    if (k.pull_rows == 1) {
+        const int rc = e->build_prow();
+        if (rc) return rc;
+    }
+    k.push_sparse_ratio = c->push_sparse_ratio == 0 ? (int32_t)kPushSparseRatio : c->push_sparse_ratio;
     e->block = c->block_size ? c->block_size : 256;
     const int occ_push = std::max(1, level_occupancy(0, e->block)), occ_pull = std::max(1, level_occupancy(1, e->block));
     e->grid_push = k.ctas_per_sm > 0 ? k.ctas_per_sm * e->num_sms : occ_push * e->num_sms;

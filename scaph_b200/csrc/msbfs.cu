@@ -274,12 +274,13 @@ static int ms_run(scaph_engine *e, const uint32_t *srcs, int nsrc, uint32_t *out
     // The learned scheduler (SCAPH_DIR_LEARNED with a network set): before
     // every level the same feature row as the single-source loop (16 globals,
     // then the frontier's share of every out-page, counted over the union of
-    // the batch's frontiers) goes through the network; it picks the direction
-    // near the alpha/beta switch point and names the out-pages that will hold
-    // frontier vertices next level, which are prefetched into free pool
-    // slots while the level runs.  Out of core the exact page traffic of
-    // either direction overrides it where one side clearly dominates.  The
-    // rows are kept (scaph_bfs_features) with record_features.
+    // the batch's frontiers) goes through the network.  Out of core its
+    // direction logit marks the push levels that lead into the pull levels,
+    // during which the in-pages the first pull level reads are prefetched
+    // into free pool slots.  Without a network, the exact page traffic of
+    // either direction overrides alpha/beta where one side clearly
+    // dominates.  The rows are kept (scaph_bfs_features) with
+    // record_features.
     const bool learned = e->cfg.direction == SCAPH_DIR_LEARNED;
     const bool net_on = learned && e->sched;
     const bool want_feat = net_on || e->cfg.record_features;
@@ -336,40 +337,50 @@ static int ms_run(scaph_engine *e, const uint32_t *srcs, int nsrc, uint32_t *out
         if (net_on) {
             // the network's direction output is trained on single-source
             // level costs, which a batch's levels do not share (a pull level
-            // serves every source at once): the batch keeps alpha/beta and
-            // the traffic rule for direction, and takes the page outputs
+            // serves every source at once): the batch keeps alpha/beta for
+            // direction and reads the logit as a sign that pull is near
             mlp_forward_host(e->sched_host, f.data(), y.data());
         }
         if (e->pager && learned && !net_on && level > 0) {
             // the exact page traffic each direction would cause overrides
             // the kernel-time choice when one side clearly dominates (not
-            // with the network's prefetch: prefetched out-pages make every
-            // push look free of traffic, and the batch then pushes levels
-            // that pull serves faster - measured on config 5: 8 push levels,
-            // 0.77x of alpha/beta cold)
+            // with the network's prefetch: prefetched pages make a direction
+            // look free of traffic - measured on config 5 with out-page
+            // prefetch: 8 push levels, 0.77x of alpha/beta cold)
             double tp = 0, tq = 0;
             ms_transfer_ms(e, lp, tp, tq);
             if (tp > 2 * tq + 1.0) dir = 1;
             else if (tq > 2 * tp + 1.0) dir = 0;
         }
         if (net_on && e->pager && dir == 0) {
-            // during a push level: the out-pages the network expects to hold
-            // frontier vertices next level that this level does not read
-            // itself (a batch's union frontier makes a page it enters dense,
-            // so such a page is copied whole anyway) - but only into the
-            // free slots beyond those the missing in-pages will need for the
-            // pull levels: a prefetched page evicted before its use is read
-            // twice (config 5 cold with no reserve: 27.6 GB moved against
-            // alpha/beta's 16.1 GB, 0.65x)
-            const int gin = e->symmetric ? 0 : 1;
-            const double miss_in =
-                gin ? (1.0 - pager_resident_fraction(e->pager, gin, nullptr)) * (double)e->gt->pages.size() : 0.0;
-            long long room = (long long)pager_free_slots(e->pager) - (long long)std::ceil(miss_in);
-            for (int p = 0; p + 1 < (int)y.size() && p < (int)np && room > 0; p++)
-                if (y[1 + p] > 2.f && lp.push_cnt[p] == 0 && !pager_is_resident(e->pager, 0, p)) {
+            // during a push level that leads into the pull levels: the
+            // in-pages holding incomplete vertices (every one of them is
+            // read whole by the first pull level) are copied into free
+            // slots while this level runs, so that the link is busy during
+            // the push levels.  The pull is expected next when the network
+            // rates this level pull-worthy (its direction logit, trained on
+            // single-source levels) or when alpha/beta, run on the frontier
+            // grown at its last rate, would switch.  Out-pages the network
+            // names are not prefetched: a batch's push levels read their
+            // sparse out-pages zero-copy, so whole-page copies of them went
+            // unused (config 5 cold: 189 pages, 7.9 GB moved for nothing,
+            // 0.74x of alpha/beta)
+            const double grow = prev_nf ? (double)nf / (double)prev_nf : 1.0;
+            const double mf_next = (double)mf * std::max(1.0, grow);
+            const double mu_next = std::max(0.0, (double)mu - mf_next);
+            const bool pull_soon = y[0] > 0.f || mf_next * alpha > mu_next;
+            if (pull_soon) {
+                const int gin = e->symmetric ? 0 : 1;
+                long long room = (long long)pager_free_slots(e->pager);
+                for (int p : lp.push_need)
+                    if (!pager_is_resident(e->pager, 0, p)) room--;
+                for (int p : lp.pull_need) {
+                    if (room <= 0) break;
+                    if (pager_is_resident(e->pager, gin, p)) continue;
                     prefetch_pages.push_back(p);
                     room--;
                 }
+            }
         }
         const uint32_t d = (uint32_t)level + 1;
         for (int k = 0; k < kMsPlanes; k++) {
@@ -418,8 +429,8 @@ static int ms_run(scaph_engine *e, const uint32_t *srcs, int nsrc, uint32_t *out
             if (dir == 0) npush++; else npull++;
             if (!prefetch_pages.empty()) {
                 // copies into free slots on the copy streams, behind this
-                // level's kernels in the queue of the link
-                if ((rc = pager_prefetch(e, e->pager, 0, prefetch_pages))) return rc;
+                // level's own copies in the queue of the link
+                if ((rc = pager_prefetch(e, e->pager, e->symmetric ? 0 : 1, prefetch_pages))) return rc;
                 npref += prefetch_pages.size();
             }
         } else if (dir == 0) {

@@ -27,7 +27,11 @@ def rmat15():
                                 dict(pull_records=1), dict(pull_records=2), dict(pull_records=1, pull_warp=1),
                                 dict(pull_warp=2, pull_records=1), dict(pull_warp=2, pull_records=1, alpha=0.01, beta=0.001),
                                 dict(pull_warp=2, pull_records=1, block_size=512), dict(pull_warp=3, pull_records=1),
-                                dict(push_defer_edges=-1)])
+                                dict(push_defer_edges=-1), dict(pull_rows=2), dict(pull_rows=1, pull_records=2),
+                                dict(pull_rows=1, pull_records=2, alpha=0.01, beta=0.001),
+                                dict(pull_rows=1, pull_records=2, pull_gather_ratio=1), dict(push_sparse_ratio=-1),
+                                dict(push_sparse_ratio=1, alpha=1000.0), dict(push_sparse_ratio=1, alpha=1000.0, block_size=128),
+                                dict(push_sparse_ratio=1, alpha=1000.0, block_size=512, push_defer_edges=1)])
 def test_tunables_keep_depths(rmat15, kw):
     """push_defer_edges=1 defers the claims of every push level (neighbours
     OR-ed into the next frontier, depths written by the finalize pass);

@@ -55,6 +55,28 @@ def test_rmat21_many_pages(rmat21, use_graph):
     eng.close()
 
 
+@pytest.mark.parametrize("use_graph", [0, 2], ids=["graph", "hostloop"])
+def test_rmat21_sparse_push_windows(rmat21, use_graph):
+    """Every level pushes through the sparse front-end (push_sparse_ratio 1)
+    with one CTA per SM: a CTA's run of frontier words (443 words, up to
+    14 K vertices) then holds more frontier vertices than its 4096-entry
+    queue at the big levels, so the queue is filled and expanded in
+    windows.  Depths bit-exact, parents a valid BFS tree, with and without
+    deferred claims."""
+    csr, g = rmat21
+    for defer in (-1, 1):
+        eng = S.Engine(g, use_graph=use_graph, alpha=1000.0, ctas_per_sm=1, push_sparse_ratio=1,
+                       push_defer_edges=defer)
+        for src in G.sources(csr, 2, 68) + [int(np.argmax(csr.degree()))]:
+            depth, parent, st = eng.bfs(src, parents=defer < 0)
+            _same(csr, src, depth)
+            assert st.pull_levels == 0
+            if defer < 0:
+                rc, bad = O.validate_tree(csr.idx, csr.ngh, src, depth, parent)
+                assert rc == 0, f"invalid BFS tree (code {rc} at {bad})"
+        eng.close()
+
+
 def test_rmat21_msbfs_64(rmat21):
     csr, g = rmat21
     eng = S.Engine(g)

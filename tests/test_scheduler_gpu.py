@@ -80,7 +80,8 @@ def test_learned_graph_mode_in_hbm_is_exact_and_matches_host_loop(setup):
 def test_learned_multi_source_out_of_core(setup):
     """The network inside the multi-source loop, out of core: the feature
     rows it sees (one per level, the union of the batch's frontiers), the
-    pages it names prefetched into free slots, and depths still bit-exact."""
+    in-pages prefetched ahead of the pull levels, and depths still
+    bit-exact."""
     csr, g, gt, train, held = setup
     total = g.npages + gt.npages
     pool = int(0.6 * total) * g.pagesize * 4
@@ -101,16 +102,16 @@ def test_learned_multi_source_out_of_core(setup):
 
 
 def test_multi_source_prefetch_keeps_depths(setup):
-    """A network whose page outputs are all confident: every page not in the
-    current frontier is prefetched into free slots each level; the rows stay
-    exact and the prefetch count is reported."""
+    """A network whose direction logit rates every level pull-worthy: each
+    push level prefetches the missing in-pages that hold
+    incomplete vertices into free slots; the rows stay exact and equal to
+    the engine's without a network, and the prefetch count is reported."""
     csr, g, gt, _, held = setup
     net = S.Mlp(scheduler.G + g.npages, 1 + g.npages, seed=5)
     p = net.params()
     n3 = 64 * (1 + g.npages)
     p[-(1 + g.npages) - n3:-(1 + g.npages)] = 0.0  # W3 = 0
     p[-(1 + g.npages):] = 5.0                      # b3: every logit 5
-    p[-(1 + g.npages)] = 0.0                       # direction logit 0
     net.set_params(p)
     total = g.npages + gt.npages
     eng = S.Engine(g, gt, pool_bytes=int(0.8 * total) * g.pagesize * 4, direction=S.DIR_LEARNED)
@@ -118,6 +119,13 @@ def test_multi_source_prefetch_keeps_depths(setup):
     eng.evict_all()
     depth, st = eng.msbfs(held)
     assert st.prefetched > 0
+    assert st.pull_levels > 0
     for i, s in enumerate(held):
         assert np.array_equal(depth[i], O.bfs(csr.idx, csr.ngh, s)), f"row {i}"
+    # the same batch without a network gives the same rows
+    plain = S.Engine(g, gt, pool_bytes=int(0.8 * total) * g.pagesize * 4)
+    plain.evict_all()
+    depth_p, _ = plain.msbfs(held)
+    assert np.array_equal(depth, depth_p)
+    plain.close()
     eng.close()
