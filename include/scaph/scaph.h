@@ -268,7 +268,11 @@ typedef struct scaph_config {
                                   frontier words as one contiguous run per
                                   CTA and expands them together (whole-
                                   graph ranges); 0 = 16, negative = never  */
-    int32_t  _reserved2;
+    int32_t  pull_runs;        /* sparse pull levels (pull_gather_ratio) on
+                                  whole-graph ranges: 0 or 1 = each CTA
+                                  reads one contiguous run of visited words
+                                  at once, 2 = 128-word tiles one after
+                                  another                                   */
 } scaph_config;
 
 typedef struct scaph_engine scaph_engine;
@@ -319,8 +323,8 @@ int scaph_bfs(scaph_engine *e, uint32_t src, uint32_t *depths, uint32_t *parents
 /* Sets an engine's run-time tunables from cfg: alpha, beta, block_size,
  * ctas_per_sm, giant_edges, pull_gather_ratio, ms_compact_l2_div,
  * ms_compact_min_deg, pull_warp, push_defer_edges, pull_records,
- * pull_rows and push_sparse_ratio (0 = default; the other fields are
- * ignored).  They
+ * pull_rows, push_sparse_ratio and pull_runs (0 = default; the other
+ * fields are ignored).  They
  * change the schedule only, never the depths.  Waits for the engine's work
  * and drops its CUDA graph (the next run rebuilds it).  Replaces setting
  * FLAGS_num_blks / FLAGS_num_thds between runs (src/app.cuh:38-52). */

@@ -55,7 +55,7 @@ class _Config(C.Structure):
                 ("link_gbs", C.c_float), ("giant_edges", C.c_int32), ("pull_gather_ratio", C.c_int32),
                 ("ms_compact_l2_div", C.c_int32), ("ms_compact_min_deg", C.c_int32), ("pull_warp", C.c_int32),
                 ("push_defer_edges", C.c_int64), ("pull_records", C.c_int32), ("pull_rows", C.c_int32),
-                ("push_sparse_ratio", C.c_int32), ("_reserved2", C.c_int32)]
+                ("push_sparse_ratio", C.c_int32), ("pull_runs", C.c_int32)]
 
 
 class _Stats(C.Structure):
@@ -476,12 +476,13 @@ class Engine:
                  stream: int | None = None, record_features: int = 0, dual_timing: int = 0,
                  link_gbs: float = 0.0, giant_edges: int = 0, pull_gather_ratio: int = 0,
                  ms_compact_l2_div: int = 0, ms_compact_min_deg: int = 0, push_defer_edges: int = 0,
-                 pull_warp: int = 0, pull_records: int = 0, pull_rows: int = 0, push_sparse_ratio: int = 0):
+                 pull_warp: int = 0, pull_records: int = 0, pull_rows: int = 0, push_sparse_ratio: int = 0,
+                 pull_runs: int = 0):
         self.graph, self.transposed = graph, transposed
         cfg = _Config(pool_bytes, unreached, direction, alpha, beta, block_size, ctas_per_sm, copy_streams,
                       prefetch, compact_threshold, use_graph, device, stream, record_features, dual_timing,
                       link_gbs, giant_edges, pull_gather_ratio, ms_compact_l2_div, ms_compact_min_deg, pull_warp,
-                      push_defer_edges, pull_records, pull_rows, push_sparse_ratio)
+                      push_defer_edges, pull_records, pull_rows, push_sparse_ratio, pull_runs)
         self._cfg = cfg
         h = C.c_void_p()
         _check(lib().scaph_engine_create(graph._h, transposed._h if transposed else None, C.byref(cfg), C.byref(h)))
@@ -571,7 +572,7 @@ class Engine:
 
     TUNABLES = ("alpha", "beta", "block_size", "ctas_per_sm", "giant_edges", "pull_gather_ratio",
                 "ms_compact_l2_div", "ms_compact_min_deg", "push_defer_edges", "pull_warp", "pull_records",
-                "pull_rows", "push_sparse_ratio")
+                "pull_rows", "push_sparse_ratio", "pull_runs")
 
     def tune(self, **kw) -> None:
         """Sets run-time tunables (scaph_engine_tune); others keep their value."""
@@ -583,7 +584,7 @@ class Engine:
 
     _TUNABLE_DEFAULTS = {"giant_edges": 1024, "pull_gather_ratio": 64, "ms_compact_l2_div": 3,
                          "ms_compact_min_deg": 16, "push_defer_edges": 1 << 20, "pull_warp": 1,
-                         "pull_rows": 2, "push_sparse_ratio": 16}
+                         "pull_rows": 2, "push_sparse_ratio": 16, "pull_runs": 1}
 
     def tunables(self) -> dict:
         """The tunables in force (0 fields shown as the defaults they mean)."""

@@ -193,6 +193,7 @@ def tune_engine(eng: Engine, sources, ptr: int, multi: bool = False, repeats: in
                 ("beta", BETAS))
     else:
         axes = (("pull_records", (0, 1, 2)), ("pull_rows", (1, 2)), ("push_sparse_ratio", (-1, 4, 16, 64)),
+                ("pull_runs", (1, 2)),
                 ("pull_warp", (1, 2, 3)),
                 ("push_defer_edges", DEFER), ("ctas_per_sm", CTAS), ("giant_edges", GIANT),
                 ("pull_gather_ratio", GATHER), ("alpha", ALPHAS), ("beta", BETAS))

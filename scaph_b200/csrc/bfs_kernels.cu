@@ -43,6 +43,9 @@ namespace {
 #define SCAPH_PULL_SERIAL 4
 #endif
 constexpr int kPushTileWords = 128;                  // frontier-bitmap words per push tile
+#ifndef SCAPH_PULL_DEFER_B
+#define SCAPH_PULL_DEFER_B 1  // pull phase B waits for several rounds' vertices (see pull_body)
+#endif
 #ifndef SCAPH_PULL_FIRST_PROBE
 #define SCAPH_PULL_FIRST_PROBE 1
 #endif
@@ -490,8 +493,13 @@ __device__ __forceinline__ void pull_body(const GraphDev &g, const BfsDev &s, ui
     __shared__ uint32_t q[kPullTileWords * 32];
     __shared__ uint32_t fnd[kPullTileWords];
     constexpr int kPPT = BLOCK >= 512 ? 1 : kPullPerThread;  // shared memory bounds the 512-thread CTA
-    __shared__ uint32_t bq_v[kPPT * BLOCK], bq_len[kPPT * BLOCK];
-    __shared__ unsigned long long bq_st[kPPT * BLOCK];
+    // phase-B queue: with SCAPH_PULL_DEFER_B the vertices of several rounds
+    // wait here and phase B runs once they would overflow it (or at the end
+    // of the queue), so that a CTA waits for its longest in-list once per
+    // few rounds instead of once per round
+    constexpr uint32_t kBq = (SCAPH_PULL_DEFER_B ? 3 : 2) * kPPT * BLOCK / 2;  // static shared memory: 48 KB
+    __shared__ uint32_t bq_v[kBq], bq_len[kBq];
+    __shared__ unsigned long long bq_st[kBq];
     __shared__ uint32_t wsum[BLOCK / 32];
 
     level_prologue<BLOCK>(sm, s);
@@ -573,6 +581,71 @@ __device__ __forceinline__ void pull_body(const GraphDev &g, const BfsDev &s, ui
             t.headers++;
             return true;
         };
+        // ---- phase B over bq[0, nb): groups of kGroup lanes, one vertex per group
+        auto phase_b = [&](uint32_t nb) {
+            for (uint32_t e0 = 0; e0 < nb; e0 += kGroups) {
+                const uint32_t e = e0 + grp;
+                const bool mine = e < nb;
+                unsigned long long a = 0, b = 0;
+                if (mine) {
+                    a = bq_st[e] + (s.head_ranked ? 0u : kPullSerial);
+                    b = bq_st[e] + bq_len[e];
+                }
+                const unsigned long long qa = a >> 2, qb = (b + 3) >> 2;
+                unsigned long long qd = qa + glane;
+                bool active = mine;
+                uint32_t hit_par = kNoParent;
+                unsigned long long hit_word = b;
+                while (__any_sync(0xFFFFFFFFu, active)) {
+                    uint32_t myhit = 0, vals[4] = {0, 0, 0, 0};
+                    if (active && qd < qb) {
+                        const uint4 val = ld_nc_v4(g.pool + qd * 4);
+                        vals[0] = val.x;
+                        vals[1] = val.y;
+                        vals[2] = val.z;
+                        vals[3] = val.w;
+#pragma unroll
+                        for (int j = 0; j < 4; j++) {
+                            const unsigned long long word = qd * 4 + j;
+                            if (word >= a && word < b && vals[j] < s.V && test_bit(s.front, vals[j])) myhit |= 1u << j;
+                        }
+                    }
+                    // every lane runs the same ballot/shuffles (warp stays converged)
+                    const uint32_t bal = __ballot_sync(0xFFFFFFFFu, myhit != 0);
+                    const uint32_t gb = (bal >> gshift) & ((1u << kGroup) - 1u);
+                    const int first = gb ? __ffs(gb) - 1 : 0;  // group lane holding the first hit
+                    const uint32_t fh = __shfl_sync(0xFFFFFFFFu, myhit, gshift + first);
+                    const int j = __ffs(fh | 0x10u) - 1;       // 4 when the group has no hit
+                    const uint32_t pick = j == 0 ? vals[0] : j == 1 ? vals[1] : j == 2 ? vals[2] : vals[3];
+                    const uint32_t hp = __shfl_sync(0xFFFFFFFFu, pick, gshift + first);
+                    if (active) {
+                        if (gb) {
+                            hit_par = hp;
+                            hit_word = (qd - glane + first) * 4 + j;
+                            active = false;
+                        } else {
+                            qd += kGroup;
+                            if (qd - glane >= qb) active = false;
+                        }
+                    }
+                }
+                if (mine && glane == 0) {
+                    t.inspected += (uint32_t)(hit_word - a) + (hit_par != kNoParent ? 1u : 0u);
+                    if (hit_par != kNoParent) {
+                        const uint32_t vv = bq_v[e];
+                        s.depth[vv] = s.level + 1;
+                        if (s.parent) s.parent[vv] = hit_par;
+                        mark_found(vv);
+                        const uint32_t dv = __ldg(&s.degree[vv]);
+                        t.next++;
+                        t.next_edges += dv;
+                        if (s.page_nodes) hist_add(sm, s, hist_same ? lut.of(vv) : page_of(s.hg, vv), dv + 3);
+                        hist_in_add(sm, s, vv);
+                    }
+                }
+            }
+        };
+        uint32_t nbq = 0;  // vertices waiting in bq for phase B (uniform across the CTA)
         for (uint32_t c0 = 0; c0 < total; c0 += kPPT * BLOCK) {
             uint32_t vv[kPPT], len[kPPT], need[kPPT], dg[kPPT];
             unsigned long long st[kPPT];
@@ -751,6 +824,14 @@ __device__ __forceinline__ void pull_body(const GraphDev &g, const BfsDev &s, ui
             for (int i = 0; i < kPPT; i++) nneed += need[i];
             uint32_t nb;
             uint32_t bo = block_exclusive_scan<BLOCK>(nneed, wsum, nb);
+            if (nbq + nb > kBq) {
+                // the waiting vertices first (block_exclusive_scan ended
+                // with a barrier, so their entries are visible)
+                phase_b(nbq);
+                __syncthreads();
+                nbq = 0;
+            }
+            bo += nbq;
 #pragma unroll
             for (int i = 0; i < kPPT; i++) {
                 if (!need[i]) continue;
@@ -759,73 +840,20 @@ __device__ __forceinline__ void pull_body(const GraphDev &g, const BfsDev &s, ui
                 bq_len[bo] = len[i];
                 bo++;
             }
-            __syncthreads();
-            // ---- phase B: groups of kGroup lanes, one vertex per group
-            for (uint32_t e0 = 0; e0 < nb; e0 += kGroups) {
-                const uint32_t e = e0 + grp;
-                const bool mine = e < nb;
-                unsigned long long a = 0, b = 0;
-                if (mine) {
-                    a = bq_st[e] + (s.head_ranked ? 0u : kPullSerial);
-                    b = bq_st[e] + bq_len[e];
-                }
-                const unsigned long long qa = a >> 2, qb = (b + 3) >> 2;
-                unsigned long long qd = qa + glane;
-                bool active = mine;
-                uint32_t hit_par = kNoParent;
-                unsigned long long hit_word = b;
-                while (__any_sync(0xFFFFFFFFu, active)) {
-                    uint32_t myhit = 0, vals[4] = {0, 0, 0, 0};
-                    if (active && qd < qb) {
-                        const uint4 val = ld_nc_v4(g.pool + qd * 4);
-                        vals[0] = val.x;
-                        vals[1] = val.y;
-                        vals[2] = val.z;
-                        vals[3] = val.w;
-#pragma unroll
-                        for (int j = 0; j < 4; j++) {
-                            const unsigned long long word = qd * 4 + j;
-                            if (word >= a && word < b && vals[j] < s.V && test_bit(s.front, vals[j])) myhit |= 1u << j;
-                        }
-                    }
-                    // every lane runs the same ballot/shuffles (warp stays converged)
-                    const uint32_t bal = __ballot_sync(0xFFFFFFFFu, myhit != 0);
-                    const uint32_t gb = (bal >> gshift) & ((1u << kGroup) - 1u);
-                    const int first = gb ? __ffs(gb) - 1 : 0;  // group lane holding the first hit
-                    const uint32_t fh = __shfl_sync(0xFFFFFFFFu, myhit, gshift + first);
-                    const int j = __ffs(fh | 0x10u) - 1;       // 4 when the group has no hit
-                    const uint32_t pick = j == 0 ? vals[0] : j == 1 ? vals[1] : j == 2 ? vals[2] : vals[3];
-                    const uint32_t hp = __shfl_sync(0xFFFFFFFFu, pick, gshift + first);
-                    if (active) {
-                        if (gb) {
-                            hit_par = hp;
-                            hit_word = (qd - glane + first) * 4 + j;
-                            active = false;
-                        } else {
-                            qd += kGroup;
-                            if (qd - glane >= qb) active = false;
-                        }
-                    }
-                }
-                if (mine && glane == 0) {
-                    t.inspected += (uint32_t)(hit_word - a) + (hit_par != kNoParent ? 1u : 0u);
-                    if (hit_par != kNoParent) {
-                        const uint32_t vv = bq_v[e];
-                        s.depth[vv] = s.level + 1;
-                        if (s.parent) s.parent[vv] = hit_par;
-                        mark_found(vv);
-                        const uint32_t dv = __ldg(&s.degree[vv]);
-                        t.next++;
-                        t.next_edges += dv;
-                        if (s.page_nodes) hist_add(sm, s, hist_same ? lut.of(vv) : page_of(s.hg, vv), dv + 3);
-                        hist_in_add(sm, s, vv);
-                    }
-                }
+            nbq += nb;
+            if (!SCAPH_PULL_DEFER_B) {
+                __syncthreads();
+                phase_b(nbq);
+                __syncthreads();
+                nbq = 0;
             }
+        }
+        if (nbq) {
+            __syncthreads();
+            phase_b(nbq);
             __syncthreads();
         }
     };
-
     // Warp-centric variant (s.pull_warp, 8-byte records present): every
     // warp owns chunks of 16 bitmap words (512 vertices) on its own -
     // compaction by warp scan into its 512-entry slice of q, found bits in
@@ -1140,6 +1168,59 @@ __device__ __forceinline__ void pull_body(const GraphDev &g, const BfsDev &s, ui
     // and B run, so that every thread has a vertex in each round.
     const bool gather = s.pull_gather != 0;
     uint32_t qn = 0;  // gathered vertices (uniform across the CTA)
+    if (gather && rl.n == 0 && s.pull_gather == 2) {
+        // whole-graph range: the CTA owns one contiguous run of visited
+        // words and reads it 4*BLOCK words per round (each thread four
+        // coalesced words), instead of one 128-word tile after another
+        constexpr uint32_t kCap = kPullTileWords * 32;  // q's capacity
+        const uint32_t wlo = vlo >> 5, whi = (uint32_t)(((unsigned long long)vhi + 31) >> 5);
+        const uint32_t per = (whi - wlo + gridDim.x - 1) / gridDim.x;
+        const uint32_t w0 = wlo + blockIdx.x * per, w1 = min(whi, w0 + per);
+        for (uint32_t cw = w0; cw < w1; cw += 4 * BLOCK) {
+            uint32_t u[4], n = 0;
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+                const uint32_t w = cw + k * BLOCK + threadIdx.x;
+                u[k] = w < w1 ? ~s.visited[w] & range_mask(w, vlo, vhi) : 0u;
+                n += __popc(u[k]);
+            }
+            if (!__syncthreads_or(n != 0)) continue;
+            uint32_t total;
+            const uint32_t off = block_exclusive_scan<BLOCK>(n, wsum, total);
+            if (qn + total > kCap) {
+                if (qn) run_queue(qn, 0, true);
+                qn = 0;
+            }
+            // windows of kCap when one run holds more than q (a dense run)
+            for (uint32_t lo = 0; lo < total; lo += kCap) {
+                uint32_t at = off;
+#pragma unroll
+                for (int k = 0; k < 4; k++) {
+                    uint32_t m = u[k];
+                    const uint32_t base = (cw + k * BLOCK + threadIdx.x) << 5;
+                    while (m) {
+                        if (at >= lo && at < lo + kCap) q[qn + at - lo] = base + (__ffs(m) - 1);
+                        at++;
+                        m &= m - 1;
+                    }
+                }
+                __syncthreads();
+                const uint32_t nwin = min(kCap, total - lo);
+                if (total > kCap) {
+                    run_queue(nwin, 0, true);
+                } else {
+                    qn += nwin;
+                    if (qn >= (uint32_t)kPPT * BLOCK) {
+                        run_queue(qn, 0, true);
+                        qn = 0;
+                    }
+                }
+            }
+        }
+        if (qn) run_queue(qn, 0, true);
+        level_epilogue<BLOCK>(sm, s, t);
+        return;
+    }
     for (uint32_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
         uint32_t rlo = vlo, rhi = vhi, local;
         range_of_tile(rl, tile, rlo, rhi, local);
@@ -1438,7 +1519,7 @@ __global__ void k_decide(BfsGraphArgs a, DecideArgs d, cudaGraphConditionalHandl
         const uint32_t src = c->src;
         const unsigned long long src_dead = (d.dead_bm[src >> 5] >> (src & 31)) & 1u;
         const unsigned long long unv = (unsigned long long)d.V - d.dead - c->vis_n + src_dead;
-        c->pull_gather = unv * d.gather_ratio < d.V ? 1u : 0u;
+        c->pull_gather = unv * d.gather_ratio < d.V ? d.pull_gather_mode : 0u;
         c->pull_rec = pull_use_records(d.pull_records, c->nf, unv) ? 1u : 0u;
     }
     c->level = L + 1;
@@ -1505,7 +1586,7 @@ __global__ void __launch_bounds__(64) k_decide_learned(BfsGraphArgs a, DecideArg
     }
     auto finish = [&](int nd) {
         c->dir = nd;
-        c->pull_gather = s_unv * d.gather_ratio < d.V ? 1u : 0u;
+        c->pull_gather = s_unv * d.gather_ratio < d.V ? d.pull_gather_mode : 0u;
         c->pull_rec = pull_use_records(d.pull_records, c->nf, s_unv) ? 1u : 0u;
         c->push_defer = nd == 0 && d.defer_edges && c->mf >= d.defer_edges && !c->parent ? 1u : 0u;
         c->push_sparse = nd == 0 && push_use_sparse(d.push_sparse_ratio, c->nf, d.V) ? 1u : 0u;

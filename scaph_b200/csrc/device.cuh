@@ -96,7 +96,7 @@ struct BfsDev {
     uint32_t *page_nodes_in;
     uint32_t *page_datas_in;
     GraphDev hgi;
-    uint32_t pull_gather;      // sparse pull level: gather several tiles per queue
+    uint32_t pull_gather;      // sparse pull level: 1 gather several tiles per queue, 2 one run of words per CTA
     uint32_t giant_edges;      // push: adjacency longer than this becomes chunks (0: kGiantEdges)
     // push: 1 = the level defers its claims: the neighbours' bits are OR-ed
     // into `next` (no per-edge atomic round trip, no scattered depth write)
@@ -189,6 +189,7 @@ struct DecideArgs {
     unsigned long long defer_edges; // push levels with this many frontier edges defer claims (0 never)
     int32_t pull_records;           // scaph_config.pull_records
     int32_t push_sparse_ratio;      // push levels below 1 frontier vertex per this many are sparse (<= 0 never)
+    uint32_t pull_gather_mode;      // BfsDev::pull_gather of a sparse pull level (1 tiles, 2 runs)
 };
 
 // Whether a pull level reads the 8-byte records (scaph_config.pull_records):

@@ -182,6 +182,7 @@ int scaph_engine::create(const Graph *g_, const Graph *gt_, const scaph_config *
     if (cfg.pull_warp < 1 || cfg.pull_warp > 3) cfg.pull_warp = 1;
     if (cfg.pull_rows < 0 || cfg.pull_rows > 2) cfg.pull_rows = 0;
     if (cfg.push_sparse_ratio == 0) cfg.push_sparse_ratio = (int32_t)kPushSparseRatio;
+    if (cfg.pull_runs < 0 || cfg.pull_runs > 2) cfg.pull_runs = 0;
     device = cfg.device;
     if (g->weighted) return set_error(SCAPH_EUNSUPPORTED, "BFS engine needs unweighted pages");
     if (gt && (gt->V != V || gt->E != E || gt->weighted))
@@ -564,7 +565,7 @@ int scaph_engine::run_host_loop(uint32_t src, uint32_t *dd, uint32_t *dp)
         }
         {
             const uint64_t unv_now = (uint64_t)V - n_dead - vis_n + (src_dead ? 1 : 0);
-            s.pull_gather = unv_now * (uint64_t)cfg.pull_gather_ratio < V ? 1u : 0u;
+            s.pull_gather = unv_now * (uint64_t)cfg.pull_gather_ratio < V ? (cfg.pull_runs == 2 ? 1u : 2u) : 0u;
             s.prec = pull_use_records(cfg.pull_records, nf, unv_now) ? d_prec : nullptr;
         }
         // deferred claims on big push levels (resident graphs, no parents)
@@ -702,6 +703,7 @@ int scaph_engine::build_graph()
     dargs.defer_edges = cfg.push_defer_edges > 0 ? (unsigned long long)cfg.push_defer_edges : 0ull;
     dargs.pull_records = cfg.pull_records;
     dargs.push_sparse_ratio = cfg.push_sparse_ratio;
+    dargs.pull_gather_mode = cfg.pull_runs == 2 ? 1u : 2u;
 
     // init (run inputs are this node's arguments, replaced per launch)
     uint32_t *depth0 = d_depth, *parent0 = nullptr, src0 = 0, unr = unreached, nclear = kMaxLevels;
@@ -1075,6 +1077,7 @@ int scaph_engine_tune(scaph_engine *e, const scaph_config *c)
         if (rc) return rc;
     }
     k.push_sparse_ratio = c->push_sparse_ratio == 0 ? (int32_t)kPushSparseRatio : c->push_sparse_ratio;
+    k.pull_runs = c->pull_runs >= 0 && c->pull_runs <= 2 ? c->pull_runs : 0;
     e->block = c->block_size ? c->block_size : 256;
     const int occ_push = std::max(1, level_occupancy(0, e->block)), occ_pull = std::max(1, level_occupancy(1, e->block));
     e->grid_push = k.ctas_per_sm > 0 ? k.ctas_per_sm * e->num_sms : occ_push * e->num_sms;

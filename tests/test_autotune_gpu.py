@@ -22,7 +22,7 @@ def rmat15():
 @pytest.mark.parametrize("kw", [dict(giant_edges=128), dict(giant_edges=8192), dict(pull_gather_ratio=1),
                                 dict(pull_gather_ratio=100000), dict(ctas_per_sm=1, block_size=512),
                                 dict(alpha=2.0, beta=200.0), dict(push_defer_edges=1),
-                                dict(push_defer_edges=1, giant_edges=256, alpha=1000.0), dict(pull_warp=1),
+                                dict(push_defer_edges=1, giant_edges=256, alpha=0.01), dict(pull_warp=1),
                                 dict(pull_warp=1, alpha=0.01, beta=0.001), dict(pull_warp=1, block_size=128),
                                 dict(pull_records=1), dict(pull_records=2), dict(pull_records=1, pull_warp=1),
                                 dict(pull_warp=2, pull_records=1), dict(pull_warp=2, pull_records=1, alpha=0.01, beta=0.001),
@@ -30,12 +30,16 @@ def rmat15():
                                 dict(push_defer_edges=-1), dict(pull_rows=2), dict(pull_rows=1, pull_records=2),
                                 dict(pull_rows=1, pull_records=2, alpha=0.01, beta=0.001),
                                 dict(pull_rows=1, pull_records=2, pull_gather_ratio=1), dict(push_sparse_ratio=-1),
-                                dict(push_sparse_ratio=1, alpha=1000.0), dict(push_sparse_ratio=1, alpha=1000.0, block_size=128),
-                                dict(push_sparse_ratio=1, alpha=1000.0, block_size=512, push_defer_edges=1)])
+                                dict(push_sparse_ratio=1, alpha=0.01), dict(push_sparse_ratio=1, alpha=0.01, block_size=128),
+                                dict(push_sparse_ratio=1, alpha=0.01, block_size=512, push_defer_edges=1),
+                                dict(pull_runs=2), dict(pull_runs=2, pull_gather_ratio=1),
+                                dict(pull_runs=1, pull_gather_ratio=1), dict(pull_runs=1, pull_gather_ratio=1, block_size=512),
+                                dict(pull_runs=1, pull_gather_ratio=1, pull_records=2, pull_rows=1)])
 def test_tunables_keep_depths(rmat15, kw):
     """push_defer_edges=1 defers the claims of every push level (neighbours
     OR-ed into the next frontier, depths written by the finalize pass);
-    with alpha 1000 every level pushes."""
+    with alpha 0.01 every level pushes (the switch to pull needs
+    more than 100 times the unvisited edges in the frontier)."""
     csr, g = rmat15
     for use_graph in (0, 2):
         eng = S.Engine(g, use_graph=use_graph)

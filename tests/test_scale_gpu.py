@@ -65,7 +65,7 @@ def test_rmat21_sparse_push_windows(rmat21, use_graph):
     deferred claims."""
     csr, g = rmat21
     for defer in (-1, 1):
-        eng = S.Engine(g, use_graph=use_graph, alpha=1000.0, ctas_per_sm=1, push_sparse_ratio=1,
+        eng = S.Engine(g, use_graph=use_graph, direction=S.DIR_PUSH, ctas_per_sm=1, push_sparse_ratio=1,
                        push_defer_edges=defer)
         for src in G.sources(csr, 2, 68) + [int(np.argmax(csr.degree()))]:
             depth, parent, st = eng.bfs(src, parents=defer < 0)
@@ -74,6 +74,26 @@ def test_rmat21_sparse_push_windows(rmat21, use_graph):
             if defer < 0:
                 rc, bad = O.validate_tree(csr.idx, csr.ngh, src, depth, parent)
                 assert rc == 0, f"invalid BFS tree (code {rc} at {bad})"
+        eng.close()
+
+
+@pytest.mark.parametrize("use_graph", [0, 2], ids=["graph", "hostloop"])
+def test_rmat21_pull_runs_windows(rmat21, use_graph):
+    """Every level after the first pulls, each as a sparse level read in one
+    run of visited words per CTA (pull_gather_ratio 1), with one CTA per
+    SM: a run then holds more unvisited vertices than the 4096-entry queue,
+    which is filled and drained in windows.  Depths bit-exact, parents a
+    valid BFS tree."""
+    csr, g = rmat21
+    for records in (0, 2):
+        eng = S.Engine(g, use_graph=use_graph, direction=S.DIR_PULL, ctas_per_sm=1, pull_gather_ratio=1,
+                       pull_runs=1, pull_records=records)
+        for src in G.sources(csr, 2, 69) + [int(np.argmax(csr.degree()))]:
+            depth, parent, st = eng.bfs(src, parents=True)
+            _same(csr, src, depth)
+            assert st.pull_levels == st.levels - 1
+            rc, bad = O.validate_tree(csr.idx, csr.ngh, src, depth, parent)
+            assert rc == 0, f"invalid BFS tree (code {rc} at {bad})"
         eng.close()
 
 
