@@ -444,10 +444,11 @@ __device__ __forceinline__ void push_body(const GraphDev &g, const BfsDev &s, ui
     level_epilogue<BLOCK>(sm, s, t);
 }
 
+// sm: the level's shared state, declared by the calling kernel (one copy
+// in a kernel that runs either of two bodies)
 template <int BLOCK>
-__device__ __forceinline__ void giant_body(const GraphDev &g, const BfsDev &s)
+__device__ __forceinline__ void giant_body(const GraphDev &g, const BfsDev &s, LevelSmem &sm)
 {
-    __shared__ LevelSmem sm;
     const uint32_t n = min(*((volatile uint32_t *)&s.ctr->giant), s.giant_cap);
     if (blockIdx.x >= n) return;  // whole CTA: no chunk for it
     level_prologue<BLOCK>(sm, s);
@@ -477,7 +478,7 @@ __device__ __forceinline__ void giant_body(const GraphDev &g, const BfsDev &s)
 
 template <int BLOCK>
 __device__ __forceinline__ void pull_body(const GraphDev &g, const BfsDev &s, uint32_t vlo, uint32_t vhi,
-                                          const RangeList &rl)
+                                          const RangeList &rl, LevelSmem &sm)
 {
     // A CTA takes a tile of kPullTileWords visited-bitmap words, compacts the
     // tile's unvisited vertices into q, and runs them one per thread (phase
@@ -489,9 +490,10 @@ __device__ __forceinline__ void pull_body(const GraphDev &g, const BfsDev &s, ui
     // then written once, without global atomics.
     constexpr int kGroup = SCAPH_PULL_GROUP;
     constexpr int kGroups = BLOCK / kGroup;
-    __shared__ LevelSmem sm;
     __shared__ uint32_t q[kPullTileWords * 32];
     __shared__ uint32_t fnd[kPullTileWords];
+    // the tile's live ranks and live words (BfsDev::live_rank), for phase A
+    __shared__ uint32_t t_rank[kPullTileWords], t_live[kPullTileWords];
     constexpr int kPPT = BLOCK >= 512 ? 1 : kPullPerThread;  // shared memory bounds the 512-thread CTA
     // phase-B queue: with SCAPH_PULL_DEFER_B the vertices of several rounds
     // wait here and phase B runs once they would overflow it (or at the end
@@ -756,11 +758,23 @@ __device__ __forceinline__ void pull_body(const GraphDev &g, const BfsDev &s, ui
                 for (int i = 0; i < kPPT; i++) {
                     if (!ok[i]) continue;
                     const uint32_t v = vv[i];
-                    dg[i] = __ldg(&s.degree[v]);  // travels with the row loads (needed if v is found)
-                    if (s.head) {
+                    if (s.head && s.live_rank && !gathered) {
+                        // the live vertices' arrays: v's live rank from the
+                        // tile's staged rank and live word
+                        const uint32_t wi = (v >> 5) - tbase;
+                        const uint32_t r = t_rank[wi] + __popc(t_live[wi] & ((1u << (v & 31)) - 1u));
+                        dg[i] = __ldg(&s.live_deg[r]);
+                        len[i] = __ldg(&s.live_indeg[r]);
+                        const uint4 h = ld_nc_v4(reinterpret_cast<const uint32_t *>(s.live_head + r));
+                        u[i][0] = h.x;
+                        u[i][1] = h.y;
+                        u[i][2] = h.z;
+                        u[i][3] = h.w;
+                    } else if (s.head) {
                         // dense rows: the in-degree and the first in-edges of
                         // consecutive vertices, independent coalesced loads; the
                         // page is read only if these do not decide
+                        dg[i] = __ldg(&s.degree[v]);  // travels with the row loads (needed if v is found)
                         len[i] = __ldg(&s.indeg[v]);
                         const uint4 h = ld_nc_v4(s.head + (size_t)kPullHead * v);
                         u[i][0] = h.x;
@@ -768,6 +782,7 @@ __device__ __forceinline__ void pull_body(const GraphDev &g, const BfsDev &s, ui
                         u[i][2] = h.z;
                         u[i][3] = h.w;
                     } else {
+                        dg[i] = __ldg(&s.degree[v]);
                         p[i] = lut.of(v);
                         const PageDev pd = lut.pages[p[i]];
                         if (pd.base != kNotResident) {
@@ -1231,6 +1246,10 @@ __device__ __forceinline__ void pull_body(const GraphDev &g, const BfsDev &s, ui
         if (threadIdx.x < kPullTileWords) {
             if (!gather) fnd[threadIdx.x] = 0;
             if (w < rwhi) unv = ~s.visited[w] & range_mask(w, rlo, rhi);
+            if (!gather && s.live_rank) {
+                t_rank[threadIdx.x] = w < rwhi ? s.live_rank[w] : 0u;
+                t_live[threadIdx.x] = w < rwhi ? ~s.dead[w] : 0u;
+            }
         }
         if (!__syncthreads_or(unv != 0)) continue;
         uint32_t total;
@@ -1367,14 +1386,16 @@ __global__ void __launch_bounds__(BLOCK, kPushMinThreads / BLOCK) k_push(GraphDe
 template <int BLOCK>
 __global__ void __launch_bounds__(BLOCK) k_push_giant(GraphDev g, BfsDev s)
 {
-    giant_body<BLOCK>(g, s);
+    __shared__ LevelSmem sm;
+    giant_body<BLOCK>(g, s, sm);
 }
 
 template <int BLOCK>
 __global__ void __launch_bounds__(BLOCK, kPullMinThreads / BLOCK) k_pull(GraphDev g, BfsDev s, uint32_t vlo, uint32_t vhi,
                                                             RangeList rl)
 {
-    pull_body<BLOCK>(g, s, vlo, vhi, rl);
+    __shared__ LevelSmem sm;
+    pull_body<BLOCK>(g, s, vlo, vhi, rl, sm);
 }
 
 template <int BLOCK>
@@ -1402,7 +1423,8 @@ template <int BLOCK>
 __global__ void __launch_bounds__(BLOCK) k_push_giant_g(GraphDev g, BfsGraphArgs a)
 {
     if (a.ctl->dir != 0) return;
-    giant_body<BLOCK>(g, level_state(a));
+    __shared__ LevelSmem sm;
+    giant_body<BLOCK>(g, level_state(a), sm);
 }
 
 template <int BLOCK>
@@ -1418,7 +1440,25 @@ __global__ void __launch_bounds__(BLOCK, kPullMinThreads / BLOCK) k_pull_g(Graph
     if (a.ctl->dir != 1) return;
     const BfsDev s = level_state(a);
     clear_third(a, s.level);
-    pull_body<BLOCK>(g, s, 0, s.V, RangeList{nullptr, nullptr, nullptr, 0});
+    __shared__ LevelSmem sm;
+    pull_body<BLOCK>(g, s, 0, s.V, RangeList{nullptr, nullptr, nullptr, 0}, sm);
+}
+
+// The giant chunks of a push level and the pull of a pull level in one
+// kernel node (a level runs one of them), so that each level launches one
+// node fewer; one LevelSmem serves either body.
+template <int BLOCK>
+__global__ void __launch_bounds__(BLOCK, kPullMinThreads / BLOCK) k_giant_pull_g(GraphDev gout, GraphDev gin,
+                                                                             BfsGraphArgs a)
+{
+    __shared__ LevelSmem sm;
+    const BfsDev s = level_state(a);
+    if (a.ctl->dir == 0) {
+        giant_body<BLOCK>(gout, s, sm);
+    } else {
+        clear_third(a, s.level);
+        pull_body<BLOCK>(gin, s, 0, s.V, RangeList{nullptr, nullptr, nullptr, 0}, sm);
+    }
 }
 
 // First node of a BFS graph: run inputs into the control block, state reset
@@ -1731,23 +1771,27 @@ cudaError_t run_level(int dir, int block, int grid, const GraphDev &g, const Bfs
     }
 }
 
-void level_graph_kernels(int block, const void **push, const void **giant, const void **pull)
+void level_graph_kernels(int block, const void **push, const void **giant, const void **pull,
+                         const void **giant_pull)
 {
     switch (block) {
     case 128:
         *push = (const void *)k_push_g<128>;
         *giant = (const void *)k_push_giant_g<128>;
         *pull = (const void *)k_pull_g<128>;
+        *giant_pull = (const void *)k_giant_pull_g<128>;
         break;
     case 512:
         *push = (const void *)k_push_g<512>;
         *giant = (const void *)k_push_giant_g<512>;
         *pull = (const void *)k_pull_g<512>;
+        *giant_pull = (const void *)k_giant_pull_g<512>;
         break;
     default:
         *push = (const void *)k_push_g<256>;
         *giant = (const void *)k_push_giant_g<256>;
         *pull = (const void *)k_pull_g<256>;
+        *giant_pull = (const void *)k_giant_pull_g<256>;
         break;
     }
 }

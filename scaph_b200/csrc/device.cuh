@@ -90,6 +90,16 @@ struct BfsDev {
     // x, y, z = the three top-ranked in-neighbours (0xFFFFFFFF past the
     // in-degree), w = pull_meta(in-degree, out-degree)
     const uint4 *prow;
+    // pull, CTA tiles on levels without records: the in-degree, out-degree
+    // and head row of the live vertices (in-degree > 0) only, in vertex
+    // order, so that a 32-byte sector holds no vertex without edges;
+    // live_rank[w] = live vertices in the words before w, dead = the bitmap
+    // of the others (null: phase A reads the V-entry arrays)
+    const uint32_t *live_rank;
+    const uint32_t *dead;
+    const uint4 *live_head;
+    const uint32_t *live_indeg;
+    const uint32_t *live_deg;
     // histogram of the discovered vertices over the IN-edge graph's pages
     // (count, sum(indeg+3)): keeps the pull-side page counts current without
     // a pass over all vertices (directed graphs; null when not wanted)

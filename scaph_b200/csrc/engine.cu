@@ -23,6 +23,15 @@
 #include <utility>
 
 #include "engine.h"
+
+// the pull's CTA tiles read the phase-A arrays of the live vertices only
+#ifndef SCAPH_PULL_LIVE
+#define SCAPH_PULL_LIVE 1
+#endif
+// graph mode runs a level's giant chunks and pull in one kernel node
+#ifndef SCAPH_GRAPH_GIANT_PULL
+#define SCAPH_GRAPH_GIANT_PULL 1
+#endif
 #include "kernels.h"
 
 using namespace scaph;
@@ -128,10 +137,60 @@ BfsDev scaph_engine::base_state(uint32_t *dd, uint32_t *dp) const
     s.head_ranked = head_ranked ? 1u : 0u;
     s.prec = d_prec;
     s.prow = cfg.pull_rows == 1 && head_ranked ? d_prow : nullptr;  // phase B rescans ranked rows from 0
+    s.live_rank = d_live_rank;
+    s.dead = d_dead;
+    s.live_head = d_live_head;
+    s.live_indeg = d_live_indeg;
+    s.live_deg = d_live_deg;
     s.push_sparse = push_use_sparse(cfg.push_sparse_ratio, 1, V) ? 1u : 0u;  // level 0
     s.giant_edges = (uint32_t)cfg.giant_edges;
     s.pull_warp = cfg.pull_warp == 3 ? 0u : (uint32_t)cfg.pull_warp;  // kernel: 0 tiles, 1 warp, 2 lanes
     return s;
+}
+
+// The pull's phase-A arrays over the live vertices only (in-degree > 0, the
+// vertices a traversal can discover), indexed by live rank: rank(v) =
+// live_rank[v / 32] + the live vertices below v in its word.  On RMAT-24
+// 56% of the vertices have no edge; in the V-entry arrays their entries
+// share every sector with live ones, so the small-frontier pull level read
+// 44 bytes of sectors per unvisited vertex for 24 bytes of fields.
+static __global__ void k_build_live(const uint32_t *dead, const uint32_t *rank, const uint32_t *head,
+                                    const uint32_t *indeg, const uint32_t *deg, uint4 *lhead, uint32_t *lindeg,
+                                    uint32_t *ldeg, uint32_t V)
+{
+    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < V; v += gridDim.x * blockDim.x) {
+        const uint32_t w = v >> 5, live = ~dead[w];
+        if (!((live >> (v & 31)) & 1u)) continue;
+        const uint32_t r = rank[w] + __popc(live & ((1u << (v & 31)) - 1u));
+        lhead[r] = reinterpret_cast<const uint4 *>(head)[v];
+        lindeg[r] = indeg[v];
+        ldeg[r] = deg[v];
+    }
+}
+
+int scaph_engine::build_live(const std::vector<uint32_t> &dead)
+{
+    if (!d_head || !head_ranked) return SCAPH_OK;
+    std::vector<uint32_t> rank(nwords + 1);
+    uint32_t n = 0;
+    for (uint32_t w = 0; w < nwords; w++) {
+        rank[w] = n;
+        const uint32_t valid = (w + 1) * 32ull <= V ? 0xFFFFFFFFu : ((1u << (V & 31)) - 1u);
+        n += __builtin_popcount(~dead[w] & valid);
+    }
+    rank[nwords] = n;
+    if (n != V - n_dead) return set_error(SCAPH_EINVAL, "live vertex count %u != %u", n, (unsigned)(V - n_dead));
+    SCAPH_CUDA(cudaMalloc(&d_live_rank, (size_t)(nwords + 1) * 4));
+    SCAPH_CUDA(cudaMemcpyAsync(d_live_rank, rank.data(), (size_t)(nwords + 1) * 4, cudaMemcpyHostToDevice, st));
+    const size_t nl = std::max<uint32_t>(n, 1);
+    SCAPH_CUDA(cudaMalloc(&d_live_head, nl * sizeof(uint4)));
+    SCAPH_CUDA(cudaMalloc(&d_live_indeg, nl * 4));
+    SCAPH_CUDA(cudaMalloc(&d_live_deg, nl * 4));
+    k_build_live<<<num_sms * 8, 256, 0, st>>>(d_dead, d_live_rank, d_head, d_indeg, d_degree, d_live_head,
+                                              d_live_indeg, d_live_deg, V);
+    SCAPH_CUDA(cudaGetLastError());
+    SCAPH_CUDA(cudaStreamSynchronize(st));  // rank lives on the host stack until here
+    return SCAPH_OK;
 }
 
 // The 16-byte pull rows (scaph_config.pull_rows = 1): the first three ranked
@@ -260,6 +319,9 @@ int scaph_engine::create(const Graph *g_, const Graph *gt_, const scaph_config *
     SCAPH_CUDA(cudaMalloc(&d_bm3, (size_t)nwords * 4 * 3));
     SCAPH_CUDA(cudaMalloc(&d_degree, (size_t)V * 4));
     SCAPH_CUDA(cudaMemcpyAsync(d_degree, g->degree.data(), (size_t)V * 4, cudaMemcpyHostToDevice, st));
+#if SCAPH_PULL_LIVE
+    if ((rc = build_live(dead))) return rc;
+#endif
     SCAPH_CUDA(cudaMalloc(&d_ctr, sizeof(LevelCounters) * kMaxLevels));
     SCAPH_CUDA(cudaMallocHost(&h_ctr, sizeof(LevelCounters) * kMaxLevels));
     SCAPH_CUDA(cudaMalloc(&d_ctl, sizeof(BfsCtl)));
@@ -308,6 +370,10 @@ void scaph_engine::destroy()
     cudaFree(d_head);
     cudaFree(d_prec);
     cudaFree(d_prow);
+    cudaFree(d_live_rank);
+    cudaFree(d_live_head);
+    cudaFree(d_live_indeg);
+    cudaFree(d_live_deg);
     cudaFree(d_snap);
     cudaFree(d_pcnt);
     cudaFree(d_pdatas);
@@ -735,30 +801,47 @@ int scaph_engine::build_graph()
     SCAPH_CUDA(cudaGraphAddNode(&n_while, graph, &n_start, 1, &wp));
     cudaGraph_t body = wp.conditional.phGraph_out[0];
 
-    const void *f_push, *f_giant, *f_pull;
-    level_graph_kernels(block, &f_push, &f_giant, &f_pull);
+    const void *f_push, *f_giant, *f_pull, *f_giant_pull;
+    level_graph_kernels(block, &f_push, &f_giant, &f_pull, &f_giant_pull);
     GraphDev gout = dout.view, gpull = gin();
     void *push_args[] = {&gout, &gargs};
-    void *pull_args[] = {&gpull, &gargs};
-    cudaGraphNode_t n_push, n_giant, n_pull;
+    cudaGraphNode_t n_push, n_pull;
     cudaKernelNodeParams lp{};
     lp.func = const_cast<void *>(f_push);
     lp.gridDim = dim3(grid_push);
     lp.blockDim = dim3(block);
     lp.kernelParams = push_args;
     SCAPH_CUDA(cudaGraphAddKernelNode(&n_push, body, nullptr, 0, &lp));
+    void *fin_args[] = {&gargs};
+    cudaKernelNodeParams fp{};
+    fp.func = const_cast<void *>(push_finalize_graph_kernel(block));
+    fp.gridDim = dim3(num_sms * 4);
+    fp.blockDim = dim3(block);
+    fp.kernelParams = fin_args;
+#if SCAPH_GRAPH_GIANT_PULL
+    // push; giant chunks or pull (one node); [finalize of deferred claims]
+    void *giant_pull_args[] = {&gout, &gpull, &gargs};
+    lp.func = const_cast<void *>(f_giant_pull);
+    lp.gridDim = dim3(std::max(grid_push, grid_pull));
+    lp.kernelParams = giant_pull_args;
+    SCAPH_CUDA(cudaGraphAddKernelNode(&n_pull, body, &n_push, 1, &lp));
+    if (cfg.push_defer_edges > 0) {
+        cudaGraphNode_t n_fin;
+        SCAPH_CUDA(cudaGraphAddKernelNode(&n_fin, body, &n_pull, 1, &fp));
+        n_pull = n_fin;
+    }
+    (void)f_giant;
+    (void)f_pull;
+#else
+    // push; giant chunks; [finalize of deferred claims]; pull
+    (void)f_giant_pull;
+    void *pull_args[] = {&gpull, &gargs};
+    cudaGraphNode_t n_giant;
     lp.func = const_cast<void *>(f_giant);
     SCAPH_CUDA(cudaGraphAddKernelNode(&n_giant, body, &n_push, 1, &lp));
     cudaGraphNode_t n_before_pull = n_giant;
-    void *fin_args[] = {&gargs};
     if (cfg.push_defer_edges > 0) {
-        // deferred-claim push levels: the finalize pass after the giant chunks
         cudaGraphNode_t n_fin;
-        cudaKernelNodeParams fp{};
-        fp.func = const_cast<void *>(push_finalize_graph_kernel(block));
-        fp.gridDim = dim3(num_sms * 4);
-        fp.blockDim = dim3(block);
-        fp.kernelParams = fin_args;
         SCAPH_CUDA(cudaGraphAddKernelNode(&n_fin, body, &n_giant, 1, &fp));
         n_before_pull = n_fin;
     }
@@ -766,6 +849,7 @@ int scaph_engine::build_graph()
     lp.gridDim = dim3(grid_pull);
     lp.kernelParams = pull_args;
     SCAPH_CUDA(cudaGraphAddKernelNode(&n_pull, body, &n_before_pull, 1, &lp));
+#endif
 
     const bool learned = cfg.direction == SCAPH_DIR_LEARNED && sched;
     MlpDev net{};
@@ -855,9 +939,10 @@ int scaph_engine::collect(bool from_graph)
         if (from_graph) {
             t.ms = (double)(lc.t_end - tprev) * 1e-6;
             tprev = lc.t_end;
-            // push, giant, pull and decide (and the finalize node when deferred
-            // claims are on) run every level; the unselected ones leave at once
-            launches += cfg.push_defer_edges > 0 ? 5 : 4;
+            // push, giant + pull (one node) and decide (and the finalize node
+            // when deferred claims are on) run every level; the unselected
+            // ones leave at once
+            launches += (cfg.push_defer_edges > 0 ? 5 : 4) - (SCAPH_GRAPH_GIANT_PULL ? 1 : 0);
         } else {
             float ms = 0;
             cudaEventElapsedTime(&ms, ev_level[2 * l], ev_level[2 * l + 1]);

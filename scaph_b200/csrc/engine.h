@@ -159,6 +159,10 @@ struct scaph_engine {
     uint32_t *d_head = nullptr;     // kPullHead in-edges per vertex (pull phase A)
     uint2 *d_prec = nullptr;        // 8-byte pull record per vertex (pull phase A)
     uint4 *d_prow = nullptr;        // 16-byte pull row per vertex (phase A without records)
+    uint32_t *d_live_rank = nullptr;  // live vertices before each bitmap word (nwords + 1)
+    uint4 *d_live_head = nullptr;     // head rows of the live vertices, by live rank
+    uint32_t *d_live_indeg = nullptr; // in-degrees of the live vertices, by live rank
+    uint32_t *d_live_deg = nullptr;   // out-degrees of the live vertices, by live rank
     bool head_ranked = false;       // d_head holds the top in-neighbours by out-degree
     std::vector<uint64_t> level_h2d;  // page bytes copied per level of the last run
     uint64_t pcie_alg = 0;            // algorithmic link bytes of the last run
@@ -209,6 +213,7 @@ struct scaph_engine {
     int bfs(uint32_t src, uint32_t *depths, uint32_t *parents, int out_on_device, scaph_bfs_stats *stats);
     int run_host_loop(uint32_t src, uint32_t *dd, uint32_t *dp);
     int build_prow();
+    int build_live(const std::vector<uint32_t> &dead);
     int features(int level, uint32_t src, uint64_t nf, uint64_t mf, uint64_t unvis, uint64_t mu, int prev_dir,
                  int ab_dir, float *f, std::vector<uint32_t> &pull_cnt, std::vector<uint32_t> &hist);
     int build_graph();

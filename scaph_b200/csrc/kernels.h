@@ -23,7 +23,10 @@ const void *push_finalize_graph_kernel(int block);
 // k_graph_init(BfsGraphArgs, u32* depth, u32* parent, u32 src, u32 unreached, const u32* dead, u32 nlevels_clear)
 // Graph mode: the push, giant-chunk and pull kernels of a level (each leaves
 // at once unless the level's direction selects it).
-void level_graph_kernels(int block, const void **push, const void **giant, const void **pull);
+// graph-mode level kernels; giant_pull runs a push level's giant chunks or
+// a pull level's pull (one node instead of two)
+void level_graph_kernels(int block, const void **push, const void **giant, const void **pull,
+                         const void **giant_pull);
 const void *graph_init_kernel();
 // k_graph_start(BfsGraphArgs)
 const void *graph_start_kernel();

@@ -14,8 +14,8 @@ cases:
   batch    mixed batch of 64 queries over 8 RMAT graphs (k_bt_*), one launch
   pager    out-of-core BFS through a small page pool (k_page_counts, copies,
            zero-copy reads), RMAT-S
-  mlp      scheduler network: training steps and forward calls (k_gemm,
-           k_bce, k_adam, k_forward1)
+  mlp      scheduler network: training steps, forward calls and the
+           device timing of both (k_gemm, k_bce, k_adam, k_forward1)
 """
 from __future__ import annotations
 
@@ -105,7 +105,9 @@ def case_mlp(scale: int, reps: int) -> str:
     net.train(X, T, W, epochs=reps, batch=256, lr=1e-3)
     for _ in range(reps):
         net.forward(X[:1])
-    return f"{reps} training steps and {reps} single-row forward calls: {time.perf_counter() - t0:.3f} s"
+    dev = net.time(n=256, reps=reps)  # CUDA-event timing; launches the single-row kernel k_forward1
+    return (f"{reps} training steps and {reps} single-row forward calls: {time.perf_counter() - t0:.3f} s; "
+            f"device us: {dev}")
 
 
 def main(argv=None) -> None:
