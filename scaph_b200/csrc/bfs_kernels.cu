@@ -1021,6 +1021,9 @@ __device__ __forceinline__ void pull_body(const GraphDev &g, const BfsDev &s, ui
         constexpr uint32_t kChunkWords = 16, kChunks = kPullTileWords / kChunkWords;
         static_assert(kChunkWords * 32 * (256 / 32) <= kPullTileWords * 32, "per-warp queues fit q");
         const int warp = threadIdx.x >> 5;
+        // records by live rank (BfsDev::live_prec): each lane of the first 16
+        // holds its word's live rank and live bits, the others shuffle them
+        const bool live = s.live_prec != nullptr;
         uint32_t *qw = q + warp * (kChunkWords * 32);
         uint32_t *fw = fnd + warp * kChunkWords;
         const uint32_t nchunks = ntiles * kChunks, warps = gridDim.x * (BLOCK / 32);
@@ -1030,10 +1033,14 @@ __device__ __forceinline__ void pull_body(const GraphDev &g, const BfsDev &s, ui
             const uint32_t rwhi = (uint32_t)(((unsigned long long)rhi + 31) >> 5);
             const uint32_t wbase = (rlo >> 5) + local * kPullTileWords + (c % kChunks) * kChunkWords;
             const uint32_t w = wbase + lane;
-            uint32_t unv = 0;
+            uint32_t unv = 0, wl_rank = 0, wl_live = 0;
             if (lane < (int)kChunkWords) {
                 fw[lane] = 0;
                 if (w < rwhi) unv = ~s.visited[w] & range_mask(w, rlo, rhi);
+                if (live && w < rwhi) {
+                    wl_rank = s.live_rank[w];
+                    wl_live = ~s.dead[w];
+                }
             }
             const uint32_t cnt = __popc(unv);
             uint32_t inc = cnt;
@@ -1062,15 +1069,24 @@ __device__ __forceinline__ void pull_body(const GraphDev &g, const BfsDev &s, ui
                 hist_in_add(sm, s, v);
             };
             for (uint32_t k0 = 0; k0 < total; k0 += 32 * kPPT) {
-                uint32_t vv[kPPT], dg[kPPT];
+                uint32_t vv[kPPT], dg[kPPT], rr[kPPT];
                 uint2 rec[kPPT];
                 bool slow[kPPT];
 #pragma unroll
                 for (int i = 0; i < kPPT; i++) {
                     const uint32_t k = k0 + i * 32 + lane;
                     vv[i] = k < total ? qw[k] : 0xFFFFFFFFu;
+                    rr[i] = 0;
+                    if (live) {  // uniform: every lane shuffles
+                        const int wi = (int)(((vv[i] >> 5) - wbase) & 31u);
+                        const uint32_t base = __shfl_sync(0xFFFFFFFFu, wl_rank, wi);
+                        const uint32_t lw = __shfl_sync(0xFFFFFFFFu, wl_live, wi);
+                        rr[i] = base + __popc(lw & ((1u << (vv[i] & 31)) - 1u));
+                    }
                     if (vv[i] == 0xFFFFFFFFu) {
                         rec[i] = make_uint2(0xFFFFFFFFu, 0u);
+                    } else if (s.prec && live) {
+                        rec[i] = ld_nc_v2(s.live_prec + rr[i]);
                     } else if (s.prec) {
                         rec[i] = ld_nc_v2(s.prec + vv[i]);
                     } else {
@@ -1105,8 +1121,9 @@ __device__ __forceinline__ void pull_body(const GraphDev &g, const BfsDev &s, ui
                     unsigned long long st = 0;
                     if (slow[i]) {
                         const uint32_t v = vv[i];
-                        len = __ldg(&s.indeg[v]);
-                        const uint4 h = ld_nc_v4(s.head + (size_t)kPullHead * v);
+                        len = live ? __ldg(&s.live_indeg[rr[i]]) : __ldg(&s.indeg[v]);
+                        const uint4 h = live ? ld_nc_v4(reinterpret_cast<const uint32_t *>(s.live_head + rr[i]))
+                                             : ld_nc_v4(s.head + (size_t)kPullHead * v);
                         if (dg[i] == kPrecDegMax) dg[i] = __ldg(&s.degree[v]);
                         uint32_t par = kNoParent, j = 0;
                         if (h.y < s.V && test_bit(s.front, h.y)) par = h.y, j = 2;

@@ -100,6 +100,7 @@ struct BfsDev {
     const uint4 *live_head;
     const uint32_t *live_indeg;
     const uint32_t *live_deg;
+    const uint2 *live_prec;    // the 8-byte records of the live vertices (read where prec is set)
     // histogram of the discovered vertices over the IN-edge graph's pages
     // (count, sum(indeg+3)): keeps the pull-side page counts current without
     // a pass over all vertices (directed graphs; null when not wanted)

@@ -28,6 +28,10 @@
 #ifndef SCAPH_PULL_LIVE
 #define SCAPH_PULL_LIVE 1
 #endif
+// ... and the warp-centric pull reads the records of the live vertices
+#ifndef SCAPH_PULL_LIVE_REC
+#define SCAPH_PULL_LIVE_REC 1
+#endif
 // graph mode runs a level's giant chunks and pull in one kernel node
 #ifndef SCAPH_GRAPH_GIANT_PULL
 #define SCAPH_GRAPH_GIANT_PULL 1
@@ -142,6 +146,7 @@ BfsDev scaph_engine::base_state(uint32_t *dd, uint32_t *dp) const
     s.live_head = d_live_head;
     s.live_indeg = d_live_indeg;
     s.live_deg = d_live_deg;
+    s.live_prec = d_live_prec;
     s.push_sparse = push_use_sparse(cfg.push_sparse_ratio, 1, V) ? 1u : 0u;  // level 0
     s.giant_edges = (uint32_t)cfg.giant_edges;
     s.pull_warp = cfg.pull_warp == 3 ? 0u : (uint32_t)cfg.pull_warp;  // kernel: 0 tiles, 1 warp, 2 lanes
@@ -155,8 +160,8 @@ BfsDev scaph_engine::base_state(uint32_t *dd, uint32_t *dp) const
 // share every sector with live ones, so the small-frontier pull level read
 // 44 bytes of sectors per unvisited vertex for 24 bytes of fields.
 static __global__ void k_build_live(const uint32_t *dead, const uint32_t *rank, const uint32_t *head,
-                                    const uint32_t *indeg, const uint32_t *deg, uint4 *lhead, uint32_t *lindeg,
-                                    uint32_t *ldeg, uint32_t V)
+                                    const uint32_t *indeg, const uint32_t *deg, const uint2 *prec, uint4 *lhead,
+                                    uint32_t *lindeg, uint32_t *ldeg, uint2 *lprec, uint32_t V)
 {
     for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < V; v += gridDim.x * blockDim.x) {
         const uint32_t w = v >> 5, live = ~dead[w];
@@ -165,12 +170,13 @@ static __global__ void k_build_live(const uint32_t *dead, const uint32_t *rank, 
         lhead[r] = reinterpret_cast<const uint4 *>(head)[v];
         lindeg[r] = indeg[v];
         ldeg[r] = deg[v];
+        if (lprec) lprec[r] = prec[v];
     }
 }
 
 int scaph_engine::build_live(const std::vector<uint32_t> &dead)
 {
-    if (!d_head || !head_ranked) return SCAPH_OK;
+    if (!d_head || !d_prec || !head_ranked) return SCAPH_OK;
     std::vector<uint32_t> rank(nwords + 1);
     uint32_t n = 0;
     for (uint32_t w = 0; w < nwords; w++) {
@@ -186,8 +192,11 @@ int scaph_engine::build_live(const std::vector<uint32_t> &dead)
     SCAPH_CUDA(cudaMalloc(&d_live_head, nl * sizeof(uint4)));
     SCAPH_CUDA(cudaMalloc(&d_live_indeg, nl * 4));
     SCAPH_CUDA(cudaMalloc(&d_live_deg, nl * 4));
-    k_build_live<<<num_sms * 8, 256, 0, st>>>(d_dead, d_live_rank, d_head, d_indeg, d_degree, d_live_head,
-                                              d_live_indeg, d_live_deg, V);
+#if SCAPH_PULL_LIVE_REC
+    SCAPH_CUDA(cudaMalloc(&d_live_prec, nl * sizeof(uint2)));
+#endif
+    k_build_live<<<num_sms * 8, 256, 0, st>>>(d_dead, d_live_rank, d_head, d_indeg, d_degree, d_prec, d_live_head,
+                                              d_live_indeg, d_live_deg, d_live_prec, V);
     SCAPH_CUDA(cudaGetLastError());
     SCAPH_CUDA(cudaStreamSynchronize(st));  // rank lives on the host stack until here
     return SCAPH_OK;
@@ -374,6 +383,7 @@ void scaph_engine::destroy()
     cudaFree(d_live_head);
     cudaFree(d_live_indeg);
     cudaFree(d_live_deg);
+    cudaFree(d_live_prec);
     cudaFree(d_snap);
     cudaFree(d_pcnt);
     cudaFree(d_pdatas);

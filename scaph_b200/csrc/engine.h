@@ -163,6 +163,7 @@ struct scaph_engine {
     uint4 *d_live_head = nullptr;     // head rows of the live vertices, by live rank
     uint32_t *d_live_indeg = nullptr; // in-degrees of the live vertices, by live rank
     uint32_t *d_live_deg = nullptr;   // out-degrees of the live vertices, by live rank
+    uint2 *d_live_prec = nullptr;     // 8-byte pull records of the live vertices, by live rank
     bool head_ranked = false;       // d_head holds the top in-neighbours by out-degree
     std::vector<uint64_t> level_h2d;  // page bytes copied per level of the last run
     uint64_t pcie_alg = 0;            // algorithmic link bytes of the last run
