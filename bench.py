@@ -4,7 +4,7 @@
 Workload (default): RMAT scale 24, edge factor 16, a/b/c/d = .57/.19/.19/.05,
 seeded, symmetrised, deduplicated, uint32 ids, paged CSR with 10 Mi-word
 pages, fully resident in HBM; 64 seeded random sources with nonzero degree,
-each run separately; Beamer alpha/beta direction switch (alpha 14, beta 24).
+each run separately; Beamer alpha/beta direction switch (alpha 14, beta 96).
 One step = one single-source BFS.  GTEPS follows the reference's formula,
 edge_count / traversal time (src/app.cuh:252).
 
@@ -133,7 +133,7 @@ def gpu_index(local_rank: int) -> int:
 
 def config_dict(V, E, scale, nsrc):
     """The workload's description; identical in both arms."""
-    return {"workload": f"rmat{scale}-ef16 single-source BFS, {nsrc} seeded sources, alpha/beta 14/24, in HBM",
+    return {"workload": f"rmat{scale}-ef16 single-source BFS, {nsrc} seeded sources, alpha/beta 14/96, in HBM",
             "graph": f"RMAT scale {scale}, ef 16, a/b/c/d .57/.19/.19/.05, symmetrised, dedup",
             "V": V, "E": E, "sources": nsrc, "pagesize_words": 10 * 1024 * 1024,
             "l2": "inputs larger than L2 (paged graph %.2f GB > 126 MB)" % (4 * (3 * V + E) / 1e9)}

@@ -198,7 +198,7 @@ typedef struct scaph_config {
                                   (reference app uses 63, app/bfs.cu:18)    */
     int32_t  direction;        /* SCAPH_DIR_*                               */
     float    alpha;            /* 0 -> 14                                   */
-    float    beta;             /* 0 -> 24                                   */
+    float    beta;             /* 0 -> 96                                   */
     int32_t  block_size;       /* threads per CTA of the level kernels; 0=256
                                   (FLAGS_num_thds, src/app.cuh:43)          */
     int32_t  ctas_per_sm;      /* 0 = from occupancy                        */

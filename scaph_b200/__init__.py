@@ -471,7 +471,7 @@ class Engine:
 
     def __init__(self, graph: PagedGraph, transposed: PagedGraph | None = None, *, pool_bytes: int = 0,
                  unreached: int = UNREACHED, direction: int = DIR_ALPHABETA, alpha: float = 14.0,
-                 beta: float = 24.0, block_size: int = 256, ctas_per_sm: int = 0, copy_streams: int = 2,
+                 beta: float = 96.0, block_size: int = 256, ctas_per_sm: int = 0, copy_streams: int = 2,
                  prefetch: int = 0, compact_threshold: int = 3, use_graph: int = 0, device: int = 0,
                  stream: int | None = None, record_features: int = 0, dual_timing: int = 0,
                  link_gbs: float = 0.0, giant_edges: int = 0, pull_gather_ratio: int = 0,

@@ -121,6 +121,15 @@ struct BfsDev {
     uint32_t _pad;
 };
 
+// Defaults of scaph_config.alpha and beta (Beamer's switch: push -> pull
+// when the frontier's out-edges exceed the unvisited edges / alpha, pull ->
+// push when the frontier shrinks below V / beta).  beta = 96 rather than
+// Beamer's 24: on RMAT-24 the level after the big pull level then pulls too
+// (31 us instead of 45 us pushed) and the tail push levels start smaller
+// (alternating A/B on one box: 611 -> 624 GTEPS).
+constexpr float kAlphaDefault = 14.0f;
+constexpr float kBetaDefault = 96.0f;
+
 // Default of scaph_config.push_defer_edges: push levels whose frontier has
 // at least 2^20 out-edges defer their claims (RMAT-24, 8 sources, graph
 // mode: 508 -> 521 GTEPS alone, 537 with the warp-centric pull).

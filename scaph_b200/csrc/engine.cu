@@ -236,8 +236,8 @@ int scaph_engine::create(const Graph *g_, const Graph *gt_, const scaph_config *
     nwords = (V + 31) / 32;
     unreached = cfg.unreached ? cfg.unreached : 0xFFFFFFFFu;
     if (unreached < 2) return set_error(SCAPH_EINVAL, "unreached sentinel must be >= 2");
-    if (cfg.alpha <= 0) cfg.alpha = 14.0f;
-    if (cfg.beta <= 0) cfg.beta = 24.0f;
+    if (cfg.alpha <= 0) cfg.alpha = kAlphaDefault;
+    if (cfg.beta <= 0) cfg.beta = kBetaDefault;
     block = cfg.block_size == 128 || cfg.block_size == 512 ? cfg.block_size : 256;
     if (cfg.giant_edges == 0) cfg.giant_edges = (int32_t)kGiantEdges;
     if (cfg.giant_edges < 128 || cfg.giant_edges > 65536)
@@ -1156,8 +1156,8 @@ int scaph_engine_tune(scaph_engine *e, const scaph_config *c)
     SCAPH_CUDA(cudaStreamSynchronize(e->st));
     e->drop_graph();  // the graph bakes in grid sizes and decision arguments
     scaph_config &k = e->cfg;
-    k.alpha = c->alpha > 0 ? c->alpha : 14.0f;
-    k.beta = c->beta > 0 ? c->beta : 24.0f;
+    k.alpha = c->alpha > 0 ? c->alpha : kAlphaDefault;
+    k.beta = c->beta > 0 ? c->beta : kBetaDefault;
     k.giant_edges = ge;
     k.pull_gather_ratio = c->pull_gather_ratio > 0 ? c->pull_gather_ratio : (int32_t)kPullGatherRatio;
     k.ms_compact_l2_div = c->ms_compact_l2_div > 0 ? c->ms_compact_l2_div : 3;

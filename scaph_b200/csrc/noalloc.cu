@@ -181,7 +181,8 @@ extern "C" int scaph_bfs_page_noalloc(const uint32_t *d_page, uint32_t nodenum, 
     // reused every level, and the loop ends once a level discovers nothing
     // (at most V levels)
     for (; nf > 0 && (uint64_t)level + 1 < unreached; level++) {
-        if (level > 0 && symmetric) dir = alpha_beta_next(dir, nf, prev_nf, mf, E - vis_e, V, 14.0f, 24.0f);
+        if (level > 0 && symmetric) dir = alpha_beta_next(dir, nf, prev_nf, mf, E - vis_e, V, kAlphaDefault,
+                                                                   kBetaDefault);
         SCAPH_CUDA(cudaMemsetAsync(ctr, 0, sizeof(LevelCounters), st));
         SCAPH_CUDA(cudaMemsetAsync(bm[cur ^ 1], 0, (size_t)nwords * 4, st));
         s.front = bm[cur];

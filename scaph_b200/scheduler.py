@@ -131,7 +131,7 @@ def ms_dataset(rows_list, n_out: int, w_page=0.5):
     return np.concatenate(Xs), np.concatenate(Ts), np.concatenate(Ws)
 
 
-def alpha_beta(cur, nf, prev_nf, mf, mu, V, alpha=14.0, beta=24.0) -> int:
+def alpha_beta(cur, nf, prev_nf, mf, mu, V, alpha=14.0, beta=96.0) -> int:
     """Beamer's rule, as the engine applies it (0 push, 1 pull)."""
     if cur == 0:
         return 1 if mf > mu / alpha else 0
@@ -184,7 +184,7 @@ def sequences(L: int):
 
 
 def label(tr: Trace, nslots: int, page_ms: float, V: int, n_out: int, n_in: int, symmetric: bool,
-          alpha=14.0, beta=24.0, resident=False, zc_words=None, page_words=None):
+          alpha=14.0, beta=96.0, resident=False, zc_words=None, page_words=None):
     """Cheapest sequence under the cost model; returns (dirs, feature rows
     recomputed along it, its cost, alpha/beta's cost).  resident=True: the
     graph is all in HBM (no page traffic, residency features 1).  Pages whose
