@@ -631,6 +631,8 @@ def extra_config5(stream, nsrc=128, nplain=8, ntrain=8):
                            "pcie_alg_bytes_per_level": st.pcie_alg_bytes / max(1, st.levels),
                            "directions": "".join("p" if t["direction"] else "P" for t in tr),
                            "level_ms": [round(float(t["ms"]), 2) for t in tr],
+                           "gap_ms": [round(float(t["push_ms"]), 2) for t in tr],
+                           "host_ms": [round(float(t["pull_ms"]), 2) for t in tr],
                            "level_h2d_mb": [round(int(t["h2d_bytes"]) / 1e6, 1) for t in tr]}
         out[name] = res
         eng.close()

@@ -361,8 +361,11 @@ typedef struct scaph_level_trace {
     uint64_t alg_bytes;         /* algorithmic HBM bytes of this level      */
     uint64_t h2d_bytes;
     double   ms;                /* device time of this level's kernels      */
-    double   push_ms;           /* dual_timing: both directions' times      */
-    double   pull_ms;
+    double   push_ms;           /* dual_timing: both directions' times;     */
+    double   pull_ms;           /* multi-source rows: push_ms = device time
+                                   between the previous level's end and this
+                                   level's start, pull_ms = host time of the
+                                   level's census and decisions            */
 } scaph_level_trace;
 int scaph_bfs_trace(scaph_engine *e, scaph_level_trace *out, int cap);
 /* Active-vertex histogram of the frontier at `level` of the last run:

@@ -1496,26 +1496,46 @@ __global__ void k_graph_init(BfsGraphArgs a, uint32_t *depth, uint32_t *parent, 
         c->push_defer = 0;
         c->pull_rec = 0;
         c->push_sparse = b.push_sparse;  // level 0: one frontier vertex
+        // the source (setsrc, app/bfs.cu:32-37): its depth, parent and bits
+        // are written by the fills below, each element by one thread
+        const unsigned long long d = b.degree[src];
+        c->nf = 1;
+        c->prev_nf = 0;
+        c->mf = d;
+        c->vis_n = 1;
+        c->vis_e = d;
         c->t_start = globaltimer();
     }
     const size_t stride = (size_t)gridDim.x * blockDim.x;
     const size_t i0 = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     // 16-byte stores where the array allows (the depth fill is most of this
     // kernel: 4 bytes per vertex)
-    auto fill = [&](uint32_t *p, uint32_t value, size_t n) {
+    // value everywhere except element at, which gets at_value
+    auto fill = [&](uint32_t *p, uint32_t value, size_t n, size_t at, uint32_t at_value) {
         size_t done = 0;
         if ((reinterpret_cast<uintptr_t>(p) & 15) == 0) {
             const uint4 v4 = make_uint4(value, value, value, value);
             const size_t n4 = n / 4;
-            for (size_t i = i0; i < n4; i += stride) reinterpret_cast<uint4 *>(p)[i] = v4;
+            for (size_t i = i0; i < n4; i += stride) {
+                uint4 x = v4;
+                if (i == at / 4) {
+                    const size_t k = at % 4;
+                    x.x = k == 0 ? at_value : value;
+                    x.y = k == 1 ? at_value : value;
+                    x.z = k == 2 ? at_value : value;
+                    x.w = k == 3 ? at_value : value;
+                }
+                reinterpret_cast<uint4 *>(p)[i] = x;
+            }
             done = n4 * 4;
         }
-        for (size_t i = done + i0; i < n; i += stride) p[i] = value;
+        for (size_t i = done + i0; i < n; i += stride) p[i] = i == at ? at_value : value;
     };
-    fill(depth, unreached, b.V);
-    if (parent) fill(parent, kNoParent, b.V);
-    for (size_t i = i0; i < b.nwords; i += stride) b.visited[i] = dead ? dead[i] : 0u;
-    fill(a.bm3, 0u, 3ull * b.nwords);
+    const uint32_t sbit = 1u << (src & 31);
+    fill(depth, unreached, b.V, src, 0u);
+    if (parent) fill(parent, kNoParent, b.V, src, src);
+    for (size_t i = i0; i < b.nwords; i += stride) b.visited[i] = (dead ? dead[i] : 0u) | (i == (src >> 5) ? sbit : 0u);
+    fill(a.bm3, 0u, 3ull * b.nwords, src >> 5, sbit);  // level 0's frontier: the source
     uint32_t *cw = reinterpret_cast<uint32_t *>(a.ctr0);
     const size_t nc = (size_t)nlevels_clear * sizeof(LevelCounters) / 4;
     for (size_t i = i0; i < nc; i += stride) cw[i] = 0u;
@@ -1523,23 +1543,6 @@ __global__ void k_graph_init(BfsGraphArgs a, uint32_t *depth, uint32_t *parent, 
         const size_t nh = (size_t)a.hist_levels * 2 * a.npages_h;
         for (size_t i = i0; i < nh; i += stride) a.hist0[i] = 0u;
     }
-}
-
-// Second node: the source (setsrc, app/bfs.cu:32-37) and the loop state.
-__global__ void k_graph_start(BfsGraphArgs a)
-{
-    BfsCtl *c = a.ctl;
-    const uint32_t s = c->src;
-    c->depth[s] = 0;
-    if (c->parent) c->parent[s] = s;
-    a.base.visited[s >> 5] |= 1u << (s & 31);
-    a.bm3[s >> 5] |= 1u << (s & 31);
-    const unsigned long long d = a.base.degree[s];
-    c->nf = 1;
-    c->prev_nf = 0;
-    c->mf = d;
-    c->vis_n = 1;
-    c->vis_e = d;
 }
 
 // Last node of each level: counters -> next direction (Beamer alpha/beta, or
@@ -1814,7 +1817,6 @@ void level_graph_kernels(int block, const void **push, const void **giant, const
 }
 
 const void *graph_init_kernel() { return (const void *)k_graph_init; }
-const void *graph_start_kernel() { return (const void *)k_graph_start; }
 const void *decide_kernel() { return (const void *)k_decide; }
 const void *decide_learned_kernel() { return (const void *)k_decide_learned; }
 

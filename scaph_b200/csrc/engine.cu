@@ -790,15 +790,8 @@ int scaph_engine::build_graph()
     kp.gridDim = dim3(num_sms * 4);
     kp.blockDim = dim3(256);
     kp.kernelParams = init_args;
+    // (the init node also writes the source's depth, parent and bits)
     SCAPH_CUDA(cudaGraphAddKernelNode(&n_init, graph, nullptr, 0, &kp));
-    void *start_args[] = {&gargs};
-    cudaKernelNodeParams sp{};
-    sp.func = const_cast<void *>(graph_start_kernel());
-    sp.gridDim = dim3(1);
-    sp.blockDim = dim3(1);
-    sp.kernelParams = start_args;
-    cudaGraphNode_t n_start;
-    SCAPH_CUDA(cudaGraphAddKernelNode(&n_start, graph, &n_init, 1, &sp));
 
     // WHILE(loop) { push; giant; pull; decide }: the level kernel the level's
     // direction does not select leaves at once (cheaper than IF nodes)
@@ -808,7 +801,7 @@ int scaph_engine::build_graph()
     wp.conditional.type = cudaGraphCondTypeWhile;
     wp.conditional.size = 1;
     cudaGraphNode_t n_while;
-    SCAPH_CUDA(cudaGraphAddNode(&n_while, graph, &n_start, 1, &wp));
+    SCAPH_CUDA(cudaGraphAddNode(&n_while, graph, &n_init, 1, &wp));
     cudaGraph_t body = wp.conditional.phGraph_out[0];
 
     const void *f_push, *f_giant, *f_pull, *f_giant_pull;
@@ -927,7 +920,7 @@ int scaph_engine::collect(bool from_graph)
     uint32_t err = 0;
     const bool src_dead = gt ? gt->degree[src] == 0 : g->degree[src] == 0;
     unsigned long long tprev = from_graph ? h_ctl->t_start : 0;
-    launches = from_graph ? 2 : (dp ? 3 : 2);
+    launches = from_graph ? 1 : (dp ? 3 : 2);
     for (int l = 0; l < last_levels; l++) {
         const LevelCounters &lc = h_ctr[l];
         err |= lc.error;

@@ -28,8 +28,6 @@ const void *push_finalize_graph_kernel(int block);
 void level_graph_kernels(int block, const void **push, const void **giant, const void **pull,
                          const void **giant_pull);
 const void *graph_init_kernel();
-// k_graph_start(BfsGraphArgs)
-const void *graph_start_kernel();
 // k_decide(BfsGraphArgs, DecideArgs, handle loop)
 const void *decide_kernel();
 // k_decide_learned(BfsGraphArgs, DecideArgs, MlpDev, handle loop): 64 threads

@@ -5,6 +5,7 @@
 // app/bfs.cu:137-140).  This file is the host loop: one launch per phase and
 // level, the direction rule between levels, depths unpacked at the end into
 // u32 depth[i][V], bit-exact with single-source BFS.
+#include <chrono>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -297,7 +298,9 @@ static int ms_run(scaph_engine *e, const uint32_t *srcs, int nsrc, uint32_t *out
         y.resize(out_dim);
     }
     uint64_t npref = 0;
+    std::vector<double> host_ms;  // per level: census and decisions on the host
     while (nf > 0 && level < kMaxLevels && (uint64_t)level + 1 < e->unreached) {
+        const auto h0 = std::chrono::steady_clock::now();
         const uint64_t mu = e->E > done_e ? e->E - done_e : 0;
         const int prev_dir = dir;
         const int ab = level == 0 ? 0 : alpha_beta_next(dir, nf, prev_nf, mf, mu, V, alpha, beta);
@@ -390,6 +393,7 @@ static int ms_run(scaph_engine *e, const uint32_t *srcs, int nsrc, uint32_t *out
             s.planes[k] = m->planes[k];
             planes_used = k + 1;
         }
+        host_ms.push_back(std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - h0).count());
         SCAPH_CUDA(cudaEventRecord(e->ev_level[2 * level], st));
         SCAPH_CUDA(cudaMemsetAsync(m->act[cur ^ 1], 0, (size_t)e->nwords * 4, st));
         s.visit_cur = m->visit[cur];
@@ -485,9 +489,12 @@ static int ms_run(scaph_engine *e, const uint32_t *srcs, int nsrc, uint32_t *out
     SCAPH_CUDA(cudaEventRecord(e->ev_stop, st));
     SCAPH_CUDA(cudaEventSynchronize(e->ev_stop));
     for (int l = 0; l < level; l++) {
-        float ms = 0;
+        float ms = 0, gap = 0;
         cudaEventElapsedTime(&ms, e->ev_level[2 * l], e->ev_level[2 * l + 1]);
+        if (l > 0) cudaEventElapsedTime(&gap, e->ev_level[2 * l - 1], e->ev_level[2 * l]);
         m->trace[l].ms = ms;
+        m->trace[l].push_ms = gap;
+        m->trace[l].pull_ms = (size_t)l < host_ms.size() ? host_ms[l] : 0.0;
     }
     if (stats) {
         memset(stats, 0, sizeof(*stats));
