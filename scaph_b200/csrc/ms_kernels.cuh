@@ -23,6 +23,12 @@
 #include "engine.h"
 #include "kernel_common.cuh"
 
+// multi-source pull phase B skips the in-edges of vertices that found
+// every source they missed
+#ifndef SCAPH_MS_EARLY_EXIT
+#define SCAPH_MS_EARLY_EXIT 1
+#endif
+
 namespace scaph {
 
 constexpr int kMsPlanes = 12;  // depths below 4096 = kMaxLevels
@@ -430,6 +436,8 @@ __device__ __forceinline__ void ms_pull_body(const GraphDev &g, const MsDev &s, 
     __shared__ uint32_t fnd[kMsTileWords], dne[kMsTileWords];
     __shared__ uint32_t bq_u[B], bq_len[B];
     __shared__ unsigned long long bq_st[B];
+    // phase-B accumulators, seeded with the bits the vertex does not miss:
+    // all ones = every missing source found
     __shared__ Mask<NW> bq_acc[B];
     __shared__ uint32_t bq_qoff[B];
     __shared__ uint32_t wsum[B / 32];
@@ -522,7 +530,8 @@ __device__ __forceinline__ void ms_pull_body(const GraphDev &g, const MsDev &s, 
                 bq_u[bo] = u;
                 bq_st[bo] = st;
                 bq_len[bo] = len;
-                bq_acc[bo] = acc;
+#pragma unroll
+                for (int i = 0; i < NW; i++) bq_acc[bo].w[i] = acc.w[i] | ~miss.w[i];
             }
             __syncthreads();
             // phase B: the remaining in-edges of the unresolved vertices,
@@ -547,13 +556,23 @@ __device__ __forceinline__ void ms_pull_body(const GraphDev &g, const MsDev &s, 
                 }
                 const unsigned long long aa = bq_st[lo] + (s.head_ranked ? 0u : 4u), bb = bq_st[lo] + bq_len[lo];
                 const unsigned long long quad = (aa >> 2) + (i - bq_qoff[lo]);
-                const uint4 val = ld_nc_v4(g.pool + quad * 4);
+                // a vertex whose accumulated masks already hold every source
+                // it misses needs no more of its in-edges: its later quads
+                // are skipped (the accumulator only gains bits, so a stale
+                // read only skips less); the lane stays active for the
+                // segmented OR below
+                bool done_lo = SCAPH_MS_EARLY_EXIT != 0;
+#pragma unroll
+                for (int w2 = 0; w2 < NW; w2++)
+                    done_lo &= *reinterpret_cast<volatile const unsigned long long *>(&bq_acc[lo].w[w2]) == ~0ull;
+                const uint4 val = done_lo ? make_uint4(0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu)
+                                          : ld_nc_v4(g.pool + quad * 4);
                 const uint32_t vals[4] = {val.x, val.y, val.z, val.w};
                 bool in[4], on[4];
                 uint2 ar[4];
 #pragma unroll
                 for (int j = 0; j < 4; j++) {
-                    in[j] = quad * 4 + j >= aa && quad * 4 + j < bb;
+                    in[j] = !done_lo && quad * 4 + j >= aa && quad * 4 + j < bb;
                     ar[j] = in[j] && vals[j] < s.V ? ld_actrank<NW>(s, vals[j]) : make_uint2(0u, 0u);
                     on[j] = (ar[j].x >> (vals[j] & 31)) & 1u;
                     a.inspected += in[j] ? 1 : 0;
