@@ -41,7 +41,7 @@ NOMINAL_HBM_GBS = 8000.0
 # Measured DRAM bytes (read + write) per k_pull launch on RMAT-24: ncu's dram__bytes_read.sum
 # + dram__bytes_write.sum (a 1-pass metric set) over 5 k_pull launches (-s 3 -c 5) of
 # `bench.py --host-loop --steps 2 --warmup 1 --no-cpu --no-extras --no-tune`, mean per launch.
-K_PULL_TRAFFIC_BYTES = 201_652_000
+K_PULL_TRAFFIC_BYTES = 133_429_000
 
 
 def parse_args():
