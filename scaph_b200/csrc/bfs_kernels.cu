@@ -1547,19 +1547,25 @@ __global__ void k_graph_init(BfsGraphArgs a, uint32_t *depth, uint32_t *parent, 
 
 // Last node of each level: counters -> next direction (Beamer alpha/beta, or
 // the forced direction) and the conditionals of the next iteration.
-__global__ void k_decide(BfsGraphArgs a, DecideArgs d, cudaGraphConditionalHandle h_loop)
+// The level's decision, run by one thread (k_decide).  Counters are read
+// through a volatile pointer, so the body also holds where other CTAs of the
+// same launch update them (a last-CTA decision was measured slower:
+// 585 vs 603 GTEPS on RMAT-24).
+__device__ __forceinline__ void decide_body(const BfsGraphArgs &a, const DecideArgs &d,
+                                            cudaGraphConditionalHandle h_loop)
 {
     BfsCtl *c = a.ctl;
     const uint32_t L = c->level;
     LevelCounters *lc = a.ctr0 + L;
+    const volatile LevelCounters *vlc = lc;
     lc->dir = c->dir;
     lc->t_end = globaltimer();
     c->prev_nf = c->nf;
-    c->nf = lc->next;
-    c->mf = lc->next_edges;
+    c->nf = vlc->next;
+    c->mf = vlc->next_edges;
     c->vis_n += c->nf;
     c->vis_e += c->mf;
-    const bool stop = c->nf == 0 || lc->error != 0 || (int)L + 1 >= d.max_levels ||
+    const bool stop = c->nf == 0 || vlc->error != 0 || (int)L + 1 >= d.max_levels ||
                       (unsigned long long)L + 2 >= d.unreached;
     if (stop) {
         c->done = 1;
@@ -1584,6 +1590,11 @@ __global__ void k_decide(BfsGraphArgs a, DecideArgs d, cudaGraphConditionalHandl
     }
     c->level = L + 1;
     cudaGraphSetConditional(h_loop, 1);
+}
+
+__global__ void k_decide(BfsGraphArgs a, DecideArgs d, cudaGraphConditionalHandle h_loop)
+{
+    decide_body(a, d, h_loop);
 }
 
 // Learned variant of k_decide (64 threads): the scheduler's feature row of

@@ -821,6 +821,7 @@ int scaph_engine::build_graph()
     fp.gridDim = dim3(num_sms * 4);
     fp.blockDim = dim3(block);
     fp.kernelParams = fin_args;
+    const bool learned = cfg.direction == SCAPH_DIR_LEARNED && sched;
 #if SCAPH_GRAPH_GIANT_PULL
     // push; giant chunks or pull (one node); [finalize of deferred claims]
     void *giant_pull_args[] = {&gout, &gpull, &gargs};
@@ -854,7 +855,6 @@ int scaph_engine::build_graph()
     SCAPH_CUDA(cudaGraphAddKernelNode(&n_pull, body, &n_before_pull, 1, &lp));
 #endif
 
-    const bool learned = cfg.direction == SCAPH_DIR_LEARNED && sched;
     MlpDev net{};
     if (learned) mlp_device_view(sched, &net);
     void *dec_args[] = {&gargs, &dargs, &h_loop};
@@ -942,10 +942,10 @@ int scaph_engine::collect(bool from_graph)
         if (from_graph) {
             t.ms = (double)(lc.t_end - tprev) * 1e-6;
             tprev = lc.t_end;
-            // push, giant + pull (one node) and decide (and the finalize node
-            // when deferred claims are on) run every level; the unselected
-            // ones leave at once
-            launches += (cfg.push_defer_edges > 0 ? 5 : 4) - (SCAPH_GRAPH_GIANT_PULL ? 1 : 0);
+            // push, giant + pull (one node), the finalize node when deferred
+            // claims are on, and decide run every level; the unselected ones
+            // leave at once
+            launches += 1 + (SCAPH_GRAPH_GIANT_PULL ? 1 : 2) + (cfg.push_defer_edges > 0 ? 1 : 0) + 1;
         } else {
             float ms = 0;
             cudaEventElapsedTime(&ms, ev_level[2 * l], ev_level[2 * l + 1]);
