@@ -28,6 +28,10 @@
 #ifndef SCAPH_MS_EARLY_EXIT
 #define SCAPH_MS_EARLY_EXIT 1
 #endif
+// ... and, resident, hands its tiles out from a counter
+#ifndef SCAPH_MS_DYN_TILES
+#define SCAPH_MS_DYN_TILES 1
+#endif
 
 namespace scaph {
 
@@ -132,6 +136,7 @@ struct MsCounters {
     unsigned long long completed_edges;  // out-degree of vertices that became complete
     unsigned int giant;
     unsigned int error;
+    unsigned int tiles;  // pull tiles handed out so far (MsDev::dyn_tiles)
 };
 
 struct MsDev {
@@ -158,6 +163,10 @@ struct MsDev {
     // L2 where the vertex-indexed array does not.  Null: read visit_cur.
     const uint2 *actrank;
     const unsigned long long *fmask;
+    // pull over the whole range in one launch per level: CTAs take tiles
+    // from ctr->tiles instead of a fixed stride, so that one holding a
+    // hub's long in-list does not leave the others idle at the end
+    uint32_t dyn_tiles;
 };
 
 // Frontier bit of v and, when set, its frontier mask (compacted or
@@ -446,7 +455,17 @@ __device__ __forceinline__ void ms_pull_body(const GraphDev &g, const MsDev &s, 
     __syncthreads();
     MsAcc a;
     const uint32_t ntiles = rl.n ? rl.tile0[rl.n] : (s.nwords + kMsTileWords - 1) / kMsTileWords;
-    for (uint32_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const bool dyn = SCAPH_MS_DYN_TILES && s.dyn_tiles && rl.n == 0;
+    __shared__ uint32_t s_tile;
+    // the CTA's next tile: from the level's counter, or a fixed stride
+    auto next_tile = [&](uint32_t cur) -> uint32_t {
+        if (!dyn) return cur + gridDim.x;
+        __syncthreads();  // every thread has read s_tile
+        if (threadIdx.x == 0) s_tile = atomicAdd(&s.ctr->tiles, 1u);
+        __syncthreads();
+        return s_tile;
+    };
+    for (uint32_t tile = dyn ? next_tile(0) : blockIdx.x; tile < ntiles; tile = next_tile(tile)) {
         uint32_t rlo = 0, rhi = s.V, local;
         range_of_tile(rl, tile, rlo, rhi, local);
         const uint32_t rwhi = (uint32_t)(((unsigned long long)rhi + 31) >> 5);

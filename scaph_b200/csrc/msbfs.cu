@@ -235,6 +235,7 @@ static int ms_run(scaph_engine *e, const uint32_t *srcs, int nsrc, uint32_t *out
     s.head = e->d_head;
     s.indeg = e->d_indeg;
     s.head_ranked = e->head_ranked ? 1u : 0u;
+    s.dyn_tiles = e->pager ? 0u : 1u;  // resident: one pull launch per level
     for (int k = 0; k < kMsPlanes; k++) s.planes[k] = m->planes[k];
 
     uint32_t *d_src = m->d_src;
