@@ -11,6 +11,9 @@ cases:
            k_pull as separate launches), RMAT-S, alpha/beta
   graph    the same traversals as one CUDA-graph launch each
   msbfs    64-source multi-source BFS (k_ms_*), RMAT-S
+  web      128-source multi-source BFS on the web-like graph of the
+           out-of-core batched configuration at 1/2^(25-S) of its size
+           (S=25: 105 M vertices), resident, with its transposed pages
   batch    mixed batch of 64 queries over 8 RMAT graphs (k_bt_*), one launch
   pager    out-of-core BFS through a small page pool (k_page_counts, copies,
            zero-copy reads), RMAT-S
@@ -64,6 +67,21 @@ def case_msbfs(scale: int, reps: int) -> str:
     return f"{reps} x 64-source MS-BFS on RMAT-{scale}: {ms / reps:.3f} ms each"
 
 
+def case_web(scale: int, reps: int) -> str:
+    from . import workloads
+    f = 2.0 ** (scale - 25)
+    csr, tcsr = workloads.config5(V=int(105_000_000 * f), E=int(3_700_000_000 * f))
+    g, gt = PagedGraph.from_csr(csr), PagedGraph.from_csr(tcsr)
+    eng = Engine(g, gt)
+    srcs = _sources(csr, 128, SEED + 4)
+    ms = 0.0
+    for _ in range(reps):
+        _, st = eng.msbfs(srcs)
+        ms += st.ms
+    eng.close()
+    return f"{reps} x 128-source MS-BFS on the web-like graph (V={csr.V}, E={csr.E}): {ms / reps:.3f} ms each"
+
+
 def case_batch(scale: int, reps: int) -> str:
     graphs = [_rmat(max(10, scale - 4 + (i % 4)), seed=SEED + 3000 + i) for i in range(8)]
     rng = np.random.default_rng(SEED + 3)
@@ -112,7 +130,7 @@ def case_mlp(scale: int, reps: int) -> str:
 
 def main(argv=None) -> None:
     ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
-    ap.add_argument("case", choices=["bfs", "graph", "msbfs", "batch", "pager", "mlp"])
+    ap.add_argument("case", choices=["bfs", "graph", "msbfs", "web", "batch", "pager", "mlp"])
     ap.add_argument("--scale", type=int, default=22)
     ap.add_argument("--reps", type=int, default=4)
     a = ap.parse_args(argv)
@@ -120,6 +138,8 @@ def main(argv=None) -> None:
         msg = case_bfs(a.scale, a.reps, a.case == "graph")
     elif a.case == "msbfs":
         msg = case_msbfs(a.scale, a.reps)
+    elif a.case == "web":
+        msg = case_web(a.scale, a.reps)
     elif a.case == "batch":
         msg = case_batch(a.scale, a.reps)
     elif a.case == "pager":
