@@ -167,6 +167,10 @@ struct MsDev {
     // from ctr->tiles instead of a fixed stride, so that one holding a
     // hub's long in-list does not leave the others idle at the end
     uint32_t dyn_tiles;
+    // every vertex is in this level's frontier (the frontier count equals
+    // V): every frontier bit is set and every frontier mask was written
+    // last level, so neighbours' masks are read without their bit
+    uint32_t all_active;
 };
 
 // Frontier bit of v and, when set, its frontier mask (compacted or
@@ -174,6 +178,7 @@ struct MsDev {
 template <int NW>
 __device__ __forceinline__ uint2 ld_actrank(const MsDev &s, uint32_t v)
 {
+    if (s.all_active) return make_uint2(0xFFFFFFFFu, 0u);
     if (s.actrank) return __ldg(&s.actrank[v >> 5]);
     return make_uint2(__ldg(&s.act_cur[v >> 5]), 0u);
 }

@@ -5,6 +5,11 @@
 // app/bfs.cu:137-140).  This file is the host loop: one launch per phase and
 // level, the direction rule between levels, depths unpacked at the end into
 // u32 depth[i][V], bit-exact with single-source BFS.
+// a multi-source level whose frontier holds every vertex skips the
+// frontier-bit lookups
+#ifndef SCAPH_MS_ALL_ACTIVE
+#define SCAPH_MS_ALL_ACTIVE 1
+#endif
 #include <chrono>
 #include <cuda_runtime.h>
 
@@ -406,6 +411,7 @@ static int ms_run(scaph_engine *e, const uint32_t *srcs, int nsrc, uint32_t *out
         const RangeList whole{nullptr, nullptr, nullptr, 0};
         s.actrank = nullptr;
         s.fmask = nullptr;
+        s.all_active = SCAPH_MS_ALL_ACTIVE && level > 0 && nf == V ? 1u : 0u;
         // the frontier's masks compacted in rank order, when that pays: they
         // fit a third of L2 (frontier vertices spread over the V-entry mask
         // array keep a sector each, which does not stay there), and the
@@ -423,6 +429,7 @@ static int ms_run(scaph_engine *e, const uint32_t *srcs, int nsrc, uint32_t *out
             SCAPH_CUDA(cudaGetLastError());
             s.actrank = m->actrank;
             s.fmask = m->fmask;
+            s.all_active = 0u;  // the compacted masks are read by rank
             launches += 3;
         }
         if (e->pager) {

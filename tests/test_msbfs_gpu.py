@@ -115,3 +115,26 @@ def test_msbfs_out_of_core_symmetric_64():
     eng = S.Engine(g, pool_bytes=(g.npages // 2) * g.pagesize * 4)
     check_batch(csr, eng, G.sources(csr, 64, 24))
     eng.close()
+
+
+@pytest.mark.parametrize("pool", [0, 1], ids=["resident", "out_of_core"])
+def test_msbfs_all_vertices_in_frontier(pool):
+    """A small web-like graph (blocks of 4096 ids, every vertex reachable)
+    with 128 sources: the union frontier holds every vertex for some levels,
+    where the pull reads neighbours' masks without their frontier bits.
+    Every row bit-exact, resident and through the pager."""
+    from scaph_b200 import workloads
+
+    csr, tcsr = workloads.config5(V=200_000, E=7_000_000)
+    g = S.PagedGraph.from_csr(csr, pagesize_words=1 << 20)
+    gt = S.PagedGraph.from_csr(tcsr, pagesize_words=1 << 20)
+    total = g.npages + gt.npages
+    eng = S.Engine(g, gt, pool_bytes=(total // 2) * g.pagesize * 4 if pool else 0)
+    srcs = G.sources(csr, 128, 90)
+    depth, st = eng.msbfs(srcs)
+    tr = eng.msbfs_trace()
+    assert any(t["frontier"] == csr.V and t["direction"] == 1 for t in tr), [t["frontier"] for t in tr]
+    for i in range(0, 128, 9):
+        ref = O.bfs(csr.idx, csr.ngh, int(srcs[i]))
+        assert np.array_equal(depth[i], ref), f"row {i}"
+    eng.close()
