@@ -32,6 +32,11 @@
 #ifndef SCAPH_MS_DYN_TILES
 #define SCAPH_MS_DYN_TILES 1
 #endif
+// ... and skips the frontier-bit lookups on levels whose frontier holds
+// every vertex (MsDev::all_active)
+#ifndef SCAPH_MS_ALL_ACTIVE
+#define SCAPH_MS_ALL_ACTIVE 1
+#endif
 
 namespace scaph {
 
@@ -175,10 +180,15 @@ struct MsDev {
 
 // Frontier bit of v and, when set, its frontier mask (compacted or
 // vertex-indexed): the act word (with rank) load, then the mask load.
-template <int NW>
+// ALL: the caller's kernel handles all-active levels (the multi-source
+// engine's pull; the mixed-batch kernels, which never have them, compile
+// without the test: with it their pull ran 9.8 -> 13.0 ms on config 4b)
+template <int NW, bool ALL = false>
 __device__ __forceinline__ uint2 ld_actrank(const MsDev &s, uint32_t v)
 {
-    if (s.all_active) return make_uint2(0xFFFFFFFFu, 0u);
+#if SCAPH_MS_ALL_ACTIVE
+    if (ALL && s.all_active) return make_uint2(0xFFFFFFFFu, 0u);
+#endif
     if (s.actrank) return __ldg(&s.actrank[v >> 5]);
     return make_uint2(__ldg(&s.act_cur[v >> 5]), 0u);
 }
@@ -441,7 +451,9 @@ __device__ __forceinline__ void ms_finalize_body(const MsDev &s)
 // ---------------------------------------------------------------------------
 // pull: incomplete vertices OR the frontier masks of their in-neighbours
 // ---------------------------------------------------------------------------
-template <int NW, int B>
+// ENGINE: the multi-source engine's pull (per-level tile counter and
+// all-active levels); the mixed-batch kernels use neither
+template <int NW, int B, bool ENGINE = false>
 __device__ __forceinline__ void ms_pull_body(const GraphDev &g, const MsDev &s, const RangeList &rl)
 {
     __shared__ PageDev lp[kLutPages];
@@ -460,7 +472,7 @@ __device__ __forceinline__ void ms_pull_body(const GraphDev &g, const MsDev &s, 
     __syncthreads();
     MsAcc a;
     const uint32_t ntiles = rl.n ? rl.tile0[rl.n] : (s.nwords + kMsTileWords - 1) / kMsTileWords;
-    const bool dyn = SCAPH_MS_DYN_TILES && s.dyn_tiles && rl.n == 0;
+    const bool dyn = ENGINE && SCAPH_MS_DYN_TILES && s.dyn_tiles && rl.n == 0;
     __shared__ uint32_t s_tile;
     // the CTA's next tile: from the level's counter, or a fixed stride
     auto next_tile = [&](uint32_t cur) -> uint32_t {
@@ -524,7 +536,7 @@ __device__ __forceinline__ void ms_pull_body(const GraphDev &g, const MsDev &s, 
                 uint2 ar[4];
 #pragma unroll
                 for (int j = 0; j < 4; j++) {
-                    ar[j] = v[j] < s.V ? ld_actrank<NW>(s, v[j]) : make_uint2(0u, 0u);
+                    ar[j] = v[j] < s.V ? ld_actrank<NW, ENGINE>(s, v[j]) : make_uint2(0u, 0u);
                     on[j] = (ar[j].x >> (v[j] & 31)) & 1u;
                 }
 #pragma unroll
@@ -597,7 +609,7 @@ __device__ __forceinline__ void ms_pull_body(const GraphDev &g, const MsDev &s, 
 #pragma unroll
                 for (int j = 0; j < 4; j++) {
                     in[j] = !done_lo && quad * 4 + j >= aa && quad * 4 + j < bb;
-                    ar[j] = in[j] && vals[j] < s.V ? ld_actrank<NW>(s, vals[j]) : make_uint2(0u, 0u);
+                    ar[j] = in[j] && vals[j] < s.V ? ld_actrank<NW, ENGINE>(s, vals[j]) : make_uint2(0u, 0u);
                     on[j] = (ar[j].x >> (vals[j] & 31)) & 1u;
                     a.inspected += in[j] ? 1 : 0;
                 }
@@ -697,7 +709,7 @@ __global__ void __launch_bounds__(kMsBlock) k_ms_finalize(MsDev s)
 template <int NW>
 __global__ void __launch_bounds__(kMsBlock) k_ms_pull(GraphDev g, MsDev s, RangeList rl)
 {
-    ms_pull_body<NW, kMsBlock>(g, s, rl);
+    ms_pull_body<NW, kMsBlock, true>(g, s, rl);
 }
 
 // clears the frontier masks of the source vertices (left over from an

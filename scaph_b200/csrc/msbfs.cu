@@ -5,11 +5,6 @@
 // app/bfs.cu:137-140).  This file is the host loop: one launch per phase and
 // level, the direction rule between levels, depths unpacked at the end into
 // u32 depth[i][V], bit-exact with single-source BFS.
-// a multi-source level whose frontier holds every vertex skips the
-// frontier-bit lookups
-#ifndef SCAPH_MS_ALL_ACTIVE
-#define SCAPH_MS_ALL_ACTIVE 1
-#endif
 #include <chrono>
 #include <cuda_runtime.h>
 
