@@ -18,8 +18,9 @@ engine's size (pages a push needs: out-pages holding the frontier; a pull:
 in-pages holding unvisited vertices) at the PCIe bandwidth; the cheapest
 sequence labels the levels.  The residency and previous-direction features
 of the training rows are recomputed along that sequence.  The alpha/beta
-switch stays the fallback and the judge: the network only picks directions
-and prefetches pages, the depths never change.
+switch stays the fallback and the yardstick of its per-level time and page
+traffic: the network only picks directions and prefetches pages, the
+depths never change.
 """
 from __future__ import annotations
 
