@@ -162,15 +162,18 @@ def tune_engine(eng: Engine, sources, ptr: int, multi: bool = False, repeats: in
     """Coordinate search over the engine's tunables on the caller's own
     workload: `sources` run one by one (single-source; `ptr` a device
     buffer of V words) or as one multi-source batch (`ptr`: len(sources) * V
-    words).  Single-source: CTAs per SM, the giant-chunk cut, the pull
-    gather ratio, the warp-centric pull, the deferred-claim push threshold,
-    alpha, beta; multi-source: the mask-compaction thresholds,
-    alpha, beta.  Each candidate is timed best of `repeats` (device time);
+    words).  Single-source: when pull reads the 8-byte records and which
+    phase-A layout it reads elsewhere, the sparse push and pull
+    front-ends, the pull kernel's shape, the deferred-claim push threshold,
+    CTAs per SM, the giant-chunk cut, the pull gather ratio, alpha, beta;
+    multi-source: the mask-compaction thresholds, alpha, beta.  Each
+    candidate is timed best of `repeats` (device time);
     the default's spread over `repeats` more runs is reported beside the
     result, so a gain can be told from noise.  The chosen tunables must
     reproduce the default's depths (checksum).  The best setting is adopted
     only if it beats the default by more than the default's spread; the
-    adopted one is set and returned under "params"."""
+    adopted one is set and returned under "params" (tests/test_autotune.py
+    checks these rules against a fake engine)."""
     t0 = time.time()
     start = eng.tunables()
     ref_sum = _engine_checksum(eng, sources, multi)
