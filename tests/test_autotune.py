@@ -3,7 +3,9 @@ fake engine whose device times are a function of its tunables: a setting
 that is clearly faster is adopted (and confirmed by interleaved reruns);
 gains inside the default's own run-to-run spread leave the defaults; a
 setting that changes the depths is refused and the defaults restored; the
-multi-source search covers its own axes."""
+multi-source search covers its own axes; the mixed-batch tuner finds the
+best launch shape and reuses it from its cache for a batch of the same
+shape."""
 import numpy as np
 import pytest
 
@@ -112,3 +114,48 @@ def test_multi_source_search_uses_its_own_axes():
     r = autotune.tune_engine(eng, list(range(64)), 0, multi=True)
     assert r["adopted"] == "tuned" and r["params"]["ms_compact_l2_div"] == 6
     assert r["params"]["pull_warp"] == eng.p["pull_warp"]  # single-source axes untouched
+
+
+class FakeGraph:
+    def __init__(self, E):
+        self.E = E
+
+
+class FakeBatch:
+    """A mixed batch whose launch time depends on its parameters."""
+
+    def __init__(self, best=(512, 2, 20.0, 24.0)):
+        self.sizes = [1000, 2000]
+        self.graphs = [FakeGraph(10_000), FakeGraph(30_000)]
+        self.params = {"block_size": 256, "ctas_per_sm": 4, "alpha": 14.0, "beta": 24.0}
+        self.best = best
+        self.runs = 0
+
+    def set_params(self, b, c, a, bt):
+        self.params = {"block_size": b, "ctas_per_sm": c, "alpha": a, "beta": bt}
+
+    def _ms(self):
+        p = self.params
+        return 1.0 + sum(x != y for x, y in zip((p["block_size"], p["ctas_per_sm"], p["alpha"], p["beta"]),
+                                                 self.best))
+
+    def run_device(self, queries, ptr):
+        self.runs += 1
+        return _Stats(self._ms())
+
+    def run(self, queries):
+        return [np.arange(8, dtype=np.uint32) + np.uint32(g) for g, _ in queries], _Stats(self._ms())
+
+
+def test_batch_tuner_finds_the_best_shape_and_caches_it(tmp_path):
+    cache = str(tmp_path / "tune.json")
+    queries = [(0, 1), (1, 5), (1, 7)]
+    b = FakeBatch(best=(512, 2, 20.0, 24.0))
+    r = autotune.tune_batch(b, queries, 0, cache=cache)
+    assert not r["cached"] and r["ms"] < r["default_ms"]
+    assert (r["params"]["block_size"], r["params"]["ctas_per_sm"], r["params"]["alpha"]) == (512, 2, 20.0)
+    assert b.params == r["params"]
+    # a second batch of the same shape takes the cached choice without timing
+    b2 = FakeBatch(best=(512, 2, 20.0, 24.0))
+    r2 = autotune.tune_batch(b2, queries, 0, cache=cache)
+    assert r2["cached"] and b2.runs == 0 and b2.params == r["params"]
